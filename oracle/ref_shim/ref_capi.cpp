@@ -1,0 +1,308 @@
+// C-ABI wrapper that drives the reference's OWN CPU ComputeUnit, compiled in
+// place from the reference sources (tdlbcpp/src) by oracle/Makefile into
+// oracle/_ref/libtdlb_ref.so.
+//
+// TEST INFRASTRUCTURE ONLY. Nothing in the product links or loads this file;
+// only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it,
+// and only as the checker / the timed reference arm.
+//
+// What it exposes:
+//   * a ComputeUnit<T,18,IJKL,EgglesSomers,{Simple|Esotwist},CPU> instance
+//     for T=float (the reference's production precision, main.cpp:50) and
+//     T=double (the FP64 oracle), stepped through the reference's own virtuals
+//     in main.cpp's order (main.cpp:438-455);
+//   * field read/write in the reference's AoS layout (Field.hpp:18-42),
+//     returned as double (float->double is exact);
+//   * integer-coded known-answer tests on the reference's own code:
+//     the Simple push golden vectors of tests/StreamingSimplePushTest.hpp,
+//     and the Esotwist read/write/writeMoments maps (StreamingEsoteric.hpp:28-180).
+#include <cstdint>
+#include <cstring>
+#include <cstdlib>
+#include <string>
+#include <vector>
+#include <iostream>
+#include <sstream>
+
+#include "Header.h"
+#include "ComputeUnit.h"
+#if TDLBREF_WITH_GOLDEN
+#include "StreamingSimplePushTest.hpp"
+#include "StreamingSimpleTest.hpp"
+#endif
+
+namespace {
+
+struct MarkerC {  // layout of tdlb_marker in include/tdlb_b200.h
+    int64_t i, j, k;
+    float iCartFraction, kCartFraction, uDelta, vDelta, wDelta, pad;
+};
+
+struct FlowC {    // layout of tdlbref_flow below
+    double initialRho, nu, cs0, g3, alpha, beta;
+    int32_t useLES;
+    int32_t pad;
+};
+
+// Silence the reference's directory-creation chatter on stdout while the
+// ComputeUnit / DiskOutputTree are constructed.
+struct MuteCout {
+    std::streambuf* old;
+    std::ostringstream sink;
+    MuteCout() : old(std::cout.rdbuf(sink.rdbuf())) {}
+    ~MuteCout() { std::cout.rdbuf(old); }
+};
+
+DiskOutputTree makeTree(const std::string& tmpdir) {
+    OutputParams out(tmpdir + "/ref_output");
+    CheckpointParams chk;
+    chk.checkpointWriteRootDir = tmpdir;
+    chk.checkpointWriteDirPrefix = "ref";
+    return DiskOutputTree(out, chk);
+}
+
+ComputeUnitParams makeCuParams(long x, long y, long z) {
+    ComputeUnitParams cu;
+    cu.nodeID = 0; cu.deviceID = -1;
+    cu.idi = cu.idj = cu.idk = 0;
+    cu.x = x; cu.y = y; cu.z = z;
+    cu.i0 = cu.j0 = cu.k0 = 0;
+    cu.ghost = 1;           // main.cpp:225 (grid.multiStep = 1)
+    cu.resolution = 1;
+    return cu;
+}
+
+struct Handle {
+    int precision;          // 4 or 8
+    int streaming;          // 0 Simple, 1 Esotwist
+    void* cu;               // ComputeUnitBase<T,18,IJKL>*
+};
+
+template <typename T>
+using Base = ComputeUnitBase<T, QLen::D3Q19, MemoryLayoutIJKL>;
+
+template <typename T>
+Base<T>* create(int streaming, long x, long y, long z, const FlowC* f, const char* tmpdir) {
+    FlowParams<T> flow;
+    flow.initialRho = T(f->initialRho);
+    flow.nu = T(f->nu);
+    flow.cs0 = T(f->cs0);
+    flow.g3 = T(f->g3);
+    flow.alpha = T(f->alpha);
+    flow.beta = T(f->beta);
+    flow.useLES = f->useLES != 0;
+    flow.streaming = streaming == 0 ? "Simple" : "Esotwist";
+    MuteCout mute;
+    DiskOutputTree tree = makeTree(tmpdir ? tmpdir : "/tmp");
+    ComputeUnitParams cu = makeCuParams(x, y, z);
+    if (streaming == 0)
+        return new ComputeUnit<T, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, Simple, CPU>(cu, flow, tree);
+    return new ComputeUnit<T, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, Esotwist, CPU>(cu, flow, tree);
+}
+
+template <typename T>
+void forcing(Base<T>* cu, const MarkerC* m, long n, double alpha, double beta) {
+    std::vector<PosPolar<tNi, T>> geom((size_t)n);
+    for (long q = 0; q < n; q++) {
+        geom[q].i = m[q].i; geom[q].j = m[q].j; geom[q].k = m[q].k;
+        geom[q].iCartFraction = T(m[q].iCartFraction);
+        geom[q].kCartFraction = T(m[q].kCartFraction);
+        geom[q].uDelta = T(m[q].uDelta);
+        geom[q].vDelta = T(m[q].vDelta);
+        geom[q].wDelta = T(m[q].wDelta);
+    }
+    cu->forcing(geom, T(alpha), T(beta));
+}
+
+template <typename T> Base<T>* as(Handle* h) { return static_cast<Base<T>*>(h->cu); }
+
+// Integer-coded fill of tests/Params/ParamsCommon.hpp:168-206 (offset 0,
+// two-digit coordinates): Q(i,j,k,l) = ((i*100+j)*100+k)*100+l.
+template <typename CU>
+void fillCoded(CU& cu) {
+    for (tNi i = 0; i < cu.xg; i++)
+        for (tNi j = 0; j < cu.yg; j++)
+            for (tNi k = 0; k < cu.zg; k++) {
+                unsigned long base = ((i * 100ul + j) * 100ul + k) * 100ul;
+                for (int l = 0; l < QLen::D3Q19; l++) cu.Q[cu.index(i, j, k)].q[l] = base + l;
+                cu.F[cu.index(i, j, k)].x = base;
+                cu.F[cu.index(i, j, k)].y = base + 1;
+                cu.F[cu.index(i, j, k)].z = base + 2;
+                cu.Nu[cu.index(i, j, k)] = base + 1;
+                cu.O[cu.index(i, j, k)] = true;
+            }
+}
+
+template <typename CU>
+void dumpQ(CU& cu, uint64_t* out) {
+    for (size_t c = 0; c < cu.size; c++)
+        for (int l = 0; l < QLen::D3Q19; l++) out[c * 18 + l] = cu.Q[c].q[l];
+}
+
+}  // namespace
+
+extern "C" {
+
+typedef FlowC tdlbref_flow;
+typedef MarkerC tdlbref_marker;
+
+void* tdlbref_create(int precision, int streaming, long x, long y, long z,
+                     const tdlbref_flow* flow, const char* tmpdir) {
+    if ((precision != 4 && precision != 8) || (streaming != 0 && streaming != 1)) return nullptr;
+    if (x < 1 || y < 1 || z < 1) return nullptr;
+    Handle* h = new Handle{precision, streaming, nullptr};
+    if (precision == 4) h->cu = create<float>(streaming, x, y, z, flow, tmpdir);
+    else h->cu = create<double>(streaming, x, y, z, flow, tmpdir);
+    return h;
+}
+
+void tdlbref_destroy(void* hv) {
+    Handle* h = (Handle*)hv;
+    if (!h) return;
+    if (h->precision == 4) delete as<float>(h); else delete as<double>(h);
+    delete h;
+}
+
+#define TDLBREF_DISPATCH(h, call) \
+    do { if ((h)->precision == 4) { auto cu = as<float>(h); call; } else { auto cu = as<double>(h); call; } } while (0)
+
+long tdlbref_size(void* hv) { Handle* h = (Handle*)hv; long s = 0; TDLBREF_DISPATCH(h, s = (long)cu->size); return s; }
+int tdlbref_even_step(void* hv) { Handle* h = (Handle*)hv; int e = 0; TDLBREF_DISPATCH(h, e = cu->evenStep ? 1 : 0); return e; }
+void tdlbref_set_even_step(void* hv, int even) { Handle* h = (Handle*)hv; TDLBREF_DISPATCH(h, cu->evenStep = (even != 0)); }
+void tdlbref_set_nu(void* hv, double nu) { Handle* h = (Handle*)hv; TDLBREF_DISPATCH(h, cu->flow.nu = nu); }
+
+void tdlbref_initialise(void* hv, double rho) { Handle* h = (Handle*)hv; TDLBREF_DISPATCH(h, cu->initialise(rho)); }
+void tdlbref_collision(void* hv) { Handle* h = (Handle*)hv; TDLBREF_DISPATCH(h, cu->collision()); }
+void tdlbref_bounce_back(void* hv) { Handle* h = (Handle*)hv; TDLBREF_DISPATCH(h, cu->bounceBackBoundary()); }
+void tdlbref_streaming_push(void* hv) { Handle* h = (Handle*)hv; TDLBREF_DISPATCH(h, cu->streamingPush()); }
+void tdlbref_moments(void* hv) { Handle* h = (Handle*)hv; TDLBREF_DISPATCH(h, cu->moments()); }
+void tdlbref_forcing(void* hv, const tdlbref_marker* m, long n, double alpha, double beta) {
+    Handle* h = (Handle*)hv;
+    if (h->precision == 4) forcing<float>(as<float>(h), m, n, alpha, beta);
+    else forcing<double>(as<double>(h), m, n, alpha, beta);
+}
+
+// One time step in main.cpp's order (main.cpp:438-454).
+void tdlbref_step(void* hv, const tdlbref_marker* m, long n, double alpha, double beta) {
+    tdlbref_collision(hv);
+    tdlbref_bounce_back(hv);
+    tdlbref_streaming_push(hv);
+    tdlbref_moments(hv);
+    tdlbref_forcing(hv, m, n, alpha, beta);
+}
+
+void tdlbref_get_q(void* hv, double* out) {
+    Handle* h = (Handle*)hv;
+    TDLBREF_DISPATCH(h, for (size_t c = 0; c < cu->size; c++) for (int l = 0; l < 18; l++) out[c * 18 + l] = (double)cu->Q[c].q[l]);
+}
+void tdlbref_set_q(void* hv, const double* in) {
+    Handle* h = (Handle*)hv;
+    TDLBREF_DISPATCH(h, for (size_t c = 0; c < cu->size; c++) for (int l = 0; l < 18; l++) cu->Q[c].q[l] = in[c * 18 + l]);
+}
+void tdlbref_get_f(void* hv, double* out) {
+    Handle* h = (Handle*)hv;
+    TDLBREF_DISPATCH(h, for (size_t c = 0; c < cu->size; c++) { out[c * 3] = cu->F[c].x; out[c * 3 + 1] = cu->F[c].y; out[c * 3 + 2] = cu->F[c].z; });
+}
+void tdlbref_set_f(void* hv, const double* in) {
+    Handle* h = (Handle*)hv;
+    TDLBREF_DISPATCH(h, for (size_t c = 0; c < cu->size; c++) { cu->F[c].x = in[c * 3]; cu->F[c].y = in[c * 3 + 1]; cu->F[c].z = in[c * 3 + 2]; });
+}
+void tdlbref_get_nu(void* hv, double* out) {
+    Handle* h = (Handle*)hv;
+    TDLBREF_DISPATCH(h, for (size_t c = 0; c < cu->size; c++) out[c] = cu->Nu[c]);
+}
+void tdlbref_set_nu_field(void* hv, const double* in) {
+    Handle* h = (Handle*)hv;
+    TDLBREF_DISPATCH(h, for (size_t c = 0; c < cu->size; c++) cu->Nu[c] = in[c]);
+}
+
+// ---------------------------------------------------------------------------
+// Integer-coded known-answer tests (T = unsigned long, as in
+// tests/StreamingSimpleTest.cpp:74 and :110).
+// ---------------------------------------------------------------------------
+
+// Simple push (push=1) or pull (push=0) on the coded fill of an x*y*z
+// interior with ghost 1. out: xg*yg*zg*18 values in AoS order.
+int tdlbref_kat_simple_stream(int push, long x, long y, long z, uint64_t* out) {
+    MuteCout mute;
+    FlowParams<unsigned long> flow;
+    DiskOutputTree tree = makeTree("/tmp");
+    ComputeUnit<unsigned long, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, Simple, CPU> cu(makeCuParams(x, y, z), flow, tree);
+    if (cu.xg > 99 || cu.yg > 99 || cu.zg > 99) return 1;
+    fillCoded(cu);
+    if (push) cu.streamingPush(); else cu.streamingPull();
+    dumpQ(cu, out);
+    return 0;
+}
+
+// The reference's committed golden vectors (tests/StreamingSimplePushTest.hpp
+// and tests/StreamingSimpleTest.hpp) for the 3x3x3 interior, ghost 1.
+int tdlbref_kat_simple_golden(int push, uint64_t* out) {
+#if TDLBREF_WITH_GOLDEN
+    MuteCout mute;
+    FlowParams<unsigned long> flow;
+    DiskOutputTree tree = makeTree("/tmp");
+    ComputeUnit<unsigned long, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, Simple, CPU> cu(makeCuParams(3, 3, 3), flow, tree);
+    if (push) TestUtils::fillExpectedComputeUnitValuesTestStreamingNievePush(cu);
+    else TestUtils::fillExpectedComputeUnitValuesTestStreamingNieve(cu);
+    dumpQ(cu, out);
+    return 0;
+#else
+    (void)push; (void)out;
+    return 2;
+#endif
+}
+
+// Esotwist transport on the coded fill: nsteps times, for every interior
+// cell, q = AccessField::read(i,j,k); AccessField::write(q,i,j,k); then flip
+// evenStep as streamingPush does (StreamingEsoteric.hpp:15-18). With
+// moments_map != 0 the step instead applies read + writeMoments (the map
+// moments() uses, CollisionEgglesSomers.hpp:196,248) without a flip.
+int tdlbref_kat_esotwist(long x, long y, long z, int start_even, int nsteps, int moments_map, uint64_t* out) {
+    MuteCout mute;
+    FlowParams<unsigned long> flow;
+    DiskOutputTree tree = makeTree("/tmp");
+    using CU = ComputeUnit<unsigned long, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, Esotwist, CPU>;
+    using AF = AccessField<unsigned long, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, Esotwist>;
+    CU cu(makeCuParams(x, y, z), flow, tree);
+    if (cu.xg > 99 || cu.yg > 99 || cu.zg > 99) return 1;
+    fillCoded(cu);
+    cu.evenStep = start_even != 0;
+    for (int s = 0; s < nsteps; s++) {
+        for (tNi i = 1; i <= cu.xg1; i++)
+            for (tNi j = 1; j <= cu.yg1; j++)
+                for (tNi k = 1; k <= cu.zg1; k++) {
+                    QVec<unsigned long, QLen::D3Q19> q = AF::read(cu, i, j, k);
+                    if (moments_map) AF::writeMoments(cu, q, i, j, k);
+                    else AF::write(cu, q, i, j, k);
+                }
+        if (!moments_map) cu.streamingPush();
+    }
+    dumpQ(cu, out);
+    return 0;
+}
+
+// Esotwist read map alone: for every interior cell, the 18 values
+// AccessField::read returns on the coded fill (parity even/odd).
+// out: x*y*z*18 values, interior cells in (i,j,k) order.
+int tdlbref_kat_esotwist_read(long x, long y, long z, int even, uint64_t* out) {
+    MuteCout mute;
+    FlowParams<unsigned long> flow;
+    DiskOutputTree tree = makeTree("/tmp");
+    using CU = ComputeUnit<unsigned long, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, Esotwist, CPU>;
+    using AF = AccessField<unsigned long, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, Esotwist>;
+    CU cu(makeCuParams(x, y, z), flow, tree);
+    if (cu.xg > 99 || cu.yg > 99 || cu.zg > 99) return 1;
+    fillCoded(cu);
+    cu.evenStep = even != 0;
+    size_t c = 0;
+    for (tNi i = 1; i <= cu.xg1; i++)
+        for (tNi j = 1; j <= cu.yg1; j++)
+            for (tNi k = 1; k <= cu.zg1; k++, c++) {
+                QVec<unsigned long, QLen::D3Q19> q = AF::read(cu, i, j, k);
+                for (int l = 0; l < 18; l++) out[c * 18 + l] = q.q[l];
+            }
+    return 0;
+}
+
+}  // extern "C"
