@@ -1,0 +1,223 @@
+/*
+ * tdlb_b200.h -- C ABI of the B200-native lattice Boltzmann time step.
+ *
+ * A drop-in for the hot path of TurbulentDynamics/tdLBCpp: one ComputeUnit
+ * (D3Q19 with 18 moving populations, Eggels-Somers collision with optional
+ * Smagorinsky LES, Simple or Esotwist streaming, the reference's wall rule,
+ * Rushton-turbine immersed-boundary forcing) held on one GPU.
+ *
+ * Each entry point names the reference interface it replaces
+ * (tdlbcpp/src/<file>:<line>). Plain pointers and sizes only; every call
+ * returns 0 on success or a negative TDLB_E* code, and tdlb_last_error()
+ * gives the message of the last failure on that handle. There is no CPU
+ * fallback: a process without a usable sm_100 GPU gets TDLB_ECUDA from
+ * tdlb_create().
+ *
+ * Threading: a handle owns one CUDA stream; calls on one handle must not
+ * race each other. Results of device work are visible to the host after the
+ * reading calls (tdlb_read_*, tdlb_checkpoint_write, tdlb_synchronize).
+ */
+#ifndef TDLB_B200_H
+#define TDLB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TDLB_ABI_VERSION 1
+
+/* status codes */
+#define TDLB_OK 0
+#define TDLB_EINVAL (-1)   /* bad argument (sizes, marker out of range, bad JSON value) */
+#define TDLB_ECUDA (-2)    /* CUDA runtime error / no usable device */
+#define TDLB_ENOMEM (-3)   /* device or host allocation failed */
+#define TDLB_EIO (-4)      /* file missing, unreadable or truncated */
+#define TDLB_ESTATE (-5)   /* call not valid in the current state */
+#define TDLB_EJSON (-6)    /* input JSON malformed or missing a required key */
+
+/* streaming schemes (FlowParams::streaming, main.cpp:242-256) */
+#define TDLB_STREAMING_SIMPLE 0
+#define TDLB_STREAMING_ESOTWIST 1
+
+/* population storage precision */
+#define TDLB_STORAGE_FP32 0
+
+typedef struct tdlb_lattice* tdlb_handle;
+
+/* An immersed-boundary marker: the fields of the reference's
+ * PosPolar<tNi,T> that forcing() reads (Forcing.hpp:72-150), cell indices in
+ * interior coordinates (0 <= i < x, 0 <= j < y, 0 <= k < z; the reference adds
+ * its ghost width). 48 bytes. */
+typedef struct tdlb_marker {
+    int64_t i, j, k;
+    float iCartFraction;
+    float kCartFraction;
+    float uDelta, vDelta, wDelta;
+    float pad;
+} tdlb_marker;
+
+/* Programmatic configuration: the GridParams / FlowParams keys the time step
+ * reads (Params/GridParams.hpp:24-32, Params/FlowParams.hpp:24-61). */
+typedef struct tdlb_config {
+    int64_t x, y, z;          /* interior lattice (GridParams x, y, z) */
+    int32_t streaming;        /* TDLB_STREAMING_* */
+    int32_t storage;          /* TDLB_STORAGE_* */
+    double initialRho;
+    double nu;                /* kinematic viscosity (FlowParams::nu, set by calcNuAndRe_m) */
+    double cs0;               /* Smagorinsky constant */
+    double g3;                /* third-order relaxation */
+    double alpha, beta;       /* IBM force relaxation (forcing(geom, alpha, beta)) */
+    int32_t useLES;
+    int32_t reserved;
+} tdlb_config;
+
+/* Replaces: the ComputeUnit constructor + allocateMemory
+ * (ComputeUnit.hpp:125-133, ComputeUnitGpu.hpp:31-47) as driven by main.cpp
+ * from the input JSON (main.cpp:135-164, :213-256). `params_json` is the text
+ * of the reference's input file (GridParams, FlowParams, RunningParams ... ;
+ * keys as in input_debug_gridx60_numSteps20.json). FlowParams.nu == 0 is
+ * replaced by calcNuAndRe_m(impellerBladeOuterRadius = int(x/6))
+ * (FlowParams.hpp:65-70, main.cpp:275). */
+int tdlb_create(const char* params_json, int device, tdlb_handle* out);
+
+/* Same, from a filled tdlb_config (nu used as given). */
+int tdlb_create_config(const tdlb_config* cfg, int device, tdlb_handle* out);
+
+/* Replaces: ~ComputeUnitBase / freeMemory (ComputeUnit.hpp:150-154). */
+int tdlb_destroy(tdlb_handle h);
+
+/* Message of the last failed call on h (or of the last failed create when
+ * h is NULL). Never NULL. */
+const char* tdlb_last_error(tdlb_handle h);
+
+/* Replaces: ComputeUnitBase::initialise(T rho) (ComputeUnit.hpp:175-190,
+ * GPU ComputeUnitGpu.hpp:209-222): moments (rho, 0, ..., 0), F = Nu = 0,
+ * Esotwist parity even. */
+int tdlb_initialise(tdlb_handle h, float rho);
+
+/* Replaces: forcing(std::vector<PosPolar>&, alfa, beta)
+ * (ComputeUnit.h:113, Forcing.hpp:56-176, GPU ComputeUnitGpu.hpp:279-294).
+ * Uploads the markers (host pointer, list order = application order),
+ * schedules them and runs the immersed-boundary kernels on the current
+ * moments. The marker list stays resident for tdlb_forcing_resident(). */
+int tdlb_forcing(tdlb_handle h, const tdlb_marker* markers, size_t n, float alpha, float beta);
+
+/* Upload + schedule markers without applying them. */
+int tdlb_set_markers(tdlb_handle h, const tdlb_marker* markers, size_t n);
+
+/* forcing() with the resident marker list. */
+int tdlb_forcing_resident(tdlb_handle h, float alpha, float beta);
+
+/* Replaces: collision() (CollisionEgglesSomers.hpp:27-181, GPU
+ * CollisionEgglesSomers.cuh:17-154) TOGETHER WITH the streaming and
+ * moments that follow it: one fused launch streams, forms moments and
+ * collides every cell. */
+int tdlb_collision(tdlb_handle h);
+
+/* Replace: bounceBackBoundary() (Boundary.hpp:13-35), streamingPush()
+ * (StreamingSimple.hpp:257-307, StreamingEsoteric.hpp:14-18) and moments()
+ * (CollisionEgglesSomers.hpp:185-256). Their work is inside
+ * tdlb_collision(); these keep the reference's call sequence valid and
+ * return 0 (streamingPush() flips the Esotwist parity in the reference; here
+ * the fused launch does). */
+int tdlb_bounce_back(tdlb_handle h);
+int tdlb_streaming_push(tdlb_handle h);
+int tdlb_moments(tdlb_handle h);
+
+/* One reference time step, main.cpp:438-454 order: collision (fused) then
+ * forcing with the resident markers. */
+int tdlb_step(tdlb_handle h, float alpha, float beta);
+
+/* Interior moments as the reference's Q holds them after moments()
+ * (QVec slots M01..M18), AoS: out[((i*y + j)*z + k)*18 + l]. */
+int tdlb_read_moments(tdlb_handle h, float* out);
+
+/* Density and velocity u = (j + F/2)/rho (QVec.hpp:385-394) of every
+ * interior cell, each array x*y*z in (i, j, k) order. Any pointer may be
+ * NULL. */
+int tdlb_read_velocity_density(tdlb_handle h, float* rho, float* ux, float* uy, float* uz);
+
+/* Interior F (3 per cell, AoS; zero where no marker touched the cell), the
+ * eddy viscosity Nu (1 per cell) and the touched flags of the last forcing
+ * pass (1 byte per cell). */
+int tdlb_read_force(tdlb_handle h, float* f3);
+int tdlb_read_nu(tdlb_handle h, float* nu);
+int tdlb_read_touched(tdlb_handle h, uint8_t* flags);
+
+/* Lattice shape and state. */
+int tdlb_get_dims(tdlb_handle h, int64_t* x, int64_t* y, int64_t* z);
+int tdlb_get_even_step(tdlb_handle h, int* even);
+
+/* Make all queued device work complete. */
+int tdlb_synchronize(tdlb_handle h);
+
+/* ---- Rushton-turbine geometry (host only; no GPU needed) ----
+ * Replaces the un-vendored tdLBGeometryRushtonTurbineLib calls of main.cpp
+ * (RushtonTurbinePolarCPP::generateFixedGeometry, :289-290;
+ * generateRotatingNonUpdatingGeometry, :293-294; generateRotatingGeometry /
+ * updateRotatingGeometry, :297-298 and :424-425; calcThisStepImpellerIncrement,
+ * :286 and :409; RushtonTurbine::impellers[0].blades.outerRadius, :275).
+ * This is the project's own geometry (spec in tdlbcpp_b200/csrc/geometry.cpp);
+ * zero-valued fields take their defaults (T = x, D = T/3, clearance T/3,
+ * blade height D/5, 1 disk plane, 6 blades, 4 baffles of width T/10, wall
+ * inset 2 cells). Each generator writes at most `cap` markers to `out` and
+ * the full count to *n; out == NULL only queries the count. */
+typedef struct tdlb_rushton {
+    int64_t x, y, z;
+    double tank_diameter;
+    double impeller_diameter;
+    double clearance;
+    double blade_height;
+    double disk_thickness;
+    int32_t n_blades;
+    int32_t n_baffles;
+    double baffle_width;
+    double wall_inset;
+    double tip_speed;          /* FlowParams::uav */
+    int64_t startup_steps;     /* RunningParams::impellerStartupStepsUntilNormalSpeed */
+} tdlb_rushton;
+
+int tdlb_rushton_fixed(const tdlb_rushton* spec, tdlb_marker* out, size_t cap, size_t* n);
+int tdlb_rushton_rotating_nonupdating(const tdlb_rushton* spec, double delta_angle, tdlb_marker* out, size_t cap, size_t* n);
+int tdlb_rushton_rotating(const tdlb_rushton* spec, double angle, double delta_angle, tdlb_marker* out, size_t cap, size_t* n);
+double tdlb_rushton_impeller_increment(const tdlb_rushton* spec, uint64_t step);
+int tdlb_rushton_blade_outer_radius(const tdlb_rushton* spec);
+
+/* Resident impeller (replaces main.cpp:409-426, which regenerates the
+ * rotating markers on the host and re-uploads the whole list every step):
+ * generates the spec's fixed, rotating-non-updating (velocities from
+ * nonupdating_delta_angle, as main.cpp:293) and rotating markers at
+ * (angle, delta_angle), keeps them on the device in that list order, and
+ * schedules the blades for every angle at once. Afterwards
+ * tdlb_rotate_impeller() moves the blades on the device and
+ * tdlb_forcing_resident()/tdlb_step() apply the list. The impeller must sit
+ * at least 2 cells inside the lattice at every angle. */
+int tdlb_attach_rushton(tdlb_handle h, const tdlb_rushton* spec, double nonupdating_delta_angle, double angle,
+                        double delta_angle);
+int tdlb_rotate_impeller(tdlb_handle h, double angle, double delta_angle);
+
+/* Copy of the resident marker list as the device holds it (list order). */
+int tdlb_read_markers(tdlb_handle h, tdlb_marker* out, size_t cap, size_t* n);
+
+/* Immersed-boundary schedule of a marker list (host only): the per-plane
+ * level of every marker (level_out[n], may be NULL) and the largest number
+ * of levels in one plane. Markers of one level share no stencil cell. */
+int tdlb_schedule_levels(const tdlb_marker* markers, size_t n, int64_t x, int64_t y, int64_t z,
+                         int32_t* level_out, int32_t* max_levels_per_plane);
+
+/* ---- known-answer-test support (integer-coded transport) ----
+ * Raw population state: for Simple the current buffer, for Esotwist the
+ * single in-place buffer. Layout: out[((i*y + j)*z + k)*18 + slot]. */
+int tdlb_debug_get_state(tdlb_handle h, float* out);
+int tdlb_debug_set_state(tdlb_handle h, const float* in, int holds_moments);
+/* One transport-only step (identity collision): streaming and, for
+ * Esotwist, the parity flip, exactly as a step with f* = f. */
+int tdlb_debug_transport(tdlb_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TDLB_B200_H */

@@ -81,7 +81,7 @@ def load(kind: str) -> ctypes.CDLL:
         "initialise": (None, [vp, cd]), "collision": (None, [vp]), "bounce_back": (None, [vp]),
         "streaming_push": (None, [vp]), "moments": (None, [vp]),
         "forcing": (None, [vp, vp, cl, cd, cd]), "step": (None, [vp, vp, cl, cd, cd]),
-        "get_q": (None, [vp, vp]), "set_q": (None, [vp, vp]), "get_f": (None, [vp, vp]),
+        "get_q": (None, [vp, vp]), "set_q": (None, [vp, vp]), "get_moments": (None, [vp, vp]), "get_f": (None, [vp, vp]),
         "set_f": (None, [vp, vp]), "get_nu": (None, [vp, vp]), "set_nu_field": (None, [vp, vp]),
         "kat_simple_stream": (ci, [ci, cl, cl, cl, vp]),
         "kat_esotwist": (ci, [cl, cl, cl, ci, ci, ci, vp]),
@@ -89,6 +89,7 @@ def load(kind: str) -> ctypes.CDLL:
     }
     if kind == "port":
         sig["get_o"] = (None, [vp, vp])
+        sig["transport"] = (None, [vp])
         sig["set_threads"] = (None, [ci])
     else:
         sig["kat_simple_golden"] = (ci, [ci, vp])
@@ -181,6 +182,15 @@ class CpuLattice:
         a = np.ascontiguousarray(q, dtype=np.float64).reshape(self.shape + (18,))
         self._fn("set_q")(self.h, _ptr(a))
 
+    def get_moments(self) -> np.ndarray:
+        """Interior moments [x, y, z, 18] through the reference's read accessor."""
+        out = np.empty((self.x, self.y, self.z, 18), np.float64)
+        self._fn("get_moments")(self.h, _ptr(out))
+        return out
+
+    def interior(self, a: np.ndarray) -> np.ndarray:
+        return a[1:-1, 1:-1, 1:-1]
+
     def get_f(self) -> np.ndarray:
         out = np.empty(self.shape + (3,), np.float64)
         self._fn("get_f")(self.h, _ptr(out))
@@ -198,6 +208,10 @@ class CpuLattice:
     def set_nu_field(self, nu: np.ndarray):
         a = np.ascontiguousarray(nu, dtype=np.float64).reshape(self.shape)
         self._fn("set_nu_field")(self.h, _ptr(a))
+
+    def transport(self):
+        """Identity-collision step: Simple push, or Esotwist read+write+flip (port only)."""
+        self._fn("transport")(self.h)
 
     def get_o(self) -> np.ndarray:
         """Cells the last forcing() touched (port only; the reference resets O)."""

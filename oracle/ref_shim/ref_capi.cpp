@@ -139,6 +139,23 @@ void dumpQ(CU& cu, uint64_t* out) {
         for (int l = 0; l < QLen::D3Q19; l++) out[c * 18 + l] = cu.Q[c].q[l];
 }
 
+// Interior moments as the reference reads them (AccessField<...>::read, the
+// accessor collision() and forcing() use), out[((i*x..)...)*18 + l] over
+// interior cells in (i, j, k) order.
+template <typename T, Streaming S>
+void readMoments(Base<T>* b, double* out) {
+    using CU = ComputeUnitForcing<T, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, S>;
+    using AF = AccessField<T, QLen::D3Q19, MemoryLayoutIJKL, EgglesSomers, S>;
+    CU& cu = *static_cast<CU*>(b);
+    size_t c = 0;
+    for (tNi i = 1; i <= cu.xg1; i++)
+        for (tNi j = 1; j <= cu.yg1; j++)
+            for (tNi k = 1; k <= cu.zg1; k++, c++) {
+                QVec<T, QLen::D3Q19> q = AF::read(cu, i, j, k);
+                for (int l = 0; l < 18; l++) out[c * 18 + l] = (double)q.q[l];
+            }
+}
+
 }  // namespace
 
 extern "C" {
@@ -214,6 +231,15 @@ void tdlbref_get_nu(void* hv, double* out) {
 void tdlbref_set_nu_field(void* hv, const double* in) {
     Handle* h = (Handle*)hv;
     TDLBREF_DISPATCH(h, for (size_t c = 0; c < cu->size; c++) cu->Nu[c] = in[c]);
+}
+
+void tdlbref_get_moments(void* hv, double* out) {
+    Handle* h = (Handle*)hv;
+    if (h->precision == 4) {
+        if (h->streaming == 0) readMoments<float, Simple>(as<float>(h), out); else readMoments<float, Esotwist>(as<float>(h), out);
+    } else {
+        if (h->streaming == 0) readMoments<double, Simple>(as<double>(h), out); else readMoments<double, Esotwist>(as<double>(h), out);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -132,6 +132,62 @@ void tdlbo_get_o(void* h, uint8_t* out) {
     DISPATCH(h, memcpy(out, LAT32(h)->Olast, LAT32(h)->size), memcpy(out, LAT64(h)->Olast, LAT64(h)->size));
 }
 
+/* Interior moments through the reference's read accessor (plain Q for
+ * Simple, the esoteric read map for Esotwist), interior cells in (i, j, k)
+ * order, 18 per cell. */
+#define GET_MOMENTS(L, out)                                                        \
+    do {                                                                           \
+        size_t c_ = 0;                                                             \
+        for (long i = 1; i <= (L)->xg - 2; i++)                                    \
+            for (long j = 1; j <= (L)->yg - 2; j++)                                \
+                for (long k = 1; k <= (L)->zg - 2; k++, c_++) {                    \
+                    __typeof__((L)->Q[0]) q_[18];                                  \
+                    if ((L)->streaming == 0) {                                     \
+                        size_t e_ = ((size_t)i * (L)->yg + j) * (L)->zg + k;       \
+                        for (int l = 0; l < 18; l++) q_[l] = (L)->Q[e_ * 18 + l];  \
+                    } else {                                                       \
+                        GET_MOMENTS_ESO(L, i, j, k, q_);                           \
+                    }                                                              \
+                    for (int l = 0; l < 18; l++) (out)[c_ * 18 + l] = q_[l];       \
+                }                                                                  \
+    } while (0)
+
+void tdlbo_get_moments(void* h, double* out) {
+    if (((Handle*)h)->precision == 4) {
+        Lattice_f32* L = LAT32(h);
+#define GET_MOMENTS_ESO(L, i, j, k, q) eso_read_f32(L, (L)->Q, i, j, k, (L)->evenStep, q)
+        GET_MOMENTS(L, out);
+#undef GET_MOMENTS_ESO
+    } else {
+        Lattice_f64* L = LAT64(h);
+#define GET_MOMENTS_ESO(L, i, j, k, q) eso_read_f64(L, (L)->Q, i, j, k, (L)->evenStep, q)
+        GET_MOMENTS(L, out);
+#undef GET_MOMENTS_ESO
+    }
+}
+
+/* One transport-only step on the current Q: Simple push
+ * (StreamingSimple.hpp:257-307) or, for Esotwist, AccessField read + write
+ * for every interior cell followed by the parity flip (the step with an
+ * identity collision). */
+void tdlbo_transport(void* h) {
+#define TRANSPORT(L, SFX)                                                                  \
+    do {                                                                                   \
+        if ((L)->streaming == 0) { stream_simple_##SFX(L, 1); break; }                     \
+        for (long i = 1; i <= (L)->xg - 2; i++)                                            \
+            for (long j = 1; j <= (L)->yg - 2; j++)                                        \
+                for (long k = 1; k <= (L)->zg - 2; k++) {                                  \
+                    __typeof__((L)->Q[0]) q_[18];                                          \
+                    eso_read_##SFX(L, (L)->Q, i, j, k, (L)->evenStep, q_);                 \
+                    eso_write_##SFX(L, (L)->Q, i, j, k, (L)->evenStep, q_);                \
+                }                                                                          \
+        (L)->evenStep = !(L)->evenStep;                                                    \
+    } while (0)
+    if (((Handle*)h)->precision == 4) { Lattice_f32* L = LAT32(h); TRANSPORT(L, f32); }
+    else { Lattice_f64* L = LAT64(h); TRANSPORT(L, f64); }
+#undef TRANSPORT
+}
+
 /* ---- integer-coded transport KATs (values exact in double) ---- */
 
 static void fill_coded_f64(Lattice_f64* L) {

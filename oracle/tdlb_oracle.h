@@ -61,6 +61,8 @@ void tdlbo_set_f(void* h, const double* in);
 void tdlbo_get_nu(void* h, double* out);
 void tdlbo_set_nu_field(void* h, const double* in);
 void tdlbo_get_o(void* h, uint8_t* out);
+void tdlbo_get_moments(void* h, double* out);
+void tdlbo_transport(void* h);
 
 /* Integer-coded transport known-answer tests, same contract as the
  * tdlbref_kat_* entry points of oracle/_ref. Values are exact in uint64. */

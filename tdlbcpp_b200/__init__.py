@@ -1,0 +1,385 @@
+"""B200-native lattice Boltzmann time step with tdLBCpp's ComputeUnit interface.
+
+The compute path is the in-tree CUDA library ``libtdlb_b200.so`` (sm_100a),
+reached through its C ABI (``include/tdlb_b200.h``) with ctypes. This module
+is the host-side mirror of the reference's ``ComputeUnitBase`` virtuals
+(tdlbcpp/src/ComputeUnit.h:86-201) for Python callers; C++ callers use
+``include/tdlb_compute_unit_b200.hpp``.
+
+There is no CPU fallback: importing works anywhere, but creating a
+``ComputeUnit`` without the built library or without an sm_100 GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+from typing import Optional
+
+import numpy as np
+
+__all__ = [
+    "ComputeUnit", "TdlbError", "MARKER_DTYPE", "library_path", "load_library",
+    "STREAMING_SIMPLE", "STREAMING_ESOTWIST",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+_LIB_NAME = "libtdlb_b200.so"
+
+STREAMING_SIMPLE = 0
+STREAMING_ESOTWIST = 1
+
+# Lattice vectors of population slots Q01..Q18 (tdlbcpp/src/Header.h:70-100);
+# opposite(d) = d ^ 1.
+CX = (1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0)
+CY = (0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1)
+CZ = (0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1)
+
+# tdlb_marker (include/tdlb_b200.h): the PosPolar fields forcing() reads.
+MARKER_DTYPE = np.dtype(
+    [
+        ("i", np.int64), ("j", np.int64), ("k", np.int64),
+        ("iCartFraction", np.float32), ("kCartFraction", np.float32),
+        ("uDelta", np.float32), ("vDelta", np.float32), ("wDelta", np.float32),
+        ("pad", np.float32),
+    ]
+)
+assert MARKER_DTYPE.itemsize == 48
+
+_ERRORS = {
+    -1: "TDLB_EINVAL", -2: "TDLB_ECUDA", -3: "TDLB_ENOMEM", -4: "TDLB_EIO", -5: "TDLB_ESTATE", -6: "TDLB_EJSON",
+}
+
+
+class TdlbError(RuntimeError):
+    """A C-ABI call returned a non-zero status (the reference would have
+    called exit(1) or thrown std::runtime_error)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{_ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    """tdlb_config: the GridParams / FlowParams fields the step reads."""
+
+    _fields_ = [
+        ("x", ctypes.c_int64), ("y", ctypes.c_int64), ("z", ctypes.c_int64),
+        ("streaming", ctypes.c_int32), ("storage", ctypes.c_int32),
+        ("initialRho", ctypes.c_double), ("nu", ctypes.c_double), ("cs0", ctypes.c_double),
+        ("g3", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+        ("useLES", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    ]
+
+
+class Rushton(ctypes.Structure):
+    """tdlb_rushton: the project's Rushton-turbine tank spec (zero = default)."""
+
+    _fields_ = [
+        ("x", ctypes.c_int64), ("y", ctypes.c_int64), ("z", ctypes.c_int64),
+        ("tank_diameter", ctypes.c_double), ("impeller_diameter", ctypes.c_double),
+        ("clearance", ctypes.c_double), ("blade_height", ctypes.c_double), ("disk_thickness", ctypes.c_double),
+        ("n_blades", ctypes.c_int32), ("n_baffles", ctypes.c_int32),
+        ("baffle_width", ctypes.c_double), ("wall_inset", ctypes.c_double), ("tip_speed", ctypes.c_double),
+        ("startup_steps", ctypes.c_int64),
+    ]
+
+
+def library_path() -> str:
+    return os.path.join(HERE, _LIB_NAME)
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load_library() -> ctypes.CDLL:
+    """Load the in-tree CUDA library; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `make -C tdlbcpp_b200` (there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    H, vp, i32, f32, sz = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_size_t
+    sigs = {
+        "tdlb_create": (i32, [ctypes.c_char_p, i32, ctypes.POINTER(H)]),
+        "tdlb_create_config": (i32, [ctypes.POINTER(Config), i32, ctypes.POINTER(H)]),
+        "tdlb_destroy": (i32, [H]),
+        "tdlb_last_error": (ctypes.c_char_p, [H]),
+        "tdlb_initialise": (i32, [H, f32]),
+        "tdlb_forcing": (i32, [H, vp, sz, f32, f32]),
+        "tdlb_set_markers": (i32, [H, vp, sz]),
+        "tdlb_forcing_resident": (i32, [H, f32, f32]),
+        "tdlb_collision": (i32, [H]),
+        "tdlb_bounce_back": (i32, [H]),
+        "tdlb_streaming_push": (i32, [H]),
+        "tdlb_moments": (i32, [H]),
+        "tdlb_step": (i32, [H, f32, f32]),
+        "tdlb_read_moments": (i32, [H, vp]),
+        "tdlb_read_velocity_density": (i32, [H, vp, vp, vp, vp]),
+        "tdlb_read_force": (i32, [H, vp]),
+        "tdlb_read_nu": (i32, [H, vp]),
+        "tdlb_read_touched": (i32, [H, vp]),
+        "tdlb_get_dims": (i32, [H, vp, vp, vp]),
+        "tdlb_get_even_step": (i32, [H, vp]),
+        "tdlb_synchronize": (i32, [H]),
+        "tdlb_debug_get_state": (i32, [H, vp]),
+        "tdlb_debug_set_state": (i32, [H, vp, i32]),
+        "tdlb_debug_transport": (i32, [H]),
+        "tdlb_rushton_fixed": (i32, [ctypes.POINTER(Rushton), vp, sz, ctypes.POINTER(sz)]),
+        "tdlb_rushton_rotating_nonupdating": (i32, [ctypes.POINTER(Rushton), ctypes.c_double, vp, sz, ctypes.POINTER(sz)]),
+        "tdlb_rushton_rotating": (i32, [ctypes.POINTER(Rushton), ctypes.c_double, ctypes.c_double, vp, sz, ctypes.POINTER(sz)]),
+        "tdlb_rushton_impeller_increment": (ctypes.c_double, [ctypes.POINTER(Rushton), ctypes.c_uint64]),
+        "tdlb_rushton_blade_outer_radius": (i32, [ctypes.POINTER(Rushton)]),
+        "tdlb_schedule_levels": (i32, [vp, sz, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, vp, vp]),
+        "tdlb_attach_rushton": (i32, [H, ctypes.POINTER(Rushton), ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+        "tdlb_rotate_impeller": (i32, [H, ctypes.c_double, ctypes.c_double]),
+        "tdlb_read_markers": (i32, [H, vp, sz, ctypes.POINTER(sz)]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def as_markers(markers) -> np.ndarray:
+    m = np.ascontiguousarray(markers)
+    if m.dtype != MARKER_DTYPE:
+        out = np.zeros(len(m), MARKER_DTYPE)
+        for name in MARKER_DTYPE.names:
+            if name in (m.dtype.names or ()):
+                out[name] = m[name]
+        m = out
+    return m
+
+
+class ComputeUnit:
+    """One lattice on one GPU, driven like the reference's ComputeUnitBase.
+
+    Construct from the reference's input JSON (a path, a JSON string or a
+    dict) or from keyword fields of ``tdlb_config``. The reference call
+    sequence per step is kept: ``collision(); bounceBackBoundary();
+    streamingPush(); moments(); forcing(markers, alpha, beta)``.
+    """
+
+    def __init__(self, params=None, device: int = 0, **config):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        if params is not None:
+            if isinstance(params, dict):
+                text = json.dumps(params)
+            elif isinstance(params, str) and params.lstrip().startswith("{"):
+                text = params
+            else:
+                with open(params) as f:
+                    text = f.read()
+            rc = self.lib.tdlb_create(text.encode(), device, ctypes.byref(h))
+        else:
+            cfg = Config()
+            cfg.streaming = STREAMING_SIMPLE
+            cfg.initialRho, cfg.cs0, cfg.g3, cfg.alpha, cfg.beta, cfg.useLES = 1.0, 0.12, 0.8, 0.97, 1.9, 0
+            for key, val in config.items():
+                if key == "streaming" and isinstance(val, str):
+                    val = STREAMING_SIMPLE if val == "Simple" else STREAMING_ESOTWIST
+                setattr(cfg, key, val)
+            rc = self.lib.tdlb_create_config(ctypes.byref(cfg), device, ctypes.byref(h))
+        if rc != 0:
+            raise TdlbError(rc, self.lib.tdlb_last_error(None).decode())
+        self.h = h
+        x, y, z = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.tdlb_get_dims(self.h, ctypes.byref(x), ctypes.byref(y), ctypes.byref(z)))
+        self.x, self.y, self.z = x.value, y.value, z.value
+
+    # ---- lifecycle ----
+    def _check(self, rc: int):
+        if rc != 0:
+            raise TdlbError(rc, self.lib.tdlb_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tdlb_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ncell(self) -> int:
+        return self.x * self.y * self.z
+
+    # ---- ComputeUnitBase virtuals (ComputeUnit.h:110-200) ----
+    def initialise(self, rho: float):
+        self._check(self.lib.tdlb_initialise(self.h, rho))
+
+    def forcing(self, markers, alpha: float, beta: float):
+        m = as_markers(markers)
+        self._check(self.lib.tdlb_forcing(self.h, _p(m), len(m), alpha, beta))
+
+    def set_markers(self, markers):
+        m = as_markers(markers)
+        self._check(self.lib.tdlb_set_markers(self.h, _p(m), len(m)))
+
+    def forcing_resident(self, alpha: float, beta: float):
+        self._check(self.lib.tdlb_forcing_resident(self.h, alpha, beta))
+
+    def collision(self):
+        self._check(self.lib.tdlb_collision(self.h))
+
+    def bounceBackBoundary(self):
+        self._check(self.lib.tdlb_bounce_back(self.h))
+
+    def streamingPush(self):
+        self._check(self.lib.tdlb_streaming_push(self.h))
+
+    def moments(self):
+        self._check(self.lib.tdlb_moments(self.h))
+
+    def step(self, alpha: float, beta: float):
+        self._check(self.lib.tdlb_step(self.h, alpha, beta))
+
+    def synchronize(self):
+        self._check(self.lib.tdlb_synchronize(self.h))
+
+    @property
+    def evenStep(self) -> bool:
+        e = ctypes.c_int()
+        self._check(self.lib.tdlb_get_even_step(self.h, ctypes.byref(e)))
+        return bool(e.value)
+
+    # ---- resident impeller (device-side rotation) ----
+    def attach_rushton(self, turbine: "RushtonTurbine", nonupdating_delta: float, angle: float, delta: float):
+        self._check(self.lib.tdlb_attach_rushton(self.h, ctypes.byref(turbine.spec), nonupdating_delta, angle, delta))
+
+    def rotate_impeller(self, angle: float, delta: float):
+        self._check(self.lib.tdlb_rotate_impeller(self.h, angle, delta))
+
+    def read_markers(self) -> np.ndarray:
+        n = ctypes.c_size_t()
+        self._check(self.lib.tdlb_read_markers(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, MARKER_DTYPE)
+        self._check(self.lib.tdlb_read_markers(self.h, _p(out), n.value, ctypes.byref(n)))
+        return out
+
+    # ---- field read-back (interior cells, (i, j, k) order) ----
+    def read_moments(self) -> np.ndarray:
+        out = np.empty((self.x, self.y, self.z, 18), np.float32)
+        self._check(self.lib.tdlb_read_moments(self.h, _p(out)))
+        return out
+
+    def read_velocity_density(self):
+        shape = (self.x, self.y, self.z)
+        rho, ux, uy, uz = (np.empty(shape, np.float32) for _ in range(4))
+        self._check(self.lib.tdlb_read_velocity_density(self.h, _p(rho), _p(ux), _p(uy), _p(uz)))
+        return rho, np.stack([ux, uy, uz], axis=-1)
+
+    def read_force(self) -> np.ndarray:
+        out = np.empty((self.x, self.y, self.z, 3), np.float32)
+        self._check(self.lib.tdlb_read_force(self.h, _p(out)))
+        return out
+
+    def read_nu(self) -> np.ndarray:
+        out = np.empty((self.x, self.y, self.z), np.float32)
+        self._check(self.lib.tdlb_read_nu(self.h, _p(out)))
+        return out
+
+    def read_touched(self) -> np.ndarray:
+        out = np.empty((self.x, self.y, self.z), np.uint8)
+        self._check(self.lib.tdlb_read_touched(self.h, _p(out)))
+        return out
+
+    # ---- known-answer-test support ----
+    def debug_get_state(self) -> np.ndarray:
+        out = np.empty((self.x, self.y, self.z, 18), np.float32)
+        self._check(self.lib.tdlb_debug_get_state(self.h, _p(out)))
+        return out
+
+    def debug_set_state(self, q: np.ndarray, holds_moments: bool):
+        a = np.ascontiguousarray(q, dtype=np.float32).reshape(self.x, self.y, self.z, 18)
+        self._check(self.lib.tdlb_debug_set_state(self.h, _p(a), int(holds_moments)))
+
+    def debug_transport(self):
+        self._check(self.lib.tdlb_debug_transport(self.h))
+
+
+# ---------------------------------------------------------------------------
+# Rushton-turbine geometry (host only), mirroring the calls main.cpp makes on
+# RushtonTurbinePolarCPP (main.cpp:274-303, :409-426).
+# ---------------------------------------------------------------------------
+class RushtonTurbine:
+    """Marker lists of the project's stirred-tank geometry for an x*y*z lattice."""
+
+    def __init__(self, x: int, y: int, z: int, tip_speed: float = 0.1, startup_steps: int = 0, **spec):
+        self.lib = load_library()
+        self.spec = Rushton()
+        self.spec.x, self.spec.y, self.spec.z = x, y, z
+        self.spec.tip_speed = tip_speed
+        self.spec.startup_steps = startup_steps
+        for k, v in spec.items():
+            setattr(self.spec, k, v)
+
+    def _gen(self, fn, *args) -> np.ndarray:
+        n = ctypes.c_size_t()
+        rc = fn(ctypes.byref(self.spec), *args, None, 0, ctypes.byref(n))
+        if rc:
+            raise TdlbError(rc, "geometry query failed")
+        out = np.zeros(n.value, MARKER_DTYPE)
+        rc = fn(ctypes.byref(self.spec), *args, _p(out), n.value, ctypes.byref(n))
+        if rc:
+            raise TdlbError(rc, "geometry generation failed")
+        return out
+
+    def fixed(self) -> np.ndarray:
+        return self._gen(self.lib.tdlb_rushton_fixed)
+
+    def rotating_nonupdating(self, delta_angle: float) -> np.ndarray:
+        return self._gen(self.lib.tdlb_rushton_rotating_nonupdating, ctypes.c_double(delta_angle))
+
+    def rotating(self, angle: float, delta_angle: float) -> np.ndarray:
+        return self._gen(self.lib.tdlb_rushton_rotating, ctypes.c_double(angle), ctypes.c_double(delta_angle))
+
+    def increment(self, step: int) -> float:
+        return self.lib.tdlb_rushton_impeller_increment(ctypes.byref(self.spec), step)
+
+    def blade_outer_radius(self) -> int:
+        return self.lib.tdlb_rushton_blade_outer_radius(ctypes.byref(self.spec))
+
+    def forcing_list(self, angle: float, delta_angle: float, nonupdating_delta: float = None) -> np.ndarray:
+        """fixed + rotating-non-updating + rotating, the order main.cpp:301-303 builds."""
+        nd = delta_angle if nonupdating_delta is None else nonupdating_delta
+        return np.concatenate([self.fixed(), self.rotating_nonupdating(nd), self.rotating(angle, delta_angle)])
+
+
+def schedule_levels(markers, x: int, y: int, z: int):
+    """Per-plane immersed-boundary level of each marker and the most levels in a plane."""
+    lib = load_library()
+    m = as_markers(markers)
+    lev = np.zeros(len(m), np.int32)
+    mx = ctypes.c_int32()
+    rc = lib.tdlb_schedule_levels(_p(m), len(m), x, y, z, _p(lev), ctypes.byref(mx))
+    if rc:
+        raise TdlbError(rc, "schedule_levels failed")
+    return lev, mx.value
+
+
+def nu_from_reynolds(re: float, tip_speed: float, blade_outer_radius: int) -> float:
+    """FlowParams::calcNuAndRe_m (FlowParams.hpp:65-70), in the reference's float arithmetic."""
+    re_m = np.float32(np.float32(re) * np.pi / 2.0)
+    return float(np.float32(np.float32(tip_speed) * np.float32(blade_outer_radius) / re_m))

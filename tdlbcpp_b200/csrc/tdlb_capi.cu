@@ -1,0 +1,698 @@
+// Host runtime and C ABI (include/tdlb_b200.h) of the B200 lattice Boltzmann
+// time step: device memory, the marker scheduler, launch sequencing and
+// state bookkeeping. Kernels live in step_kernels.cu and ibm_kernels.cu.
+#include "tdlb_b200.h"
+#include "tdlb_kernels.cuh"
+#include "tdlb_runtime.hpp"
+#include "tdlb_geometry.hpp"
+
+#include <nlohmann/json.hpp>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using tdlb::Dims;
+using tdlb::Planes;
+
+namespace {
+
+thread_local std::string g_create_error = "no error";
+
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+#define TDLB_CK(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            throw Fail{TDLB_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)};        \
+    } while (0)
+
+long long round_up(long long a, long long m) { return (a + m - 1) / m * m; }
+
+}  // namespace
+
+struct tdlb_lattice {
+    tdlb_config cfg{};
+    Dims g{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    tdlb::CollideParams cp{};
+
+    float* bufA = nullptr;       // 18 planes
+    float* bufB = nullptr;       // 18 planes (Simple only)
+    float* Nu = nullptr;
+    float* F = nullptr;          // 3 planes: Fx, Fy, Fz
+    uint32_t* mask = nullptr;    // 2 x (rows * kw) words
+    long long mask_words = 0;
+
+    // state
+    int cur = 0;                 // Simple: which buffer holds the state (0 A, 1 B)
+    bool holds_moments = true;   // state is in moment form (after initialise)
+    bool even = true;            // Esotwist parity (ComputeUnit.hpp:116)
+    int pass = 0;                // forcing passes so far; mask[pass & 1] is current
+    bool initialised = false;
+
+    // markers
+    tdlb::Marker* d_markers = nullptr;
+    int* d_sched = nullptr;
+    int* d_level_ptr = nullptr;
+    int* d_plane_lv = nullptr;
+    float* d_scratch = nullptr;
+    long long marker_cap = 0;
+    long long level_cap = 0;
+    int n_markers = 0;
+    int n_levels = 0;
+    tdlb::MarkerSchedule sched;
+    // resident impeller: markers [rot_begin, rot_begin + n_rot) rotate
+    double* d_rot_xz = nullptr;
+    int rot_begin = -1;
+    int n_rot = 0;
+    double rot_ci = 0, rot_ck = 0;
+
+    std::string err = "no error";
+
+    Planes planes(float* base) const {
+        Planes p;
+        for (int d = 0; d < tdlb::NQ; d++) p.p[d] = base + (size_t)d * (size_t)g.plane;
+        return p;
+    }
+    float* state_buf() const { return cfg.streaming == TDLB_STREAMING_SIMPLE && cur == 1 ? bufB : bufA; }
+    float* other_buf() const { return cur == 1 ? bufA : bufB; }
+    uint32_t* mask_cur() const { return mask + (size_t)(pass & 1) * mask_words; }
+    uint32_t* mask_next() const { return mask + (size_t)((pass + 1) & 1) * mask_words; }
+    int state_mode() const {
+        if (cfg.streaming == TDLB_STREAMING_SIMPLE) return holds_moments ? 1 : 0;
+        return holds_moments ? 3 : 2;
+    }
+};
+
+namespace {
+
+void release(tdlb_lattice* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    cudaFree(h->bufA);
+    cudaFree(h->bufB);
+    cudaFree(h->Nu);
+    cudaFree(h->F);
+    cudaFree(h->mask);
+    cudaFree(h->d_markers);
+    cudaFree(h->d_sched);
+    cudaFree(h->d_level_ptr);
+    cudaFree(h->d_plane_lv);
+    cudaFree(h->d_scratch);
+    cudaFree(h->d_rot_xz);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+void validate_config(const tdlb_config& c) {
+    if (c.x < 1 || c.y < 1 || c.z < 1) throw Fail{TDLB_EINVAL, "grid extents must be >= 1"};
+    if (c.x > 32767 || c.y > 32767 || c.z > 32767) throw Fail{TDLB_EINVAL, "grid extent above 32767"};
+    if (c.streaming != TDLB_STREAMING_SIMPLE && c.streaming != TDLB_STREAMING_ESOTWIST)
+        throw Fail{TDLB_EINVAL, "streaming must be Simple (0) or Esotwist (1)"};
+    if (c.storage != TDLB_STORAGE_FP32) throw Fail{TDLB_EINVAL, "unsupported storage precision"};
+    if (!(c.nu >= 0.0) || !std::isfinite(c.nu)) throw Fail{TDLB_EINVAL, "nu must be finite and >= 0"};
+}
+
+tdlb_lattice* build(const tdlb_config& c, int device) {
+    validate_config(c);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        throw Fail{TDLB_ECUDA, "no CUDA device available (this library has no CPU path)"};
+    if (device < 0 || device >= ndev) throw Fail{TDLB_EINVAL, "device index out of range"};
+    cudaDeviceProp prop;
+    TDLB_CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) throw Fail{TDLB_ECUDA, "this library is built for sm_100a (B200); device is sm_" +
+                                                     std::to_string(prop.major) + std::to_string(prop.minor)};
+    auto* h = new tdlb_lattice();
+    try {
+        h->cfg = c;
+        h->device = device;
+        TDLB_CK(cudaSetDevice(device));
+        TDLB_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        Dims& g = h->g;
+        g.nx = (int)c.x; g.ny = (int)c.y; g.nz = (int)c.z;
+        g.kp = (int)round_up(c.z, 16);
+        g.kw = (g.kp + 31) / 32;
+        g.plane = round_up((long long)g.nx * g.ny * g.kp, 64);
+        h->mask_words = round_up((long long)g.nx * g.ny * g.kw, 64);
+        if (tdlb::ibm_smem_bytes(g) > 200 * 1024)
+            throw Fail{TDLB_EINVAL, "x * ceil(z/32) too large for the per-plane IBM flag tile"};
+        h->cp = tdlb::make_collide_params(c.nu, c.cs0, c.g3);
+
+        const size_t pop_bytes = (size_t)tdlb::NQ * g.plane * sizeof(float);
+        size_t free_b = 0, total_b = 0;
+        TDLB_CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t need = pop_bytes * (c.streaming == TDLB_STREAMING_SIMPLE ? 2 : 1) +
+                            (size_t)4 * g.plane * sizeof(float) + 2 * h->mask_words * sizeof(uint32_t);
+        if (need > free_b) throw Fail{TDLB_ENOMEM, "lattice needs " + std::to_string(need) + " B, " +
+                                                       std::to_string(free_b) + " B free on device"};
+        TDLB_CK(cudaMalloc(&h->bufA, pop_bytes));
+        if (c.streaming == TDLB_STREAMING_SIMPLE) TDLB_CK(cudaMalloc(&h->bufB, pop_bytes));
+        TDLB_CK(cudaMalloc(&h->Nu, (size_t)g.plane * sizeof(float)));
+        TDLB_CK(cudaMalloc(&h->F, (size_t)3 * g.plane * sizeof(float)));
+        TDLB_CK(cudaMalloc(&h->mask, (size_t)2 * h->mask_words * sizeof(uint32_t)));
+        TDLB_CK(cudaMemsetAsync(h->bufA, 0, pop_bytes, h->stream));
+        if (h->bufB) TDLB_CK(cudaMemsetAsync(h->bufB, 0, pop_bytes, h->stream));
+        TDLB_CK(cudaMemsetAsync(h->Nu, 0, (size_t)g.plane * sizeof(float), h->stream));
+        TDLB_CK(cudaMemsetAsync(h->F, 0, (size_t)3 * g.plane * sizeof(float), h->stream));
+        TDLB_CK(cudaMemsetAsync(h->mask, 0, (size_t)2 * h->mask_words * sizeof(uint32_t), h->stream));
+        TDLB_CK(cudaStreamSynchronize(h->stream));
+        const size_t smem = tdlb::ibm_smem_bytes(g);
+        if (smem > 48 * 1024) TDLB_CK(tdlb::ibm_prepare_smem(smem));
+    } catch (...) {
+        release(h);
+        delete h;
+        throw;
+    }
+    return h;
+}
+
+// Reference JSON -> tdlb_config (main.cpp:135-164 reads these sections).
+tdlb_config config_from_json(const char* text) {
+    nlohmann::json j;
+    try {
+        j = nlohmann::json::parse(text);
+    } catch (const std::exception& e) {
+        throw Fail{TDLB_EJSON, std::string("input JSON: ") + e.what()};
+    }
+    tdlb_config c{};
+    try {
+        const auto& grid = j.at("GridParams");
+        const auto& flow = j.at("FlowParams");
+        c.x = (int64_t)grid.at("x").get<uint64_t>();
+        c.y = (int64_t)grid.at("y").get<uint64_t>();
+        c.z = (int64_t)grid.at("z").get<uint64_t>();
+        const int64_t ghost = (int64_t)grid.value("multiStep", (uint64_t)1);
+        if (ghost != 1) throw Fail{TDLB_EINVAL, "GridParams.multiStep (ghost width) must be 1"};
+        c.initialRho = flow.at("initialRho").get<double>();
+        c.nu = flow.at("nu").get<double>();
+        c.cs0 = flow.at("cs0").get<double>();
+        c.g3 = flow.at("g3").get<double>();
+        c.alpha = flow.at("alpha").get<double>();
+        c.beta = flow.at("beta").get<double>();
+        c.useLES = flow.at("useLES").get<bool>() ? 1 : 0;
+        // main.cpp:242-256: "Simple" selects Simple, anything else Esotwist
+        c.streaming = flow.at("streaming").get<std::string>() == "Simple" ? TDLB_STREAMING_SIMPLE : TDLB_STREAMING_ESOTWIST;
+        if (c.nu == 0.0) {
+            // calcNuAndRe_m(impellerBladeOuterRadius) (FlowParams.hpp:65-70);
+            // the blade outer radius of the Rushton geometry, D/2 = T/6.
+            const float reM = (float)flow.at("reMNonDimensional").get<double>();
+            const float uav = (float)flow.at("uav").get<double>();
+            const float Re_m = (float)(reM * M_PI / 2.0);
+            const int radius = (int)(c.x / 6);
+            c.nu = (double)(float)(uav * (float)radius / Re_m);
+        }
+    } catch (const Fail&) {
+        throw;
+    } catch (const std::exception& e) {
+        throw Fail{TDLB_EJSON, std::string("input JSON: ") + e.what()};
+    }
+    c.storage = TDLB_STORAGE_FP32;
+    return c;
+}
+
+template <typename F>
+int guarded(tdlb_lattice* h, F&& fn) {
+    if (!h) return TDLB_EINVAL;
+    try {
+        cudaSetDevice(h->device);
+        fn();
+        return TDLB_OK;
+    } catch (const Fail& f) {
+        h->err = f.msg;
+        return f.code;
+    } catch (const std::bad_alloc&) {
+        h->err = "host allocation failed";
+        return TDLB_ENOMEM;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        return TDLB_EINVAL;
+    }
+}
+
+void require_init(tdlb_lattice* h) {
+    if (!h->initialised) throw Fail{TDLB_ESTATE, "call tdlb_initialise() first"};
+}
+
+tdlb::StepArgs step_args(tdlb_lattice* h, bool collide) {
+    tdlb::StepArgs a{};
+    a.A = h->planes(h->state_buf());
+    if (h->cfg.streaming == TDLB_STREAMING_SIMPLE) a.B = h->planes(h->other_buf());
+    a.Nu = h->Nu;
+    a.Fx = h->F;
+    a.Fy = h->F + h->g.plane;
+    a.Fz = h->F + 2 * h->g.plane;
+    a.mask = h->mask_cur();
+    a.g = h->g;
+    a.p = h->cp;
+    a.les = h->cfg.useLES;
+    a.from_moments = h->holds_moments ? 1 : 0;
+    a.collide = collide ? 1 : 0;
+    a.even = h->even ? 1 : 0;
+    return a;
+}
+
+void run_step(tdlb_lattice* h, bool collide) {
+    tdlb::StepArgs a = step_args(h, collide);
+    if (h->cfg.streaming == TDLB_STREAMING_SIMPLE) {
+        TDLB_CK(tdlb::launch_step_simple(a, h->stream));
+        h->cur ^= 1;
+    } else {
+        TDLB_CK(tdlb::launch_step_esotwist(a, h->stream));
+        h->even = !h->even;   // StreamingEsoteric.hpp:15-18
+    }
+    h->holds_moments = false;
+}
+
+void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, int rot_begin = -1,
+                    const double* rot_xz = nullptr) {
+    if (n > 0 && !m) throw Fail{TDLB_EINVAL, "markers is NULL"};
+    if (n > (size_t)0x7fffffff) throw Fail{TDLB_EINVAL, "too many markers"};
+    const Dims& g = h->g;
+    for (size_t q = 0; q < n; q++) {
+        if (m[q].i < 0 || m[q].i >= g.nx || m[q].j < 0 || m[q].j >= g.ny || m[q].k < 0 || m[q].k >= g.nz) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf, "marker %zu at (%lld,%lld,%lld) outside the %dx%dx%d interior", q,
+                          (long long)m[q].i, (long long)m[q].j, (long long)m[q].k, g.nx, g.ny, g.nz);
+            throw Fail{TDLB_EINVAL, buf};
+        }
+    }
+    static_assert(sizeof(tdlb_marker) == sizeof(tdlb::Marker), "marker layout");
+    h->sched.build(reinterpret_cast<const tdlb::Marker*>(m), (int)n, g.nx, g.ny, g.nz, rot_begin, rot_xz);
+    h->rot_begin = -1;   // a plain upload detaches the resident impeller
+    h->n_rot = 0;
+    const long long nl = (long long)h->sched.level_ptr.size();
+    if ((long long)n > h->marker_cap) {
+        cudaFree(h->d_markers); cudaFree(h->d_sched); cudaFree(h->d_scratch);
+        h->d_markers = nullptr; h->d_sched = nullptr; h->d_scratch = nullptr;
+        const long long cap = std::max<long long>(round_up((long long)n, 1024), 1024);
+        TDLB_CK(cudaMalloc(&h->d_markers, cap * sizeof(tdlb::Marker)));
+        TDLB_CK(cudaMalloc(&h->d_sched, cap * sizeof(int)));
+        TDLB_CK(cudaMalloc(&h->d_scratch, (size_t)tdlb::SF_COUNT * cap * sizeof(float)));
+        h->marker_cap = cap;
+    }
+    if (nl > h->level_cap || !h->d_plane_lv) {
+        cudaFree(h->d_level_ptr); cudaFree(h->d_plane_lv);
+        h->d_level_ptr = nullptr; h->d_plane_lv = nullptr;
+        const long long cap = std::max<long long>(round_up(nl, 1024), 1024);
+        TDLB_CK(cudaMalloc(&h->d_level_ptr, cap * sizeof(int)));
+        TDLB_CK(cudaMalloc(&h->d_plane_lv, (size_t)(g.ny + 1) * sizeof(int)));
+        h->level_cap = cap;
+    }
+    if (n) {
+        TDLB_CK(cudaMemcpyAsync(h->d_markers, m, n * sizeof(tdlb::Marker), cudaMemcpyHostToDevice, h->stream));
+        TDLB_CK(cudaMemcpyAsync(h->d_sched, h->sched.order.data(), n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    }
+    TDLB_CK(cudaMemcpyAsync(h->d_level_ptr, h->sched.level_ptr.data(), nl * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    TDLB_CK(cudaMemcpyAsync(h->d_plane_lv, h->sched.plane_lv.data(), (g.ny + 1) * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    // the host vectors are reused by the next upload: wait for the copies
+    TDLB_CK(cudaStreamSynchronize(h->stream));
+    h->n_markers = (int)n;
+    h->n_levels = (int)nl - 1;
+}
+
+void run_forcing(tdlb_lattice* h, float alpha, float beta) {
+    if (!h->d_plane_lv) throw Fail{TDLB_ESTATE, "no markers set (tdlb_set_markers / tdlb_forcing)"};
+    tdlb::IbmArgs a{};
+    a.markers = h->d_markers;
+    a.sched = h->d_sched;
+    a.level_ptr = h->d_level_ptr;
+    a.plane_lv = h->d_plane_lv;
+    a.n = h->n_markers;
+    a.scratch = h->d_scratch;
+    a.cap = h->marker_cap;
+    a.A = h->planes(h->state_buf());
+    a.state_mode = h->state_mode();
+    a.even = h->even ? 1 : 0;
+    a.Fx = h->F;
+    a.Fy = h->F + h->g.plane;
+    a.Fz = h->F + 2 * h->g.plane;
+    a.mask_old = h->mask_cur();
+    a.mask_new = h->mask_next();
+    a.g = h->g;
+    a.alpha = alpha;
+    a.beta = beta;
+    TDLB_CK(tdlb::launch_ibm(a, h->stream));
+    h->pass++;
+}
+
+// Copy an interior-cell plane set (npl planes of the device layout) to a
+// host AoS array out[cell*npl + l], cells in (i, j, k) order.
+void planes_to_host_aos(tdlb_lattice* h, const float* dev, int npl, float* out) {
+    const Dims& g = h->g;
+    std::vector<float> tmp((size_t)npl * g.plane);
+    TDLB_CK(cudaMemcpyAsync(tmp.data(), dev, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    TDLB_CK(cudaStreamSynchronize(h->stream));
+    size_t c = 0;
+    for (int i = 0; i < g.nx; i++)
+        for (int j = 0; j < g.ny; j++)
+            for (int k = 0; k < g.nz; k++, c++) {
+                const size_t e = ((size_t)i * g.ny + j) * g.kp + k;
+                for (int l = 0; l < npl; l++) out[c * npl + l] = tmp[(size_t)l * g.plane + e];
+            }
+}
+
+void host_aos_to_planes(tdlb_lattice* h, const float* in, int npl, float* dev) {
+    const Dims& g = h->g;
+    std::vector<float> tmp((size_t)npl * g.plane, 0.f);
+    size_t c = 0;
+    for (int i = 0; i < g.nx; i++)
+        for (int j = 0; j < g.ny; j++)
+            for (int k = 0; k < g.nz; k++, c++) {
+                const size_t e = ((size_t)i * g.ny + j) * g.kp + k;
+                for (int l = 0; l < npl; l++) tmp[(size_t)l * g.plane + e] = in[c * npl + l];
+            }
+    TDLB_CK(cudaMemcpyAsync(dev, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    TDLB_CK(cudaStreamSynchronize(h->stream));
+}
+
+// Moments of the current state into a temporary 18-plane device buffer.
+float* state_moments(tdlb_lattice* h) {
+    float* M = nullptr;
+    TDLB_CK(cudaMalloc(&M, (size_t)tdlb::NQ * h->g.plane * sizeof(float)));
+    cudaError_t e = tdlb::launch_state_moments(h->planes(h->state_buf()), h->planes(M), h->g, h->state_mode(),
+                                               h->even ? 1 : 0, h->stream);
+    if (e != cudaSuccess) {
+        cudaFree(M);
+        throw Fail{TDLB_ECUDA, std::string("state moments: ") + cudaGetErrorString(e)};
+    }
+    return M;
+}
+
+struct DevBuf {
+    float* p;
+    ~DevBuf() { cudaFree(p); }
+};
+
+}  // namespace
+
+extern "C" {
+
+int tdlb_create_config(const tdlb_config* cfg, int device, tdlb_handle* out) {
+    if (!cfg || !out) {
+        g_create_error = "NULL argument";
+        return TDLB_EINVAL;
+    }
+    *out = nullptr;
+    try {
+        *out = build(*cfg, device);
+        return TDLB_OK;
+    } catch (const Fail& f) {
+        g_create_error = f.msg;
+        return f.code;
+    } catch (const std::bad_alloc&) {
+        g_create_error = "host allocation failed";
+        return TDLB_ENOMEM;
+    }
+}
+
+int tdlb_create(const char* params_json, int device, tdlb_handle* out) {
+    if (!params_json || !out) {
+        g_create_error = "NULL argument";
+        return TDLB_EINVAL;
+    }
+    *out = nullptr;
+    try {
+        tdlb_config c = config_from_json(params_json);
+        *out = build(c, device);
+        return TDLB_OK;
+    } catch (const Fail& f) {
+        g_create_error = f.msg;
+        return f.code;
+    } catch (const std::bad_alloc&) {
+        g_create_error = "host allocation failed";
+        return TDLB_ENOMEM;
+    }
+}
+
+int tdlb_destroy(tdlb_handle h) {
+    if (!h) return TDLB_EINVAL;
+    release(h);
+    delete h;
+    return TDLB_OK;
+}
+
+const char* tdlb_last_error(tdlb_handle h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int tdlb_initialise(tdlb_handle h, float rho) {
+    return guarded(h, [&] {
+        const Dims& g = h->g;
+        h->cur = 0;
+        h->even = true;
+        h->holds_moments = true;
+        h->pass = 0;
+        TDLB_CK(tdlb::launch_fill_uniform_moments(h->planes(h->bufA), g, rho, h->stream));
+        TDLB_CK(cudaMemsetAsync(h->Nu, 0, (size_t)g.plane * sizeof(float), h->stream));
+        TDLB_CK(cudaMemsetAsync(h->F, 0, (size_t)3 * g.plane * sizeof(float), h->stream));
+        TDLB_CK(cudaMemsetAsync(h->mask, 0, (size_t)2 * h->mask_words * sizeof(uint32_t), h->stream));
+        h->initialised = true;
+    });
+}
+
+int tdlb_set_markers(tdlb_handle h, const tdlb_marker* markers, size_t n) {
+    return guarded(h, [&] { upload_markers(h, markers, n); });
+}
+
+int tdlb_forcing_resident(tdlb_handle h, float alpha, float beta) {
+    return guarded(h, [&] {
+        require_init(h);
+        run_forcing(h, alpha, beta);
+    });
+}
+
+int tdlb_forcing(tdlb_handle h, const tdlb_marker* markers, size_t n, float alpha, float beta) {
+    return guarded(h, [&] {
+        require_init(h);
+        upload_markers(h, markers, n);
+        run_forcing(h, alpha, beta);
+    });
+}
+
+int tdlb_collision(tdlb_handle h) {
+    return guarded(h, [&] {
+        require_init(h);
+        run_step(h, true);
+    });
+}
+
+int tdlb_bounce_back(tdlb_handle h) { return h ? TDLB_OK : TDLB_EINVAL; }
+int tdlb_streaming_push(tdlb_handle h) { return h ? TDLB_OK : TDLB_EINVAL; }
+int tdlb_moments(tdlb_handle h) { return h ? TDLB_OK : TDLB_EINVAL; }
+
+int tdlb_step(tdlb_handle h, float alpha, float beta) {
+    return guarded(h, [&] {
+        require_init(h);
+        run_step(h, true);
+        run_forcing(h, alpha, beta);
+    });
+}
+
+int tdlb_read_moments(tdlb_handle h, float* out) {
+    return guarded(h, [&] {
+        require_init(h);
+        if (!out) throw Fail{TDLB_EINVAL, "out is NULL"};
+        DevBuf M{state_moments(h)};
+        planes_to_host_aos(h, M.p, tdlb::NQ, out);
+    });
+}
+
+int tdlb_read_velocity_density(tdlb_handle h, float* rho, float* ux, float* uy, float* uz) {
+    return guarded(h, [&] {
+        require_init(h);
+        const Dims& g = h->g;
+        DevBuf M{state_moments(h)};
+        const size_t ncell = (size_t)g.nx * g.ny * g.nz;
+        std::vector<float> m(ncell * tdlb::NQ), f(ncell * 3);
+        planes_to_host_aos(h, M.p, tdlb::NQ, m.data());
+        planes_to_host_aos(h, h->F, 3, f.data());
+        std::vector<uint8_t> t(ncell);
+        std::vector<uint32_t> words((size_t)h->mask_words);
+        TDLB_CK(cudaMemcpy(words.data(), h->mask_cur(), words.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t c = 0; c < ncell; c++) {
+            const int k = (int)(c % g.nz);
+            const size_t row = c / g.nz;
+            const bool on = (words[row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
+            const float fx = on ? f[c * 3] : 0.f, fy = on ? f[c * 3 + 1] : 0.f, fz = on ? f[c * 3 + 2] : 0.f;
+            const float r = m[c * tdlb::NQ];
+            // QVec.hpp:385-394, in the reference's precision
+            if (rho) rho[c] = r;
+            if (ux) ux[c] = (float)((1.0 / r) * (m[c * tdlb::NQ + 1] + 0.5 * fx));
+            if (uy) uy[c] = (float)((1.0 / r) * (m[c * tdlb::NQ + 2] + 0.5 * fy));
+            if (uz) uz[c] = (float)((1.0 / r) * (m[c * tdlb::NQ + 3] + 0.5 * fz));
+        }
+    });
+}
+
+int tdlb_read_force(tdlb_handle h, float* f3) {
+    return guarded(h, [&] {
+        require_init(h);
+        if (!f3) throw Fail{TDLB_EINVAL, "out is NULL"};
+        const Dims& g = h->g;
+        planes_to_host_aos(h, h->F, 3, f3);
+        std::vector<uint32_t> words((size_t)h->mask_words);
+        TDLB_CK(cudaMemcpy(words.data(), h->mask_cur(), words.size() * 4, cudaMemcpyDeviceToHost));
+        const size_t ncell = (size_t)g.nx * g.ny * g.nz;
+        for (size_t c = 0; c < ncell; c++) {
+            const int k = (int)(c % g.nz);
+            const size_t row = c / g.nz;
+            if (!((words[row * g.kw + (k >> 5)] >> (k & 31)) & 1u)) f3[c * 3] = f3[c * 3 + 1] = f3[c * 3 + 2] = 0.f;
+        }
+    });
+}
+
+int tdlb_read_nu(tdlb_handle h, float* nu) {
+    return guarded(h, [&] {
+        require_init(h);
+        if (!nu) throw Fail{TDLB_EINVAL, "out is NULL"};
+        planes_to_host_aos(h, h->Nu, 1, nu);
+    });
+}
+
+int tdlb_read_touched(tdlb_handle h, uint8_t* flags) {
+    return guarded(h, [&] {
+        require_init(h);
+        if (!flags) throw Fail{TDLB_EINVAL, "out is NULL"};
+        const Dims& g = h->g;
+        std::vector<uint32_t> words((size_t)h->mask_words);
+        TDLB_CK(cudaMemcpyAsync(words.data(), h->mask_cur(), words.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        TDLB_CK(cudaStreamSynchronize(h->stream));
+        const size_t ncell = (size_t)g.nx * g.ny * g.nz;
+        for (size_t c = 0; c < ncell; c++) {
+            const int k = (int)(c % g.nz);
+            const size_t row = c / g.nz;
+            flags[c] = (uint8_t)((words[row * g.kw + (k >> 5)] >> (k & 31)) & 1u);
+        }
+    });
+}
+
+int tdlb_get_dims(tdlb_handle h, int64_t* x, int64_t* y, int64_t* z) {
+    return guarded(h, [&] {
+        if (x) *x = h->g.nx;
+        if (y) *y = h->g.ny;
+        if (z) *z = h->g.nz;
+    });
+}
+
+int tdlb_get_even_step(tdlb_handle h, int* even) {
+    return guarded(h, [&] {
+        if (!even) throw Fail{TDLB_EINVAL, "out is NULL"};
+        *even = h->even ? 1 : 0;
+    });
+}
+
+int tdlb_synchronize(tdlb_handle h) {
+    return guarded(h, [&] { TDLB_CK(cudaStreamSynchronize(h->stream)); });
+}
+
+int tdlb_attach_rushton(tdlb_handle h, const tdlb_rushton* spec, double nonupdating_delta_angle, double angle,
+                        double delta_angle) {
+    return guarded(h, [&] {
+        if (!spec) throw Fail{TDLB_EINVAL, "spec is NULL"};
+        if (spec->x != h->g.nx || spec->y != h->g.ny || spec->z != h->g.nz)
+            throw Fail{TDLB_EINVAL, "Rushton spec extents differ from the lattice"};
+        const tdlb::RushtonGeom G = tdlb::RushtonGeom::from(*spec);
+        std::vector<tdlb_marker> all = G.fixed();
+        const std::vector<tdlb_marker> nonupd = G.rotating_nonupdating(nonupdating_delta_angle);
+        all.insert(all.end(), nonupd.begin(), nonupd.end());
+        const int rot_begin = (int)all.size();
+        const std::vector<tdlb_marker> rot = G.rotating(angle, delta_angle);
+        all.insert(all.end(), rot.begin(), rot.end());
+        const std::vector<tdlb::RotatingPolar> pol = G.rotating_polar();
+        std::vector<double> xz(2 * pol.size());
+        double rmax = 0;
+        for (size_t q = 0; q < pol.size(); q++) {
+            xz[2 * q] = pol[q].x0;
+            xz[2 * q + 1] = pol[q].z0;
+            rmax = std::max(rmax, std::sqrt(pol[q].x0 * pol[q].x0 + pol[q].z0 * pol[q].z0));
+        }
+        if (G.ci - rmax < 2.0 || G.ci + rmax > h->g.nx - 3.0 || G.ck - rmax < 2.0 || G.ck + rmax > h->g.nz - 3.0)
+            throw Fail{TDLB_EINVAL, "impeller does not stay 2 cells inside the lattice"};
+        upload_markers(h, all.data(), all.size(), rot_begin, xz.data());
+        cudaFree(h->d_rot_xz);
+        h->d_rot_xz = nullptr;
+        if (!xz.empty()) {
+            TDLB_CK(cudaMalloc(&h->d_rot_xz, xz.size() * sizeof(double)));
+            TDLB_CK(cudaMemcpy(h->d_rot_xz, xz.data(), xz.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        h->rot_begin = rot_begin;
+        h->n_rot = (int)pol.size();
+        h->rot_ci = G.ci;
+        h->rot_ck = G.ck;
+    });
+}
+
+int tdlb_rotate_impeller(tdlb_handle h, double angle, double delta_angle) {
+    return guarded(h, [&] {
+        if (h->rot_begin < 0) throw Fail{TDLB_ESTATE, "no impeller attached (tdlb_attach_rushton)"};
+        TDLB_CK(tdlb::launch_rotate_markers(h->d_rot_xz, h->d_markers + h->rot_begin, h->n_rot, std::cos(angle),
+                                            std::sin(angle), delta_angle, h->rot_ci, h->rot_ck, h->g.nx, h->g.nz,
+                                            h->stream));
+    });
+}
+
+int tdlb_read_markers(tdlb_handle h, tdlb_marker* out, size_t cap, size_t* n) {
+    return guarded(h, [&] {
+        if (n) *n = (size_t)h->n_markers;
+        if (!out) return;
+        if (cap < (size_t)h->n_markers) throw Fail{TDLB_EINVAL, "cap smaller than the marker count"};
+        if (h->n_markers)
+            TDLB_CK(cudaMemcpyAsync(out, h->d_markers, (size_t)h->n_markers * sizeof(tdlb_marker), cudaMemcpyDeviceToHost,
+                                    h->stream));
+        TDLB_CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int tdlb_schedule_levels(const tdlb_marker* markers, size_t n, int64_t x, int64_t y, int64_t z, int32_t* level_out,
+                         int32_t* max_levels_per_plane) {
+    if ((n && !markers) || x < 1 || y < 1 || z < 1 || n > (size_t)0x7fffffff) return TDLB_EINVAL;
+    for (size_t q = 0; q < n; q++)
+        if (markers[q].i < 0 || markers[q].i >= x || markers[q].j < 0 || markers[q].j >= y || markers[q].k < 0 ||
+            markers[q].k >= z)
+            return TDLB_EINVAL;
+    tdlb::MarkerSchedule s;
+    s.build(reinterpret_cast<const tdlb::Marker*>(markers), (int)n, (int)x, (int)y, (int)z);
+    if (level_out) {
+        // level within its plane, from the plane's first level
+        for (int64_t j = 0; j < y; j++)
+            for (int lv = s.plane_lv[(size_t)j]; lv < s.plane_lv[(size_t)j + 1]; lv++)
+                for (int p = s.level_ptr[(size_t)lv]; p < s.level_ptr[(size_t)lv + 1]; p++)
+                    level_out[s.order[(size_t)p]] = lv - s.plane_lv[(size_t)j];
+    }
+    if (max_levels_per_plane) *max_levels_per_plane = s.max_levels_per_plane;
+    return TDLB_OK;
+}
+
+int tdlb_debug_get_state(tdlb_handle h, float* out) {
+    return guarded(h, [&] {
+        if (!out) throw Fail{TDLB_EINVAL, "out is NULL"};
+        planes_to_host_aos(h, h->state_buf(), tdlb::NQ, out);
+    });
+}
+
+int tdlb_debug_set_state(tdlb_handle h, const float* in, int holds_moments) {
+    return guarded(h, [&] {
+        if (!in) throw Fail{TDLB_EINVAL, "in is NULL"};
+        host_aos_to_planes(h, in, tdlb::NQ, h->state_buf());
+        h->holds_moments = holds_moments != 0;
+        h->initialised = true;
+    });
+}
+
+int tdlb_debug_transport(tdlb_handle h) {
+    return guarded(h, [&] {
+        require_init(h);
+        run_step(h, false);
+    });
+}
+
+}  // extern "C"

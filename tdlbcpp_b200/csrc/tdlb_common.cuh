@@ -1,0 +1,218 @@
+// Shared device definitions for the B200 lattice Boltzmann time step.
+//
+// Lattice: D3Q19-style with 18 moving populations and no rest population
+// (tdlbcpp/src/Header.h:35, :64-100). Population slot d has lattice vector
+// (CX[d], CY[d], CZ[d]); opposite(d) = d ^ 1.
+//
+// Device layout (one lattice = one "tank"):
+//   * interior cells only (the reference's ghost layer is never read by the
+//     step, so it is not stored);
+//   * cell (i, j, k), 0 <= i < nx, 0 <= j < ny, 0 <= k < nz, row r = i*ny + j,
+//     element e = r*kp + k, kp = row pitch = nz rounded up to 16 floats;
+//   * 18 population planes (SoA), each `plane` elements long and 256-byte
+//     aligned, addressed through an 18-pointer table;
+//   * F as three SoA planes (Fx, Fy, Fz), Nu as one plane, and the IBM "touched"
+//     flags as one bit per cell: word r*kw + k/32, bit k%32.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tdlb {
+
+constexpr int NQ = 18;
+
+// Lattice vectors in slot order Q01..Q18 (Header.h:70-100).
+__host__ __device__ constexpr int cx_of(int d) {
+    return d == 0 ? 1 : d == 1 ? -1 : d == 6 ? 1 : d == 7 ? -1 : d == 8 ? 1 : d == 9 ? -1
+         : d == 12 ? 1 : d == 13 ? -1 : d == 14 ? 1 : d == 15 ? -1 : 0;
+}
+__host__ __device__ constexpr int cy_of(int d) {
+    return d == 2 ? 1 : d == 3 ? -1 : d == 6 ? 1 : d == 7 ? -1 : d == 10 ? 1 : d == 11 ? -1
+         : d == 12 ? -1 : d == 13 ? 1 : d == 16 ? 1 : d == 17 ? -1 : 0;
+}
+__host__ __device__ constexpr int cz_of(int d) {
+    return d == 4 ? 1 : d == 5 ? -1 : d == 8 ? 1 : d == 9 ? -1 : d == 10 ? 1 : d == 11 ? -1
+         : d == 14 ? -1 : d == 15 ? 1 : d == 16 ? -1 : d == 17 ? 1 : 0;
+}
+
+struct Dims {
+    int nx, ny, nz;     // interior extent
+    int kp;             // row pitch in elements (multiple of 16)
+    int kw;             // bitmask words per row
+    long long plane;    // elements per population plane (multiple of 64)
+    __host__ __device__ long long rows() const { return (long long)nx * ny; }
+};
+
+// 18 plane base pointers of one population buffer.
+struct Planes {
+    float* p[NQ];
+};
+
+// Collision constants (FlowParams fields the step reads).
+struct CollideParams {
+    float nu;       // molecular viscosity
+    float b0, c0;   // 1/(1+6 nu), 1-6 nu  (CollisionEgglesSomers.hpp:31-32)
+    float cs0sq;    // Smagorinsky cs0^2
+    float g3;       // third-order relaxation
+};
+
+__host__ inline CollideParams make_collide_params(double nu, double cs0, double g3) {
+    CollideParams p;
+    p.nu = (float)nu;
+    p.b0 = (float)(1.0 / (1.0 + 6.0 * (double)(float)nu));
+    p.c0 = (float)(1.0 - 6.0 * (double)(float)nu);
+    p.cs0sq = (float)cs0 * (float)cs0;
+    p.g3 = (float)g3;
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// Moments of 18 populations (the linear map of CollisionEgglesSomers.hpp:
+// 186-256), factored through sums/differences of opposite pairs so that each
+// moment costs a few adds. m[0] = rho, m[1..3] = momentum, m[4..9] second
+// order (M05..M10), m[10..15] third order (M11..M16), m[16..17] fourth order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void moments_of(const float* q, float* m) {
+    const float s01 = q[0] + q[1], d01 = q[0] - q[1];
+    const float s03 = q[2] + q[3], d03 = q[2] - q[3];
+    const float s05 = q[4] + q[5], d05 = q[4] - q[5];
+    // xy edges: Q07 (+,+) Q08 (-,-) Q13 (+,-) Q14 (-,+)
+    const float xa = q[6] + q[7], xb = q[6] - q[7], xc = q[12] + q[13], xd = q[12] - q[13];
+    // xz edges: Q09 (+,+) Q10 (-,-) Q15 (+,-) Q16 (-,+)
+    const float ya = q[8] + q[9], yb = q[8] - q[9], yc = q[14] + q[15], yd = q[14] - q[15];
+    // yz edges: Q11 (+,+) Q12 (-,-) Q17 (+,-) Q18 (-,+)
+    const float za = q[10] + q[11], zb = q[10] - q[11], zc = q[16] + q[17], zd = q[16] - q[17];
+
+    const float exy = xa + xc, exz = ya + yc, eyz = za + zc;
+    const float px = xb + xd, py = xb - xd;        // xy-edge x and y momentum
+    const float qx = yb + yd, qz = yb - yd;        // xz-edge x and z momentum
+    const float ry = zb + zd, rz = zb - zd;        // yz-edge y and z momentum
+
+    m[0] = s01 + s03 + s05 + exy + exz + eyz;
+    m[1] = d01 + px + qx;
+    m[2] = d03 + py + ry;
+    m[3] = d05 + qz + rz;
+    m[4] = exy + exz - s03 - s05;
+    m[5] = xa - xc;
+    m[6] = exy + eyz - s01 - s05;
+    m[7] = ya - yc;
+    m[8] = za - zc;
+    m[9] = exz + eyz - s01 - s03;
+    m[10] = 2.f * px - d01 - qx;
+    m[11] = 2.f * py - d03 - ry;
+    m[12] = 3.f * (qx - d01);
+    m[13] = 3.f * (ry - d03);
+    m[14] = qz + rz - 2.f * d05;
+    m[15] = 3.f * (rz - qz);
+    m[16] = 0.5f * (s01 + s03 + exz + eyz) - s05 - exy;
+    m[17] = 1.5f * (s01 - s03 - exz + eyz);
+}
+
+// rho and momentum only (what the immersed boundary interpolates).
+__device__ __forceinline__ void moments4_of(const float* q, float* m) {
+    const float s01 = q[0] + q[1], d01 = q[0] - q[1];
+    const float s03 = q[2] + q[3], d03 = q[2] - q[3];
+    const float s05 = q[4] + q[5], d05 = q[4] - q[5];
+    const float xa = q[6] + q[7], xb = q[6] - q[7], xc = q[12] + q[13], xd = q[12] - q[13];
+    const float ya = q[8] + q[9], yb = q[8] - q[9], yc = q[14] + q[15], yd = q[14] - q[15];
+    const float za = q[10] + q[11], zb = q[10] - q[11], zc = q[16] + q[17], zd = q[16] - q[17];
+    m[0] = s01 + s03 + s05 + xa + xc + ya + yc + za + zc;
+    m[1] = d01 + (xb + xd) + (yb + yd);
+    m[2] = d03 + (xb - xd) + (zb + zd);
+    m[3] = d05 + (yb - yd) + (zb - zd);
+}
+
+// ---------------------------------------------------------------------------
+// Eggels-Somers collision with optional Smagorinsky LES
+// (CollisionEgglesSomers.hpp:27-176) for one cell, in FP32.
+//   m      : 18 pre-collision moments
+//   fx..fz : IBM force at the cell (zero where the cell was not touched)
+//   nu     : in = previous eddy viscosity, out = new one (LES only)
+//   out    : 18 post-collision populations
+// The inverse filter (:137-171) is applied through the even/odd structure of
+// each group of opposite directions. alpha[M17] = alpha[M18] = 0, so the
+// fourth-order columns drop out.
+// ---------------------------------------------------------------------------
+template <bool LES>
+__device__ __forceinline__ void collide(const float* m, float fx, float fy, float fz, float& nu,
+                                        const CollideParams& p, float* out) {
+    const float rho = m[0];
+    const float inv_rho = __frcp_rn(rho);
+    const float jx = fmaf(0.5f, fx, m[1]);
+    const float jy = fmaf(0.5f, fy, m[2]);
+    const float jz = fmaf(0.5f, fz, m[3]);
+    const float ux = inv_rho * jx, uy = inv_rho * jy, uz = inv_rho * jz;
+
+    float b = p.b0, c = p.c0;
+    if (LES) {
+        // fct = 3 / (rho (1 + 6 (Nu + nu)))       (:52)
+        const float fct = 3.f * __frcp_rn(rho * fmaf(6.f, nu + p.nu, 1.f));
+        // literal grouping of :55-65: m + 0.5*F*u - m
+        const float dudx = fct * (fmaf(0.5f * fx, ux, m[1]) - m[4]);
+        const float dvdy = fct * (fmaf(0.5f * fy, uy, m[2]) - m[6]);
+        const float dwdz = fct * (fmaf(0.5f * fz, uz, m[3]) - m[9]);
+        const float divv = dudx + dvdy + dwdz;
+        const float sxy = 2.f * fct * (fmaf(0.5f * fy, ux, m[2]) - m[5]);
+        const float sxz = 2.f * fct * (fmaf(0.5f * fz, ux, m[3]) - m[7]);
+        const float syz = 2.f * fct * (fmaf(0.5f * fz, uy, m[3]) - m[8]);
+        const float sh = 2.f * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + sxy * sxy + sxz * sxz + syz * syz
+                       - (2.f / 3.f) * divv * divv;
+        nu = p.cs0sq * sqrtf(fabsf(sh));            // (:74)
+        const float nut = nu + p.nu;
+        b = __frcp_rn(fmaf(6.f, nut, 1.f));
+        c = fmaf(-6.f, nut, 1.f);
+    }
+
+    constexpr float r24 = 1.f / 24.f;
+    const float a0 = rho * r24;
+    const float a1 = (m[1] + fx) * r24;
+    const float a2 = (m[2] + fy) * r24;
+    const float a3 = (m[3] + fz) * r24;
+    const float br = b * r24;
+    const float a4 = (2.f * jx * ux - m[4] * c) * br;
+    const float a5 = (2.f * jx * uy - m[5] * c) * br;
+    const float a6 = (2.f * jy * uy - m[6] * c) * br;
+    const float a7 = (2.f * jx * uz - m[7] * c) * br;
+    const float a8 = (2.f * jy * uz - m[8] * c) * br;
+    const float a9 = (2.f * jz * uz - m[9] * c) * br;
+    const float g = -p.g3 * r24;
+    const float a10 = g * m[10], a11 = g * m[11], a12 = g * m[12];
+    const float a13 = g * m[13], a14 = g * m[14], a15 = g * m[15];
+
+    // faces
+    const float e01 = 2.f * a0 + 3.f * (a4 - a6 - a9);
+    const float o01 = 4.f * a1 - 2.f * (a10 + a12);
+    out[0] = e01 + o01;
+    out[1] = e01 - o01;
+    const float e03 = 2.f * a0 + 3.f * (a6 - a4 - a9);
+    const float o03 = 4.f * a2 - 2.f * (a11 + a13);
+    out[2] = e03 + o03;
+    out[3] = e03 - o03;
+    const float e05 = 2.f * a0 + 3.f * (a9 - a4 - a6);
+    const float o05 = 4.f * (a3 - a14);
+    out[4] = e05 + o05;
+    out[5] = e05 - o05;
+    // xy edges: Q07 (+x+y) Q14 (-x+y) Q08 (-x-y) Q13 (+x-y)
+    const float exy = a0 + 1.5f * (a4 + a6 - a9);
+    const float X = 2.f * (a1 + a10), Y = 2.f * (a2 + a11), Z = 6.f * a5;
+    out[6] = exy + X + Y + Z;
+    out[13] = exy - X + Y - Z;
+    out[7] = exy - X - Y + Z;
+    out[12] = exy + X - Y - Z;
+    // xz edges: Q09 (+x+z) Q16 (-x+z) Q10 (-x-z) Q15 (+x-z)
+    const float exz = a0 + 1.5f * (a4 - a6 + a9);
+    const float Xp = 2.f * a1 - a10 + a12, Zp = 2.f * a3 + a14 - a15, W = 6.f * a7;
+    out[8] = exz + Xp + Zp + W;
+    out[15] = exz - Xp + Zp - W;
+    out[9] = exz - Xp - Zp + W;
+    out[14] = exz + Xp - Zp - W;
+    // yz edges: Q11 (+y+z) Q18 (-y+z) Q12 (-y-z) Q17 (+y-z)
+    const float eyz = a0 + 1.5f * (a6 - a4 + a9);
+    const float Yp = 2.f * a2 - a11 + a13, Zq = 2.f * a3 + a14 + a15, Wp = 6.f * a8;
+    out[10] = eyz + Yp + Zq + Wp;
+    out[17] = eyz - Yp + Zq - Wp;
+    out[11] = eyz - Yp - Zq + Wp;
+    out[16] = eyz + Yp - Zq - Wp;
+}
+
+}  // namespace tdlb
