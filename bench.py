@@ -1,0 +1,404 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the B200 lattice Boltzmann time step.
+
+Workload (default): the stirred tank at scale -- a 400^3 FP32 lattice,
+Rushton turbine (T = 400, D = T/3, 6 blades, 4 baffles), Eggels-Somers
+collision with Smagorinsky LES (Cs = 0.1), tip speed 0.1, Re = 20000,
+Simple (A/B) streaming, rotating impeller. `--workload esotwist` runs the
+same tank with single-buffer esoteric-twist streaming.
+
+One "step" = the reference's main-loop step (main.cpp:409-454): impeller
+update, collision + streaming + moments (one fused kernel), immersed-boundary
+forcing. Metric: MLUPS = interior cells x steps / s.
+
+  value   device-resident steps (markers rotated on the device), CUDA events
+          on the library's stream, barrier + synchronize on both sides, max
+          over ranks; the 9.6 GB lattice is far larger than L2, so no flush.
+  e2e     the public C-ABI driven the way main.cpp drives the reference: per
+          step the host generates the blade markers at the new angle, copies
+          them from pinned memory (H2D), runs collision + forcing, and reads
+          back the FP64 impeller load (D2H); wall-clock, synchronized.
+  roofline  the fused step kernel: 152 algorithmic bytes per cell (18
+          populations read + written, Nu read + written) / its average
+          CUDA-event duration, against the measured copy bandwidth.
+  cpu_baseline  the reference's own CPU ComputeUnit (compiled in place into
+          oracle/_ref) on a bounded sample of the same workload.
+
+`--impl reference` times the reference's CPU implementation instead: every
+host thread advances its own reference ComputeUnit on a 400 x 16 x 400 slab
+through the impeller plane of the same tank, one step per "step".
+
+Multi-GPU: `torchrun --nproc-per-node N bench.py --gpus N` runs one replica
+per GPU (independent tanks, no collective: weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+EDGE = 400
+RE = 20000.0
+TIP = 0.1
+ALPHA, BETA = 0.97, 1.9
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "traffic_per_cell.txt")
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(workload: str):
+    """DRAM bytes per cell of the fused kernel from the committed ncu summary."""
+    if not os.path.exists(PROFILE_TRAFFIC):
+        return None
+    with open(PROFILE_TRAFFIC) as f:
+        for line in f:
+            if line.startswith(workload + ":"):
+                return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = []
+        for r in csv.reader(io.StringIO(self.out or "")):
+            if len(r) < 9:
+                continue
+            try:
+                rows.append([x.strip() for x in r])
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[c - 5] for r in rows for c in range(5, 9) if r[c].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- our arm
+
+def make_unit(tb, workload: str, edge: int, device: int):
+    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=TIP, startup_steps=0)
+    nu = tb.nu_from_reynolds(RE, TIP, rt.blade_outer_radius())
+    streaming = tb.STREAMING_ESOTWIST if workload == "esotwist" else tb.STREAMING_SIMPLE
+    cu = tb.ComputeUnit(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0,
+                        streaming=streaming, device=device)
+    return cu, rt, nu
+
+
+def run_ours(args, rank, world, device):
+    import torch
+    import tdlbcpp_b200 as tb
+
+    torch.cuda.set_device(device)
+    edge = args.edge
+    cu, rt, nu = make_unit(tb, args.workload, edge, device)
+    stream = torch.cuda.ExternalStream(cu.stream, device=device)
+    dth = rt.increment(1)
+    cu.attach_rushton(rt, dth, 0.0, dth)
+    cu.initialise(1.0)
+    cu.forcing_resident(ALPHA, BETA)          # main.cpp:305
+    n_markers = len(cu.read_markers())
+    n_rot = len(rt.rotating(0.0, dth))
+    cells = edge ** 3
+    angle = 0.0
+
+    def device_step(ev0=None, ev1=None):
+        nonlocal angle
+        angle += dth
+        cu.rotate_impeller(angle, dth)
+        if ev0 is not None:
+            ev0.record(stream)
+        cu.collision()
+        if ev1 is not None:
+            ev1.record(stream)
+        cu.forcing_resident(ALPHA, BETA)
+
+    for _ in range(args.warmup):
+        device_step()
+    cu.synchronize()
+
+    # ---- value: device-resident steps
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    cu.synchronize()
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clk:
+        t0.record(stream)
+        for s in range(args.steps):
+            device_step(*kev[s])
+        t1.record(stream)
+        cu.synchronize()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    kernel_ms = sum(a.elapsed_time(b) for a, b in kev) / args.steps
+    ms = max_over_ranks(ms, world)
+    kernel_ms_max = max_over_ranks(kernel_ms, world)
+
+    # ---- e2e: host-driven steps through the C ABI
+    pinned = torch.empty(n_rot * tb.MARKER_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+    host_rot = np.frombuffer(pinned.numpy(), dtype=tb.MARKER_DTYPE)
+    load = torch.empty(5 * 8, dtype=torch.uint8, pin_memory=True)
+    load_np = np.frombuffer(load.numpy(), dtype=np.float64)
+    spec = rt.spec
+    k_e2e = max(3, args.steps // 5)
+
+    def e2e_step():
+        nonlocal angle
+        angle += dth
+        n = tb.ctypes.c_size_t()
+        rc = cu.lib.tdlb_rushton_rotating(tb.ctypes.byref(spec), angle, dth, tb._p(host_rot), n_rot, tb.ctypes.byref(n))
+        assert rc == 0 and n.value == n_rot
+        cu.set_rotating_markers(host_rot)
+        cu.collision()
+        cu.forcing_resident(ALPHA, BETA)
+        cu.impeller_load(load_np)
+
+    e2e_step()
+    barrier(world)
+    cu.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(k_e2e):
+        e2e_step()
+    cu.synchronize()
+    w1 = time.perf_counter()
+    barrier(world)
+    e2e_s = max_over_ranks(w1 - w0, world)
+    cu.close()
+
+    result = {
+        "value_mlups": world * cells * args.steps / (ms / 1e3) / 1e6,
+        "ms_per_step": ms / args.steps,
+        "kernel_ms": kernel_ms_max,
+        "e2e_mlups": world * cells * k_e2e / e2e_s / 1e6,
+        "e2e_steps": k_e2e,
+        "h2d": n_rot * tb.MARKER_DTYPE.itemsize,
+        "d2h": 5 * 8,
+        "clocks": clk.summary(),
+        "n_markers": n_markers,
+        "n_rot": n_rot,
+        "nu": nu,
+        "load": load_np.tolist(),
+    }
+    return result
+
+
+# ---------------------------------------------------------------- reference arm
+
+def slab_markers(tb, rt, j0, height, angle, dth):
+    m = rt.forcing_list(angle, dth, nonupdating_delta=dth)
+    m = m[(m["j"] >= j0) & (m["j"] < j0 + height)].copy()
+    m["j"] -= j0
+    return m
+
+
+def reference_sample(steps, warmup, threads, edge=EDGE, height=16):
+    """Every thread advances its own reference ComputeUnit (FP32, Simple,
+    LES) on an edge x height x edge slab through the impeller plane."""
+    import tdlbcpp_b200 as tb
+    from oracle import pyoracle as po
+
+    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=TIP, startup_steps=0)
+    nu = tb.nu_from_reynolds(RE, TIP, rt.blade_outer_radius())
+    dth = rt.increment(1)
+    j0 = int(round(edge / 3.0)) - height // 2
+    flow = po.Flow(initialRho=1.0, nu=nu, cs0=0.1, g3=0.8, alpha=ALPHA, beta=BETA, useLES=True)
+    lats = [po.CpuLattice("ref", edge, height, edge, flow, "Simple", 4, tmpdir="/tmp") for _ in range(threads)]
+    mk = slab_markers(tb, rt, j0, height, 0.0, dth)
+    for L in lats:
+        L.initialise(1.0)
+        L.forcing(mk, ALPHA, BETA)
+    angle = 0.0
+    times = []
+    for s in range(warmup + steps):
+        angle += dth
+        mk = slab_markers(tb, rt, j0, height, angle, dth)
+        ths = [threading.Thread(target=L.step, args=(mk, ALPHA, BETA)) for L in lats]
+        t = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        if s >= warmup:
+            times.append(time.perf_counter() - t)
+    for L in lats:
+        L.close()
+    cells = threads * edge * height * edge
+    total = sum(times)
+    return {"value": cells * len(times) / total / 1e6, "cores": threads, "seconds": total,
+            "sample": f"{threads} x reference ComputeUnit<float,...,Simple,CPU> on a {edge}x{height}x{edge} slab "
+                      f"through the impeller plane, {len(times)} step(s) each"}
+
+
+def host_threads(edge=EDGE, height=16):
+    """Threads for the reference sample: every host core, bounded by the RAM
+    one reference slab takes (~100 B per cell with ghosts) and capped at 64."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+        per = (edge + 2) * (height + 2) * (edge + 2) * 110
+        n = min(n, max(1, int(avail * 0.5 // per)))
+    except (ValueError, OSError):
+        pass
+    return max(1, min(n, 64))
+
+
+# ---------------------------------------------------------------- plumbing
+
+_PG = None
+
+
+def init_dist(args):
+    global _PG
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        _PG = dist
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1 and _PG is not None:
+        _PG.barrier()
+
+
+def max_over_ranks(x, world):
+    if world > 1 and _PG is not None:
+        import torch
+        t = torch.tensor([float(x)], device="cuda")
+        _PG.all_reduce(t, op=_PG.ReduceOp.MAX)
+        return float(t.item())
+    return float(x)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["simple", "esotwist"], default="simple")
+    ap.add_argument("--edge", type=int, default=EDGE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3   # timing rule: at least 3 warm-up steps
+    workload = f"rushton-{args.edge}^3-{args.workload}-fp32-les"
+    config = {"workload": workload, "grid": [args.edge] * 3, "streaming": args.workload.capitalize(),
+              "collision": "EgglesSomers+LES(cs0=0.1)", "re": RE, "tip_speed": TIP, "ibm": "Rushton turbine, rotating",
+              "l2": "lattice > L2 every step (no flush needed)"}
+
+    rank, world, local = init_dist(args)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        nthr = host_threads()
+        steps = max(1, args.steps // 25)
+        r = reference_sample(steps, min(args.warmup, 1), nthr)
+        line = {"metric": "MLUPS", "value": r["value"], "unit": "MLUPS", "n_gpus": args.gpus, "steps": steps,
+                "warmup": min(args.warmup, 1), "ms_per_step": r["seconds"] / steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": config,
+                "impl": "reference",
+                "cpu_baseline": {"value": r["value"], "unit": "MLUPS", "cores": r["cores"], "kind": "reference",
+                                 "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    res = run_ours(args, rank, world, local)
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peak()
+    cells = args.edge ** 3
+    bpc = 152
+    achieved = bpc * cells / (res["kernel_ms"] / 1e3) / 1e9
+    traffic_pc = profile_traffic(workload)
+    line = {
+        "metric": "MLUPS", "value": res["value_mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": config,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "kernel": "k_step_simple" if args.workload == "simple" else "k_step_esotwist",
+                     "bytes_per_cell": bpc, "kernel_ms": res["kernel_ms"],
+                     "traffic": None if traffic_pc is None else traffic_pc * cells},
+        "e2e": {"value": res["e2e_mlups"], "unit": "MLUPS", "h2d_bytes_per_step": res["h2d"],
+                "d2h_bytes_per_step": res["d2h"], "steps": res["e2e_steps"]},
+        "gpu_launches": 4 * args.steps,
+        "clocks": res["clocks"],
+        "markers": res["n_markers"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        r = reference_sample(1, 0, host_threads())
+        line["cpu_baseline"] = {"value": r["value"], "unit": "MLUPS", "cores": r["cores"], "kind": "reference",
+                                "sample": r["sample"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

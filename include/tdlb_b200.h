@@ -154,6 +154,14 @@ int tdlb_get_even_step(tdlb_handle h, int* even);
 /* Make all queued device work complete. */
 int tdlb_synchronize(tdlb_handle h);
 
+/* Step-kernel variant: cells per thread (1, 2 or 4; default 4 = float4
+ * traffic). All variants compute identical results. */
+int tdlb_set_cells_per_thread(tdlb_handle h, int v);
+
+/* The cudaStream_t (as void*) all of h's device work is queued on, for
+ * callers that time it with CUDA events or order their own work after it. */
+int tdlb_get_stream(tdlb_handle h, void** stream);
+
 /* ---- Rushton-turbine geometry (host only; no GPU needed) ----
  * Replaces the un-vendored tdLBGeometryRushtonTurbineLib calls of main.cpp
  * (RushtonTurbinePolarCPP::generateFixedGeometry, :289-290;
@@ -198,6 +206,19 @@ int tdlb_rushton_blade_outer_radius(const tdlb_rushton* spec);
 int tdlb_attach_rushton(tdlb_handle h, const tdlb_rushton* spec, double nonupdating_delta_angle, double angle,
                         double delta_angle);
 int tdlb_rotate_impeller(tdlb_handle h, double angle, double delta_angle);
+
+/* Host-driven alternative to tdlb_rotate_impeller(), the way main.cpp does
+ * it (:424-426): replace the attached blades with n host-generated markers
+ * (same count and order as attached; e.g. tdlb_rushton_rotating at the new
+ * angle). Only the blades are copied and rescheduled. */
+int tdlb_set_rotating_markers(tdlb_handle h, const tdlb_marker* markers, size_t n);
+
+/* FP64 load on the attached impeller (rotating-non-updating + rotating
+ * markers) from the last forcing pass: out[0..2] = force the markers apply
+ * to the fluid, -beta * sum of each marker's (interpolated - target)
+ * momentum; out[3] = its torque about the tank axis (j); out[4] = markers
+ * summed. A project-defined diagnostic: the reference computes none. */
+int tdlb_impeller_load(tdlb_handle h, double* out5);
 
 /* Copy of the resident marker list as the device holds it (list order). */
 int tdlb_read_markers(tdlb_handle h, tdlb_marker* out, size_t cap, size_t* n);

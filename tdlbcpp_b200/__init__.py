@@ -138,6 +138,10 @@ def load_library() -> ctypes.CDLL:
         "tdlb_attach_rushton": (i32, [H, ctypes.POINTER(Rushton), ctypes.c_double, ctypes.c_double, ctypes.c_double]),
         "tdlb_rotate_impeller": (i32, [H, ctypes.c_double, ctypes.c_double]),
         "tdlb_read_markers": (i32, [H, vp, sz, ctypes.POINTER(sz)]),
+        "tdlb_set_rotating_markers": (i32, [H, vp, sz]),
+        "tdlb_impeller_load": (i32, [H, vp]),
+        "tdlb_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
+        "tdlb_set_cells_per_thread": (i32, [H, i32]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -270,6 +274,27 @@ class ComputeUnit:
 
     def rotate_impeller(self, angle: float, delta: float):
         self._check(self.lib.tdlb_rotate_impeller(self.h, angle, delta))
+
+    def set_rotating_markers(self, markers):
+        m = as_markers(markers)
+        self._check(self.lib.tdlb_set_rotating_markers(self.h, _p(m), len(m)))
+
+    def impeller_load(self, out: np.ndarray = None) -> np.ndarray:
+        """FP64 (Fx, Fy, Fz, torque_j, n_markers) on the attached impeller."""
+        if out is None:
+            out = np.zeros(5, np.float64)
+        self._check(self.lib.tdlb_impeller_load(self.h, _p(out)))
+        return out
+
+    def set_cells_per_thread(self, v: int):
+        """Step-kernel variant (1, 2 or 4 cells per thread); results are identical."""
+        self._check(self.lib.tdlb_set_cells_per_thread(self.h, v))
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.tdlb_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
 
     def read_markers(self) -> np.ndarray:
         n = ctypes.c_size_t()

@@ -85,13 +85,57 @@ __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int eve
     }
 }
 
-__global__ void __launch_bounds__(128) k_ibm_gather(IbmArgs a) {
+// ---------------------------------------------------------------------------
+// First segment (markers that do not move), prepared once per upload.
+// ---------------------------------------------------------------------------
+__global__ void k_ibm_prepare(IbmArgs a, float* __restrict__ prep) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n) return;
+    if (p >= a.n0) return;
     const Marker mk = a.markers[a.sched[p]];
+    const long long n0 = a.n0;
+    int c = 0;
+    for (int k1 = -1; k1 <= 1; k1++)
+        for (int i1 = -1; i1 <= 1; i1++, c++)
+            prep[(PF_W + c) * n0 + p] =
+                calc_weight(-mk.iCartFraction + (float)i1) * calc_weight(-mk.kCartFraction + (float)k1);
+    prep[PF_U * n0 + p] = mk.uDelta;
+    prep[PF_V * n0 + p] = mk.vDelta;
+    prep[PF_WV * n0 + p] = mk.wDelta;
+}
+
+// Per pass: rho and momentum of every unique stencil cell of the first
+// segment (cells sorted by row, so neighbouring threads pull neighbouring
+// cells), and the F each cell starts the pass with (zero unless the previous
+// pass touched it, Forcing.hpp:162-174).
+__global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.ncell) return;
+    const Dims& g = a.g;
+    const int e = a.cell_e[c];
+    const int row = e / g.kp;
+    const int k = e - row * g.kp;
+    const int i = row / g.ny;
+    const int j = row - i * g.ny;
+    float m4[4];
+    cell_moments4(a.A, a.state_mode, a.even, g, i, j, k, m4);
+    const long long C = a.ncell;
+#pragma unroll
+    for (int s = 0; s < 4; s++) a.cell_m[s * C + c] = m4[s];
+    const bool live = (a.mask_old[(long long)row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
+    a.cell_F[c] = live ? a.Fx[e] : 0.f;
+    a.cell_F[C + c] = live ? a.Fy[e] : 0.f;
+    a.cell_F[2 * C + c] = live ? a.Fz[e] : 0.f;
+}
+
+// Second segment (the blades): weights and the moments of the 9 stencil
+// cells of every blade marker.
+__global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n - a.n0) return;
+    const Marker mk = a.markers[a.sched[a.n0 + t]];
     const int i = (int)mk.i, j = (int)mk.j, k = (int)mk.k;
-    float* s = a.scratch;
-    const long long cap = a.cap;
+    float* s = a.tail;
+    const long long cap = a.tail_cap;
     int c = 0;
     for (int k1 = -1; k1 <= 1; k1++) {
         for (int i1 = -1; i1 <= 1; i1++, c++) {
@@ -99,33 +143,102 @@ __global__ void __launch_bounds__(128) k_ibm_gather(IbmArgs a) {
             const int i2 = wrap_i(i + i1, a.g.nx), k2 = wrap_i(k + k1, a.g.nz);
             float m4[4];
             cell_moments4(a.A, a.state_mode, a.even, a.g, i2, j, k2, m4);
-            s[(SF_W + c) * cap + p] = w;
-            s[(SF_RHO + c) * cap + p] = m4[0];
-            s[(SF_MX + c) * cap + p] = m4[1];
-            s[(SF_MY + c) * cap + p] = m4[2];
-            s[(SF_MZ + c) * cap + p] = m4[3];
-            s[(SF_CELL + c) * cap + p] = __int_as_float((i2 << 16) | k2);
+            s[(TF_W + c) * cap + t] = w;
+            s[(TF_RHO + c) * cap + t] = m4[0];
+            s[(TF_MX + c) * cap + t] = m4[1];
+            s[(TF_MY + c) * cap + t] = m4[2];
+            s[(TF_MZ + c) * cap + t] = m4[3];
+            s[(TF_CELL + c) * cap + t] = __int_as_float((i2 << 16) | k2);
         }
     }
-    s[SF_U * cap + p] = mk.uDelta;
-    s[SF_V * cap + p] = mk.vDelta;
-    s[SF_WV * cap + p] = mk.wDelta;
+    s[TF_U * cap + t] = mk.uDelta;
+    s[TF_V * cap + t] = mk.vDelta;
+    s[TF_WV * cap + t] = mk.wDelta;
 }
 
-__global__ void __launch_bounds__(256) k_ibm_spread(IbmArgs a) {
-    extern __shared__ uint32_t touched[];   // this plane's mask words, [nx][kw]
-    const int j = blockIdx.x;
+// One CTA per j-plane: the plane's first-segment levels on an F tile in
+// shared memory, then write-back and flags, then the blade levels on the
+// dense F, then the plane's touched flags.
+__global__ void __launch_bounds__(512) k_ibm_spread(IbmArgs a) {
+    extern __shared__ uint32_t smem[];
     const Dims g = a.g;
+    const int j = blockIdx.x;
     const int nwords = g.nx * g.kw;
+    uint32_t* touched = smem;                                   // [nx][kw]
+    float* tile = reinterpret_cast<float*>(smem + nwords);      // [3][smem_cells]
+    const int c0 = a.plane_cell[j], nc = a.plane_cell[j + 1] - c0;
+    const long long C = a.ncell;
+    float *fx, *fy, *fz;
+    if (a.smem_cells > 0) {
+        fx = tile; fy = tile + a.smem_cells; fz = tile + 2 * a.smem_cells;
+    } else {
+        fx = a.cell_F + c0; fy = a.cell_F + C + c0; fz = a.cell_F + 2 * C + c0;
+    }
     for (int w = threadIdx.x; w < nwords; w += blockDim.x) touched[w] = 0u;
+    if (a.smem_cells > 0)
+        for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+            fx[t] = a.cell_F[c0 + t];
+            fy[t] = a.cell_F[C + c0 + t];
+            fz[t] = a.cell_F[2 * C + c0 + t];
+        }
     __syncthreads();
 
-    const float* s = a.scratch;
-    const long long cap = a.cap;
-    const int lv0 = a.plane_lv[j], lv1 = a.plane_lv[j + 1];
-    for (int lv = lv0; lv < lv1; lv++) {
+    // ---- first segment: F lives in the tile; each marker in list order
+    //      relative to every marker it shares a cell with (level walk)
+    const long long n0 = a.n0;
+    const float* rho = a.cell_m + c0;
+    const float* mx = a.cell_m + C + c0;
+    const float* my = a.cell_m + 2 * C + c0;
+    const float* mz = a.cell_m + 3 * C + c0;
+    for (int lv = a.plane_lv0[j]; lv < a.plane_lv0[j + 1]; lv++) {
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
         for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            float w[9];
+            int li[9];
+            float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                w[c] = a.prep[(PF_W + c) * n0 + p];
+                li[c] = __float_as_int(a.prep[(PF_CELL + c) * n0 + p]);
+                rhoSum = fmaf(w[c], rho[li[c]], rhoSum);
+                xSum = fmaf(w[c], fmaf(0.5f, fx[li[c]], mx[li[c]]), xSum);
+                ySum = fmaf(w[c], fmaf(0.5f, fy[li[c]], my[li[c]]), ySum);
+                zSum = fmaf(w[c], fmaf(0.5f, fz[li[c]], mz[li[c]]), zSum);
+            }
+            xSum = fmaf(-rhoSum, a.prep[PF_U * n0 + p], xSum);
+            ySum = fmaf(-rhoSum, a.prep[PF_V * n0 + p], ySum);
+            zSum = fmaf(-rhoSum, a.prep[PF_WV * n0 + p], zSum);
+            a.sums[p] = xSum;
+            a.sums[a.n + p] = ySum;
+            a.sums[2 * a.n + p] = zSum;
+#pragma unroll
+            for (int c = 0; c < 9; c++) {   // sequential: a wrapped stencil sees its own update
+                const float bw = a.beta * w[c];
+                fx[li[c]] = fmaf(a.alpha, fx[li[c]], -bw * xSum);
+                fy[li[c]] = fmaf(a.alpha, fy[li[c]], -bw * ySum);
+                fz[li[c]] = fmaf(a.alpha, fz[li[c]], -bw * zSum);
+            }
+        }
+        __syncthreads();
+    }
+    // ---- write the tile back to F and flag the plane's cells
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+        const int e = a.cell_e[c0 + t];
+        a.Fx[e] = fx[t];
+        a.Fy[e] = fy[t];
+        a.Fz[e] = fz[t];
+        const int row = e / g.kp, k = e - row * g.kp, i = row / g.ny;
+        atomicOr(&touched[i * g.kw + (k >> 5)], 1u << (k & 31));
+    }
+    __syncthreads();
+
+    // ---- second segment (blades): dense F, touched flags of this pass
+    const float* s = a.tail;
+    const long long cap = a.tail_cap;
+    for (int lv = a.plane_lv1[j]; lv < a.plane_lv1[j + 1]; lv++) {
+        const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
+        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            const int t = p - a.n0;
             float w[9];
             long long e[9];
             int sw[9];
@@ -133,45 +246,46 @@ __global__ void __launch_bounds__(256) k_ibm_spread(IbmArgs a) {
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                w[c] = s[(SF_W + c) * cap + p];
-                const int packed = __float_as_int(s[(SF_CELL + c) * cap + p]);
+                w[c] = s[(TF_W + c) * cap + t];
+                const int packed = __float_as_int(s[(TF_CELL + c) * cap + t]);
                 const int i2 = packed >> 16, k2 = packed & 0xffff;
                 const long long row = (long long)i2 * g.ny + j;
                 e[c] = row * g.kp + k2;
                 sw[c] = i2 * g.kw + (k2 >> 5);
                 bit[c] = 1u << (k2 & 31);
                 const bool live = (touched[sw[c]] & bit[c]) || (a.mask_old[row * g.kw + (k2 >> 5)] & bit[c]);
-                const float fx = live ? a.Fx[e[c]] : 0.f;
-                const float fy = live ? a.Fy[e[c]] : 0.f;
-                const float fz = live ? a.Fz[e[c]] : 0.f;
-                rhoSum = fmaf(w[c], s[(SF_RHO + c) * cap + p], rhoSum);
-                xSum = fmaf(w[c], fmaf(0.5f, fx, s[(SF_MX + c) * cap + p]), xSum);
-                ySum = fmaf(w[c], fmaf(0.5f, fy, s[(SF_MY + c) * cap + p]), ySum);
-                zSum = fmaf(w[c], fmaf(0.5f, fz, s[(SF_MZ + c) * cap + p]), zSum);
+                const float vx = live ? a.Fx[e[c]] : 0.f;
+                const float vy = live ? a.Fy[e[c]] : 0.f;
+                const float vz = live ? a.Fz[e[c]] : 0.f;
+                rhoSum = fmaf(w[c], s[(TF_RHO + c) * cap + t], rhoSum);
+                xSum = fmaf(w[c], fmaf(0.5f, vx, s[(TF_MX + c) * cap + t]), xSum);
+                ySum = fmaf(w[c], fmaf(0.5f, vy, s[(TF_MY + c) * cap + t]), ySum);
+                zSum = fmaf(w[c], fmaf(0.5f, vz, s[(TF_MZ + c) * cap + t]), zSum);
             }
-            xSum = fmaf(-rhoSum, s[SF_U * cap + p], xSum);
-            ySum = fmaf(-rhoSum, s[SF_V * cap + p], ySum);
-            zSum = fmaf(-rhoSum, s[SF_WV * cap + p], zSum);
+            xSum = fmaf(-rhoSum, s[TF_U * cap + t], xSum);
+            ySum = fmaf(-rhoSum, s[TF_V * cap + t], ySum);
+            zSum = fmaf(-rhoSum, s[TF_WV * cap + t], zSum);
+            a.sums[p] = xSum;
+            a.sums[a.n + p] = ySum;
+            a.sums[2 * a.n + p] = zSum;
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                // re-evaluated per cell: a stencil that wraps onto itself
-                // (extent < 3) sees its own earlier update, as in the reference
                 const long long row = e[c] / g.kp;
                 const int k2 = (int)(e[c] - row * g.kp);
                 const bool live = (touched[sw[c]] & bit[c]) || (a.mask_old[row * g.kw + (k2 >> 5)] & bit[c]);
-                const float fx = live ? a.Fx[e[c]] : 0.f;
-                const float fy = live ? a.Fy[e[c]] : 0.f;
-                const float fz = live ? a.Fz[e[c]] : 0.f;
+                const float vx = live ? a.Fx[e[c]] : 0.f;
+                const float vy = live ? a.Fy[e[c]] : 0.f;
+                const float vz = live ? a.Fz[e[c]] : 0.f;
                 const float bw = a.beta * w[c];
-                a.Fx[e[c]] = fmaf(a.alpha, fx, -bw * xSum);
-                a.Fy[e[c]] = fmaf(a.alpha, fy, -bw * ySum);
-                a.Fz[e[c]] = fmaf(a.alpha, fz, -bw * zSum);
+                a.Fx[e[c]] = fmaf(a.alpha, vx, -bw * xSum);
+                a.Fy[e[c]] = fmaf(a.alpha, vy, -bw * ySum);
+                a.Fz[e[c]] = fmaf(a.alpha, vz, -bw * zSum);
                 atomicOr(&touched[sw[c]], bit[c]);
             }
         }
         __syncthreads();
     }
-    // publish this plane's touched flags (planes without markers publish zeros)
+    // ---- publish this plane's touched flags (planes without markers publish zeros)
     for (int w = threadIdx.x; w < nwords; w += blockDim.x) {
         const int i = w / g.kw, wk = w - i * g.kw;
         a.mask_new[((long long)i * g.ny + j) * g.kw + wk] = touched[w];
@@ -203,20 +317,81 @@ cudaError_t launch_rotate_markers(const double* xz, Marker* out, int n, double c
     return cudaGetLastError();
 }
 
-size_t ibm_smem_bytes(const Dims& g) { return (size_t)g.nx * g.kw * sizeof(uint32_t); }
+// Deterministic FP64 reduction of the marker forces: fixed grid, fixed
+// per-thread stride, fixed shared-memory tree, then one block sums the
+// partials in order.
+__global__ void __launch_bounds__(256) k_marker_load(IbmArgs a, int begin, double ci, double ck, double* partial) {
+    __shared__ double red[5][256];
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += gridDim.x * blockDim.x) {
+        const int q = a.sched[p];
+        if (q < begin) continue;
+        const Marker mk = a.markers[q];
+        const double fx = -(double)a.beta * (double)a.sums[p];
+        const double fy = -(double)a.beta * (double)a.sums[a.n + p];
+        const double fz = -(double)a.beta * (double)a.sums[2 * a.n + p];
+        const double di = (double)mk.i + (double)mk.iCartFraction - ci;
+        const double dk = (double)mk.k + (double)mk.kCartFraction - ck;
+        acc[0] += fx;
+        acc[1] += fy;
+        acc[2] += fz;
+        acc[3] += dk * fx - di * fz;   // (r x F) along j, r = (di, 0, dk)
+        acc[4] += 1.0;
+    }
+    for (int c = 0; c < 5; c++) red[c][threadIdx.x] = acc[c];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int c = 0; c < 5; c++) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 5; c++) partial[blockIdx.x * 5 + c] = red[c][0];
+}
+
+__global__ void k_marker_load_final(const double* partial, int nblocks, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int b = 0; b < nblocks; b++)
+        for (int c = 0; c < 5; c++) acc[c] += partial[b * 5 + c];
+    for (int c = 0; c < 5; c++) out[c] = acc[c];
+}
+
+cudaError_t launch_marker_load(const IbmArgs& a, int begin, double ci, double ck, double* partial, double* out,
+                               cudaStream_t st) {
+    k_marker_load<<<kLoadBlocks, 256, 0, st>>>(a, begin, ci, ck, partial);
+    k_marker_load_final<<<1, 32, 0, st>>>(partial, kLoadBlocks, out);
+    return cudaGetLastError();
+}
+
+size_t ibm_smem_bytes(const Dims& g, int cells) {
+    return (size_t)g.nx * g.kw * sizeof(uint32_t) + (size_t)3 * cells * sizeof(float);
+}
 
 cudaError_t ibm_prepare_smem(size_t bytes) {
     return cudaFuncSetAttribute(k_ibm_spread, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, cudaStream_t st) {
+    (void)mcell;
+    if (a.n0 <= 0) return cudaSuccess;
+    k_ibm_prepare<<<(a.n0 + 255) / 256, 256, 0, st>>>(a, prep);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
-    if (a.n > 0) {
-        k_ibm_gather<<<(a.n + 127) / 128, 128, 0, st>>>(a);
+    if (a.ncell > 0) {
+        k_ibm_cells<<<(a.ncell + 255) / 256, 256, 0, st>>>(a);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }
-    const size_t smem = ibm_smem_bytes(a.g);
-    k_ibm_spread<<<a.g.ny, 256, smem, st>>>(a);
+    if (a.n > a.n0) {
+        k_ibm_gather_tail<<<(a.n - a.n0 + 127) / 128, 128, 0, st>>>(a);
+        cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
+    }
+    const size_t smem = ibm_smem_bytes(a.g, a.smem_cells);
+    k_ibm_spread<<<a.g.ny, 512, smem, st>>>(a);
     return cudaGetLastError();
 }
 

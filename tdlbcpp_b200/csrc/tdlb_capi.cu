@@ -59,24 +59,42 @@ struct tdlb_lattice {
     bool holds_moments = true;   // state is in moment form (after initialise)
     bool even = true;            // Esotwist parity (ComputeUnit.hpp:116)
     int pass = 0;                // forcing passes so far; mask[pass & 1] is current
+    int vec = 4;                 // cells per thread of the step kernels
     bool initialised = false;
 
-    // markers
+    // markers: the resident list and its two-segment schedule
     tdlb::Marker* d_markers = nullptr;
     int* d_sched = nullptr;
     int* d_level_ptr = nullptr;
-    int* d_plane_lv = nullptr;
-    float* d_scratch = nullptr;
+    int* d_plane_lv0 = nullptr;
+    int* d_plane_lv1 = nullptr;
+    // first-segment cell lists and per-pass IBM buffers
+    tdlb::CellList cells;
+    int* d_cell_e = nullptr;
+    int* d_plane_cell = nullptr;
+    float* d_prep = nullptr;      // PF_COUNT * n0
+    float* d_cell_m = nullptr;    // 4 * C0
+    float* d_cell_F = nullptr;    // 3 * C0
+    float* d_tail = nullptr;      // TF_COUNT * tail_cap
+    long long tail_cap = 0;
+    float* d_sums = nullptr;      // 3 * marker_cap
+    int smem_cells = 0;
     long long marker_cap = 0;
     long long level_cap = 0;
-    int n_markers = 0;
-    int n_levels = 0;
-    tdlb::MarkerSchedule sched;
-    // resident impeller: markers [rot_begin, rot_begin + n_rot) rotate
-    double* d_rot_xz = nullptr;
-    int rot_begin = -1;
-    int n_rot = 0;
+    int n_markers = 0;      // list length
+    int n0 = 0;             // markers of the first segment (the rest rotate)
+    std::vector<tdlb_marker> h_markers;   // host copy of the resident list
+    tdlb::MarkerSchedule seg0, seg1;
+    bool markers_set = false;
+    float last_beta = 0.f;        // beta of the last forcing pass (for the load)
+    // resident impeller: markers [n0, n_markers) are blades
+    double* d_rot_xz = nullptr;   // their impeller-frame offsets (device rotation)
+    bool rot_device = false;
     double rot_ci = 0, rot_ck = 0;
+    int impeller_begin = -1;      // first marker of the impeller (-1: none)
+    double* d_load = nullptr;     // kLoadBlocks*5 partials + 5 results
+    tdlb_marker* h_stage = nullptr;   // pinned staging of the blade upload
+    size_t stage_cap = 0;
 
     std::string err = "no error";
 
@@ -108,9 +126,18 @@ void release(tdlb_lattice* h) {
     cudaFree(h->d_markers);
     cudaFree(h->d_sched);
     cudaFree(h->d_level_ptr);
-    cudaFree(h->d_plane_lv);
-    cudaFree(h->d_scratch);
+    cudaFree(h->d_plane_lv0);
+    cudaFree(h->d_plane_lv1);
+    cudaFree(h->d_cell_e);
+    cudaFree(h->d_plane_cell);
+    cudaFree(h->d_prep);
+    cudaFree(h->d_cell_m);
+    cudaFree(h->d_cell_F);
+    cudaFree(h->d_tail);
+    cudaFree(h->d_sums);
     cudaFree(h->d_rot_xz);
+    cudaFree(h->d_load);
+    cudaFreeHost(h->h_stage);
     if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -145,7 +172,9 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
         g.kw = (g.kp + 31) / 32;
         g.plane = round_up((long long)g.nx * g.ny * g.kp, 64);
         h->mask_words = round_up((long long)g.nx * g.ny * g.kw, 64);
-        if (tdlb::ibm_smem_bytes(g) > 200 * 1024)
+        if ((long long)g.nx * g.ny * g.kp >= (1LL << 31) - 64)
+            throw Fail{TDLB_EINVAL, "lattice too large: one population plane must stay below 2^31 elements"};
+        if (tdlb::ibm_smem_bytes(g, 0) > 200 * 1024)
             throw Fail{TDLB_EINVAL, "x * ceil(z/32) too large for the per-plane IBM flag tile"};
         h->cp = tdlb::make_collide_params(c.nu, c.cs0, c.g3);
 
@@ -167,8 +196,6 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
         TDLB_CK(cudaMemsetAsync(h->F, 0, (size_t)3 * g.plane * sizeof(float), h->stream));
         TDLB_CK(cudaMemsetAsync(h->mask, 0, (size_t)2 * h->mask_words * sizeof(uint32_t), h->stream));
         TDLB_CK(cudaStreamSynchronize(h->stream));
-        const size_t smem = tdlb::ibm_smem_bytes(g);
-        if (smem > 48 * 1024) TDLB_CK(tdlb::ibm_prepare_smem(smem));
     } catch (...) {
         release(h);
         delete h;
@@ -259,6 +286,7 @@ tdlb::StepArgs step_args(tdlb_lattice* h, bool collide) {
     a.from_moments = h->holds_moments ? 1 : 0;
     a.collide = collide ? 1 : 0;
     a.even = h->even ? 1 : 0;
+    a.vec = h->vec;
     return a;
 }
 
@@ -274,63 +302,140 @@ void run_step(tdlb_lattice* h, bool collide) {
     h->holds_moments = false;
 }
 
-void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, int rot_begin = -1,
-                    const double* rot_xz = nullptr) {
-    if (n > 0 && !m) throw Fail{TDLB_EINVAL, "markers is NULL"};
-    if (n > (size_t)0x7fffffff) throw Fail{TDLB_EINVAL, "too many markers"};
-    const Dims& g = h->g;
+tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta);
+
+void validate_markers(const Dims& g, const tdlb_marker* m, size_t n, size_t base) {
     for (size_t q = 0; q < n; q++) {
         if (m[q].i < 0 || m[q].i >= g.nx || m[q].j < 0 || m[q].j >= g.ny || m[q].k < 0 || m[q].k >= g.nz) {
             char buf[160];
-            std::snprintf(buf, sizeof buf, "marker %zu at (%lld,%lld,%lld) outside the %dx%dx%d interior", q,
+            std::snprintf(buf, sizeof buf, "marker %zu at (%lld,%lld,%lld) outside the %dx%dx%d interior", base + q,
                           (long long)m[q].i, (long long)m[q].j, (long long)m[q].k, g.nx, g.ny, g.nz);
             throw Fail{TDLB_EINVAL, buf};
         }
     }
+}
+
+void ensure_level_cap(tdlb_lattice* h, long long need) {
+    if (need <= h->level_cap && h->d_level_ptr) return;
+    TDLB_CK(cudaStreamSynchronize(h->stream));
+    cudaFree(h->d_level_ptr);
+    h->d_level_ptr = nullptr;
+    const long long cap = std::max<long long>(round_up(need * 2, 1024), 1024);
+    TDLB_CK(cudaMalloc(&h->d_level_ptr, cap * sizeof(int)));
+    h->level_cap = cap;
+}
+
+// Device copy of the second segment's schedule (slots n0.., levels L0..).
+void upload_seg1(tdlb_lattice* h) {
+    const Dims& g = h->g;
+    const int L0 = h->seg0.nlevels;
+    ensure_level_cap(h, (long long)L0 + h->seg1.nlevels + 1);
+    const int n1 = h->n_markers - h->n0;
+    if (n1) TDLB_CK(cudaMemcpyAsync(h->d_sched + h->n0, h->seg1.order.data(), (size_t)n1 * sizeof(int),
+                                    cudaMemcpyHostToDevice, h->stream));
+    TDLB_CK(cudaMemcpyAsync(h->d_level_ptr + L0, h->seg1.level_ptr.data(), h->seg1.level_ptr.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, h->stream));
+    TDLB_CK(cudaMemcpyAsync(h->d_plane_lv1, h->seg1.plane_lv.data(), (size_t)(g.ny + 1) * sizeof(int),
+                            cudaMemcpyHostToDevice, h->stream));
+}
+
+// Make `m[0, n)` the resident list: segment 0 = [0, n0) with exact levels,
+// segment 1 = [n0, n), rotation-invariant when rot_xz is given.
+void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, const double* rot_xz) {
+    if (n > 0 && !m) throw Fail{TDLB_EINVAL, "markers is NULL"};
+    if (n > (size_t)0x7fffffff) throw Fail{TDLB_EINVAL, "too many markers"};
+    const Dims& g = h->g;
+    validate_markers(g, m, n, 0);
     static_assert(sizeof(tdlb_marker) == sizeof(tdlb::Marker), "marker layout");
-    h->sched.build(reinterpret_cast<const tdlb::Marker*>(m), (int)n, g.nx, g.ny, g.nz, rot_begin, rot_xz);
-    h->rot_begin = -1;   // a plain upload detaches the resident impeller
-    h->n_rot = 0;
-    const long long nl = (long long)h->sched.level_ptr.size();
+    TDLB_CK(cudaStreamSynchronize(h->stream));   // host vectors below are read by queued copies
+    h->h_markers.assign(m, m + n);
+    const auto* mk = reinterpret_cast<const tdlb::Marker*>(h->h_markers.data());
+    h->n_markers = (int)n;
+    h->n0 = (int)n0;
+    h->seg0.build(mk, 0, (int)n0, g.nx, g.ny, g.nz, 0, 0);
+    h->seg1.build(mk, (int)n0, (int)n, g.nx, g.ny, g.nz, (int)n0, h->seg0.nlevels, rot_xz);
     if ((long long)n > h->marker_cap) {
-        cudaFree(h->d_markers); cudaFree(h->d_sched); cudaFree(h->d_scratch);
-        h->d_markers = nullptr; h->d_sched = nullptr; h->d_scratch = nullptr;
+        cudaFree(h->d_markers); cudaFree(h->d_sched); cudaFree(h->d_sums);
+        h->d_markers = nullptr; h->d_sched = nullptr; h->d_sums = nullptr;
         const long long cap = std::max<long long>(round_up((long long)n, 1024), 1024);
         TDLB_CK(cudaMalloc(&h->d_markers, cap * sizeof(tdlb::Marker)));
         TDLB_CK(cudaMalloc(&h->d_sched, cap * sizeof(int)));
-        TDLB_CK(cudaMalloc(&h->d_scratch, (size_t)tdlb::SF_COUNT * cap * sizeof(float)));
+        TDLB_CK(cudaMalloc(&h->d_sums, (size_t)3 * cap * sizeof(float)));
         h->marker_cap = cap;
     }
-    if (nl > h->level_cap || !h->d_plane_lv) {
-        cudaFree(h->d_level_ptr); cudaFree(h->d_plane_lv);
-        h->d_level_ptr = nullptr; h->d_plane_lv = nullptr;
-        const long long cap = std::max<long long>(round_up(nl, 1024), 1024);
-        TDLB_CK(cudaMalloc(&h->d_level_ptr, cap * sizeof(int)));
-        TDLB_CK(cudaMalloc(&h->d_plane_lv, (size_t)(g.ny + 1) * sizeof(int)));
-        h->level_cap = cap;
+    const long long ntail = (long long)n - (long long)n0;
+    if (ntail > h->tail_cap) {
+        cudaFree(h->d_tail);
+        h->d_tail = nullptr;
+        const long long cap = round_up(ntail, 256);
+        TDLB_CK(cudaMalloc(&h->d_tail, (size_t)tdlb::TF_COUNT * cap * sizeof(float)));
+        h->tail_cap = cap;
     }
-    if (n) {
-        TDLB_CK(cudaMemcpyAsync(h->d_markers, m, n * sizeof(tdlb::Marker), cudaMemcpyHostToDevice, h->stream));
-        TDLB_CK(cudaMemcpyAsync(h->d_sched, h->sched.order.data(), n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    // first segment: unique cells per plane, slot data
+    h->cells.build(mk, h->seg0, g.nx, g.ny, g.nz, g.kp);
+    const long long C0 = (long long)h->cells.cell_e.size();
+    cudaFree(h->d_cell_e); cudaFree(h->d_plane_cell); cudaFree(h->d_prep); cudaFree(h->d_cell_m); cudaFree(h->d_cell_F);
+    h->d_cell_e = nullptr; h->d_plane_cell = nullptr; h->d_prep = nullptr; h->d_cell_m = nullptr; h->d_cell_F = nullptr;
+    TDLB_CK(cudaMalloc(&h->d_plane_cell, (size_t)(g.ny + 1) * sizeof(int)));
+    if (C0) {
+        TDLB_CK(cudaMalloc(&h->d_cell_e, C0 * sizeof(int)));
+        TDLB_CK(cudaMalloc(&h->d_cell_m, 4 * C0 * sizeof(float)));
+        TDLB_CK(cudaMalloc(&h->d_cell_F, 3 * C0 * sizeof(float)));
     }
-    TDLB_CK(cudaMemcpyAsync(h->d_level_ptr, h->sched.level_ptr.data(), nl * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    TDLB_CK(cudaMemcpyAsync(h->d_plane_lv, h->sched.plane_lv.data(), (g.ny + 1) * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    // the host vectors are reused by the next upload: wait for the copies
+    if (n0) TDLB_CK(cudaMalloc(&h->d_prep, (size_t)tdlb::PF_COUNT * n0 * sizeof(float)));
+    {
+        const size_t fit = 220 * 1024;
+        const int mc = h->cells.max_plane_cells;
+        h->smem_cells = tdlb::ibm_smem_bytes(g, mc) <= fit ? mc : 0;
+        const size_t bytes = tdlb::ibm_smem_bytes(g, h->smem_cells);
+        if (bytes > 48 * 1024) TDLB_CK(tdlb::ibm_prepare_smem(bytes));
+    }
+    if (!h->d_plane_lv0) {
+        TDLB_CK(cudaMalloc(&h->d_plane_lv0, (size_t)(g.ny + 1) * sizeof(int)));
+        TDLB_CK(cudaMalloc(&h->d_plane_lv1, (size_t)(g.ny + 1) * sizeof(int)));
+    }
+    ensure_level_cap(h, (long long)h->seg0.nlevels + h->seg1.nlevels + 1);
+    if (n) TDLB_CK(cudaMemcpyAsync(h->d_markers, m, n * sizeof(tdlb::Marker), cudaMemcpyHostToDevice, h->stream));
+    if (n0) TDLB_CK(cudaMemcpyAsync(h->d_sched, h->seg0.order.data(), n0 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    TDLB_CK(cudaMemcpyAsync(h->d_level_ptr, h->seg0.level_ptr.data(), h->seg0.level_ptr.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, h->stream));
+    TDLB_CK(cudaMemcpyAsync(h->d_plane_lv0, h->seg0.plane_lv.data(), (size_t)(g.ny + 1) * sizeof(int),
+                            cudaMemcpyHostToDevice, h->stream));
+    upload_seg1(h);
+    TDLB_CK(cudaMemcpyAsync(h->d_plane_cell, h->cells.plane_cell.data(), (size_t)(g.ny + 1) * sizeof(int),
+                            cudaMemcpyHostToDevice, h->stream));
+    if (C0) TDLB_CK(cudaMemcpyAsync(h->d_cell_e, h->cells.cell_e.data(), C0 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    if (n0) {
+        TDLB_CK(cudaMemcpyAsync(h->d_prep + (size_t)tdlb::PF_CELL * n0, h->cells.mcell.data(), (size_t)9 * n0 * sizeof(int),
+                                cudaMemcpyHostToDevice, h->stream));
+        tdlb::IbmArgs a = ibm_args(h, 0.f, 0.f);
+        TDLB_CK(tdlb::launch_ibm_prepare(a, h->d_prep, nullptr, h->stream));
+    }
     TDLB_CK(cudaStreamSynchronize(h->stream));
-    h->n_markers = (int)n;
-    h->n_levels = (int)nl - 1;
+    h->markers_set = true;
+    h->rot_device = false;
+    h->impeller_begin = -1;
 }
 
-void run_forcing(tdlb_lattice* h, float alpha, float beta) {
-    if (!h->d_plane_lv) throw Fail{TDLB_ESTATE, "no markers set (tdlb_set_markers / tdlb_forcing)"};
+tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     tdlb::IbmArgs a{};
     a.markers = h->d_markers;
     a.sched = h->d_sched;
     a.level_ptr = h->d_level_ptr;
-    a.plane_lv = h->d_plane_lv;
+    a.plane_lv0 = h->d_plane_lv0;
+    a.plane_lv1 = h->d_plane_lv1;
     a.n = h->n_markers;
-    a.scratch = h->d_scratch;
-    a.cap = h->marker_cap;
+    a.n0 = h->n0;
+    a.cell_e = h->d_cell_e;
+    a.plane_cell = h->d_plane_cell;
+    a.ncell = (int)h->cells.cell_e.size();
+    a.prep = h->d_prep;
+    a.cell_m = h->d_cell_m;
+    a.cell_F = h->d_cell_F;
+    a.tail = h->d_tail;
+    a.tail_cap = h->tail_cap;
+    a.sums = h->d_sums;
+    a.smem_cells = h->smem_cells;
     a.A = h->planes(h->state_buf());
     a.state_mode = h->state_mode();
     a.even = h->even ? 1 : 0;
@@ -342,8 +447,14 @@ void run_forcing(tdlb_lattice* h, float alpha, float beta) {
     a.g = h->g;
     a.alpha = alpha;
     a.beta = beta;
-    TDLB_CK(tdlb::launch_ibm(a, h->stream));
+    return a;
+}
+
+void run_forcing(tdlb_lattice* h, float alpha, float beta) {
+    if (!h->markers_set) throw Fail{TDLB_ESTATE, "no markers set (tdlb_set_markers / tdlb_forcing)"};
+    TDLB_CK(tdlb::launch_ibm(ibm_args(h, alpha, beta), h->stream));
     h->pass++;
+    h->last_beta = beta;
 }
 
 // Copy an interior-cell plane set (npl planes of the device layout) to a
@@ -460,7 +571,7 @@ int tdlb_initialise(tdlb_handle h, float rho) {
 }
 
 int tdlb_set_markers(tdlb_handle h, const tdlb_marker* markers, size_t n) {
-    return guarded(h, [&] { upload_markers(h, markers, n); });
+    return guarded(h, [&] { upload_markers(h, markers, n, n, nullptr); });
 }
 
 int tdlb_forcing_resident(tdlb_handle h, float alpha, float beta) {
@@ -473,7 +584,7 @@ int tdlb_forcing_resident(tdlb_handle h, float alpha, float beta) {
 int tdlb_forcing(tdlb_handle h, const tdlb_marker* markers, size_t n, float alpha, float beta) {
     return guarded(h, [&] {
         require_init(h);
-        upload_markers(h, markers, n);
+        upload_markers(h, markers, n, n, nullptr);
         run_forcing(h, alpha, beta);
     });
 }
@@ -590,6 +701,20 @@ int tdlb_get_even_step(tdlb_handle h, int* even) {
     });
 }
 
+int tdlb_set_cells_per_thread(tdlb_handle h, int v) {
+    return guarded(h, [&] {
+        if (v != 1 && v != 2 && v != 4) throw Fail{TDLB_EINVAL, "cells per thread must be 1, 2 or 4"};
+        h->vec = v;
+    });
+}
+
+int tdlb_get_stream(tdlb_handle h, void** stream) {
+    return guarded(h, [&] {
+        if (!stream) throw Fail{TDLB_EINVAL, "out is NULL"};
+        *stream = (void*)h->stream;
+    });
+}
+
 int tdlb_synchronize(tdlb_handle h) {
     return guarded(h, [&] { TDLB_CK(cudaStreamSynchronize(h->stream)); });
 }
@@ -602,9 +727,10 @@ int tdlb_attach_rushton(tdlb_handle h, const tdlb_rushton* spec, double nonupdat
             throw Fail{TDLB_EINVAL, "Rushton spec extents differ from the lattice"};
         const tdlb::RushtonGeom G = tdlb::RushtonGeom::from(*spec);
         std::vector<tdlb_marker> all = G.fixed();
+        const int n_fixed = (int)all.size();
         const std::vector<tdlb_marker> nonupd = G.rotating_nonupdating(nonupdating_delta_angle);
         all.insert(all.end(), nonupd.begin(), nonupd.end());
-        const int rot_begin = (int)all.size();
+        const size_t n0 = all.size();
         const std::vector<tdlb_marker> rot = G.rotating(angle, delta_angle);
         all.insert(all.end(), rot.begin(), rot.end());
         const std::vector<tdlb::RotatingPolar> pol = G.rotating_polar();
@@ -617,26 +743,65 @@ int tdlb_attach_rushton(tdlb_handle h, const tdlb_rushton* spec, double nonupdat
         }
         if (G.ci - rmax < 2.0 || G.ci + rmax > h->g.nx - 3.0 || G.ck - rmax < 2.0 || G.ck + rmax > h->g.nz - 3.0)
             throw Fail{TDLB_EINVAL, "impeller does not stay 2 cells inside the lattice"};
-        upload_markers(h, all.data(), all.size(), rot_begin, xz.data());
+        upload_markers(h, all.data(), all.size(), n0, xz.data());
         cudaFree(h->d_rot_xz);
         h->d_rot_xz = nullptr;
         if (!xz.empty()) {
             TDLB_CK(cudaMalloc(&h->d_rot_xz, xz.size() * sizeof(double)));
             TDLB_CK(cudaMemcpy(h->d_rot_xz, xz.data(), xz.size() * sizeof(double), cudaMemcpyHostToDevice));
         }
-        h->rot_begin = rot_begin;
-        h->n_rot = (int)pol.size();
+        h->rot_device = true;
         h->rot_ci = G.ci;
         h->rot_ck = G.ck;
+        h->impeller_begin = n_fixed;
     });
 }
 
 int tdlb_rotate_impeller(tdlb_handle h, double angle, double delta_angle) {
     return guarded(h, [&] {
-        if (h->rot_begin < 0) throw Fail{TDLB_ESTATE, "no impeller attached (tdlb_attach_rushton)"};
-        TDLB_CK(tdlb::launch_rotate_markers(h->d_rot_xz, h->d_markers + h->rot_begin, h->n_rot, std::cos(angle),
+        if (!h->rot_device) throw Fail{TDLB_ESTATE, "no impeller attached (tdlb_attach_rushton)"};
+        TDLB_CK(tdlb::launch_rotate_markers(h->d_rot_xz, h->d_markers + h->n0, h->n_markers - h->n0, std::cos(angle),
                                             std::sin(angle), delta_angle, h->rot_ci, h->rot_ck, h->g.nx, h->g.nz,
                                             h->stream));
+    });
+}
+
+int tdlb_set_rotating_markers(tdlb_handle h, const tdlb_marker* markers, size_t n) {
+    return guarded(h, [&] {
+        if (h->impeller_begin < 0) throw Fail{TDLB_ESTATE, "no impeller attached (tdlb_attach_rushton)"};
+        if (n != (size_t)(h->n_markers - h->n0)) throw Fail{TDLB_EINVAL, "rotating marker count differs from the attached blades"};
+        if (n && !markers) throw Fail{TDLB_EINVAL, "markers is NULL"};
+        validate_markers(h->g, markers, n, (size_t)h->n0);
+        TDLB_CK(cudaStreamSynchronize(h->stream));   // previous tail copies read h_markers / seg1
+        std::copy(markers, markers + n, h->h_markers.begin() + h->n0);
+        const auto* mk = reinterpret_cast<const tdlb::Marker*>(h->h_markers.data());
+        h->seg1.build(mk, h->n0, h->n_markers, h->g.nx, h->g.ny, h->g.nz, h->n0, h->seg0.nlevels, nullptr);
+        if (n > h->stage_cap) {
+            cudaFreeHost(h->h_stage);
+            h->h_stage = nullptr;
+            TDLB_CK(cudaHostAlloc((void**)&h->h_stage, n * sizeof(tdlb_marker), cudaHostAllocDefault));
+            h->stage_cap = n;
+        }
+        std::copy(markers, markers + n, h->h_stage);
+        if (n) TDLB_CK(cudaMemcpyAsync(h->d_markers + h->n0, h->h_stage, n * sizeof(tdlb::Marker),
+                                       cudaMemcpyHostToDevice, h->stream));
+        upload_seg1(h);
+        h->rot_device = false;   // the blades now follow the host's list
+    });
+}
+
+int tdlb_impeller_load(tdlb_handle h, double* out5) {
+    return guarded(h, [&] {
+        if (!out5) throw Fail{TDLB_EINVAL, "out is NULL"};
+        if (h->impeller_begin < 0) throw Fail{TDLB_ESTATE, "no impeller attached (tdlb_attach_rushton)"};
+        if (h->pass == 0) throw Fail{TDLB_ESTATE, "no forcing pass yet"};
+        if (!h->d_load) TDLB_CK(cudaMalloc(&h->d_load, (size_t)(tdlb::kLoadBlocks * 5 + 5) * sizeof(double)));
+        tdlb::IbmArgs a = ibm_args(h, 0.f, h->last_beta);
+        TDLB_CK(tdlb::launch_marker_load(a, h->impeller_begin, h->rot_ci, h->rot_ck, h->d_load,
+                                         h->d_load + tdlb::kLoadBlocks * 5, h->stream));
+        TDLB_CK(cudaMemcpyAsync(out5, h->d_load + tdlb::kLoadBlocks * 5, 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                                h->stream));
+        TDLB_CK(cudaStreamSynchronize(h->stream));
     });
 }
 
@@ -660,7 +825,7 @@ int tdlb_schedule_levels(const tdlb_marker* markers, size_t n, int64_t x, int64_
             markers[q].k >= z)
             return TDLB_EINVAL;
     tdlb::MarkerSchedule s;
-    s.build(reinterpret_cast<const tdlb::Marker*>(markers), (int)n, (int)x, (int)y, (int)z);
+    s.build(reinterpret_cast<const tdlb::Marker*>(markers), 0, (int)n, (int)x, (int)y, (int)z, 0, 0);
     if (level_out) {
         // level within its plane, from the plane's first level
         for (int64_t j = 0; j < y; j++)

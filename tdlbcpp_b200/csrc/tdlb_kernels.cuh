@@ -19,6 +19,7 @@ struct StepArgs {
     int from_moments;       // state holds moments (after initialise / checkpoint load)
     int collide;            // 0: transport only (identity collision; known-answer tests)
     int even;               // Esotwist parity (evenStep)
+    int vec;                // cells per thread: 1, 2 or 4 (float, float2, float4 traffic)
 };
 
 cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st);
@@ -35,25 +36,45 @@ struct Marker {
 };
 static_assert(sizeof(Marker) == 48, "Marker layout");
 
-// Per-marker scratch written by the gather phase, read by the spread phase,
-// field-major so consecutive markers of a level load contiguously.
-enum ScratchField {
-    SF_W = 0,               // 9 stencil weights, (k1, i1) order
-    SF_RHO = 9,             // 9 densities
-    SF_MX = 18, SF_MY = 27, SF_MZ = 36,   // 9 momenta each
-    SF_U = 45, SF_V = 46, SF_WV = 47,     // marker velocity
-    SF_CELL = 48,           // 9 cell element indices (int32 bit patterns)
-    SF_COUNT = 57
+// Blade (second-segment) scratch written by k_ibm_gather_tail, read by the
+// spread walk; field-major over the segment's slots.
+enum TailField {
+    TF_W = 0,               // 9 stencil weights, (k1, i1) order
+    TF_RHO = 9,             // 9 densities
+    TF_MX = 18, TF_MY = 27, TF_MZ = 36,   // 9 momenta each
+    TF_U = 45, TF_V = 46, TF_WV = 47,     // marker velocity
+    TF_CELL = 48,           // 9 packed (i << 16 | k) cells (int32 bit patterns)
+    TF_COUNT = 57
+};
+
+// First-segment (static markers) data prepared once per upload, per slot
+// p < n0: 9 weights, 9 plane-local cell indices, the marker velocity.
+enum PrepField {
+    PF_W = 0,
+    PF_CELL = 9,            // int32 bit patterns
+    PF_U = 18, PF_V = 19, PF_WV = 20,
+    PF_COUNT = 21
 };
 
 struct IbmArgs {
     const Marker* markers;      // device copy of the marker list (list order)
     const int* sched;           // execution order: marker index per slot
     const int* level_ptr;       // [nlevels+1] slot offsets of each level
-    const int* plane_lv;        // [ny+1] first level of each j-plane
+    const int* plane_lv0;       // [ny+1] levels of each j-plane, first segment
+    const int* plane_lv1;       // [ny+1] levels of each j-plane, second segment (walked after the first)
     int n;                      // number of markers
-    float* scratch;             // SF_COUNT * cap floats
-    long long cap;              // scratch stride (>= n)
+    int n0;                     // markers (slots) of the first segment
+    // first segment: unique stencil cells, sorted by (j, i, k)
+    const int* cell_e;          // [C0] element index of each cell
+    const int* plane_cell;      // [ny+1] cell range of each plane
+    int ncell;                  // C0
+    const float* prep;          // PF_COUNT * n0 (slot-major fields)
+    float* cell_m;              // 4 * C0: rho, jx, jy, jz of each cell this pass
+    float* cell_F;              // 3 * C0: F of each cell at the start of this pass
+    float* tail;                // TF_COUNT * ntail_cap
+    long long tail_cap;
+    float* sums;                // 3 * n: each slot's spread sums (for the impeller load)
+    int smem_cells;             // F tile capacity per plane in shared memory (0: use cell_F in place)
     Planes A;                   // current state
     int state_mode;             // 0 Simple pops, 1 moments, 2 Esotwist pops, 3 Esotwist moments
     int even;                   // Esotwist parity of the state's read map
@@ -65,9 +86,20 @@ struct IbmArgs {
 };
 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st);
-size_t ibm_smem_bytes(const Dims& g);
+// Per-upload preparation of the first segment (weights, velocities).
+cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, cudaStream_t st);
+// Shared memory the spread kernel needs: the plane's touched-flag tile plus
+// an F tile of `cells` cells.
+size_t ibm_smem_bytes(const Dims& g, int cells);
 // Opt the spread kernel in to `bytes` of dynamic shared memory (> 48 KiB).
 cudaError_t ibm_prepare_smem(size_t bytes);
+// FP64 force and torque of markers [begin, n) (by list index) of the last
+// forcing pass: out[0..2] = -beta * sum of spread sums, out[3] = torque about
+// the tank axis (ci, ck), out[4] = number of markers summed. `partial` holds
+// kLoadBlocks * 5 doubles.
+constexpr int kLoadBlocks = 128;
+cudaError_t launch_marker_load(const IbmArgs& a, int begin, double ci, double ck, double* partial, double* out,
+                               cudaStream_t st);
 // Recompute n rotating markers (offsets xz[2n]) for cos/sin (ca, sa).
 cudaError_t launch_rotate_markers(const double* xz, Marker* out, int n, double ca, double sa, double omega, double ci,
                                   double ck, int nx, int nz, cudaStream_t st);

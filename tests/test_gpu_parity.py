@@ -45,12 +45,14 @@ def ghosted(interior, fill=-7.0):
 
 # ---------------------------------------------------------------- transport
 
-@pytest.mark.parametrize("dims", [(3, 3, 3), (4, 5, 6), (7, 3, 5), (5, 6, 37), (2, 9, 70), (1, 1, 1)])
-def test_transport_simple_bit_exact(gpu, port_oracle, dims):
+@pytest.mark.parametrize("vec", [1, 2, 4])
+@pytest.mark.parametrize("dims", [(3, 3, 3), (4, 5, 6), (7, 3, 5), (5, 6, 37), (2, 9, 70), (1, 1, 1), (3, 2, 131)])
+def test_transport_simple_bit_exact(gpu, port_oracle, dims, vec):
     tb, po = gpu, port_oracle
     x, y, z = dims
     codes = coded_state(x, y, z)
     cu = tb.ComputeUnit(x=x, y=y, z=z, nu=1e-3)
+    cu.set_cells_per_thread(vec)
     cu.debug_set_state(codes, holds_moments=False)
     ref = po.CpuLattice("port", x, y, z, po.Flow(), "Simple", 8)
     ref.set_q(ghosted(codes))
@@ -61,12 +63,14 @@ def test_transport_simple_bit_exact(gpu, port_oracle, dims):
     cu.close()
 
 
-@pytest.mark.parametrize("dims", [(3, 3, 3), (4, 5, 6), (7, 3, 5), (5, 6, 37), (2, 9, 70), (1, 2, 1)])
-def test_transport_esotwist_bit_exact(gpu, port_oracle, dims):
+@pytest.mark.parametrize("vec", [1, 2, 4])
+@pytest.mark.parametrize("dims", [(3, 3, 3), (4, 5, 6), (7, 3, 5), (5, 6, 37), (2, 9, 70), (1, 2, 1), (3, 2, 131)])
+def test_transport_esotwist_bit_exact(gpu, port_oracle, dims, vec):
     tb, po = gpu, port_oracle
     x, y, z = dims
     codes = coded_state(x, y, z)
     cu = tb.ComputeUnit(x=x, y=y, z=z, nu=1e-3, streaming=tb.STREAMING_ESOTWIST)
+    cu.set_cells_per_thread(vec)
     cu.debug_set_state(codes, holds_moments=False)
     ref = po.CpuLattice("port", x, y, z, po.Flow(), "Esotwist", 8)
     ref.set_q(ghosted(codes))
@@ -272,6 +276,31 @@ def test_rushton_tank_60_cubed_20_steps_vs_reference(gpu, ref_oracle, port_oracl
     assert rel_l2(ug, u64) <= 2.0 * rel_l2(ur, u64) + 1e-7
     assert rel_l2(mg[..., 0], m64[..., 0]) <= 2.0 * rel_l2(mr[..., 0], m64[..., 0]) + 1e-7
     cu.close()
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_step_variants_bit_identical(gpu, streaming):
+    """1, 2 and 4 cells per thread run the same per-cell arithmetic: the
+    states after several full steps must be bit-identical."""
+    tb = gpu
+    x, y, z = 10, 9, 37
+    rng = np.random.default_rng(5)
+    mk = random_markers(tb, rng, 60, x, y, z)
+    states = []
+    for vec in (1, 2, 4):
+        cu = tb.ComputeUnit(x=x, y=y, z=z, nu=5e-4, cs0=0.1, useLES=1,
+                            streaming=tb.STREAMING_SIMPLE if streaming == "Simple" else tb.STREAMING_ESOTWIST)
+        cu.set_cells_per_thread(vec)
+        cu.initialise(1.0)
+        cu.forcing(mk, ALPHA, BETA)
+        for _ in range(5):
+            cu.collision()
+            cu.forcing(mk, ALPHA, BETA)
+        states.append((cu.debug_get_state(), cu.read_nu(), cu.read_force()))
+        cu.close()
+    for other in states[1:]:
+        for a, b in zip(states[0], other):
+            np.testing.assert_array_equal(a, b)
 
 
 def test_marker_positions_bit_exact_on_device(gpu):
