@@ -90,6 +90,7 @@ def load(kind: str) -> ctypes.CDLL:
     if kind == "port":
         sig["get_o"] = (None, [vp, vp])
         sig["transport"] = (None, [vp])
+        sig["get_forcing_sums"] = (None, [vp, vp, cl])
         sig["set_threads"] = (None, [ci])
     else:
         sig["kat_simple_golden"] = (ci, [ci, vp])
@@ -212,6 +213,12 @@ class CpuLattice:
     def transport(self):
         """Identity-collision step: Simple push, or Esotwist read+write+flip (port only)."""
         self._fn("transport")(self.h)
+
+    def get_forcing_sums(self, n: int) -> np.ndarray:
+        """Per-marker spread sums [n, 3] of the last forcing() (port only)."""
+        out = np.empty((n, 3), np.float64)
+        self._fn("get_forcing_sums")(self.h, _ptr(out), n)
+        return out
 
     def get_o(self) -> np.ndarray:
         """Cells the last forcing() touched (port only; the reference resets O)."""

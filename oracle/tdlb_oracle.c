@@ -69,7 +69,7 @@ typedef struct Handle {
         L->Olast = calloc(L->size, 1);                                            \
     } while (0)
 
-#define FREE_LATTICE(L) do { free(L->Q); free(L->Qtmp); free(L->F); free(L->Nu); free(L->O); free(L->Olast); free(L); } while (0)
+#define FREE_LATTICE(L) do { free(L->Q); free(L->Qtmp); free(L->F); free(L->Nu); free(L->O); free(L->Olast); free(L->sums); free(L); } while (0)
 
 void tdlbo_set_threads(int n) {
 #ifdef _OPENMP
@@ -128,6 +128,12 @@ void tdlbo_get_f(void* h, double* out) { DISPATCH(h, COPY_OUT(LAT32(h), F, LAT32
 void tdlbo_set_f(void* h, const double* in) { DISPATCH(h, COPY_IN(LAT32(h), F, LAT32(h)->size * 3, in, float), COPY_IN(LAT64(h), F, LAT64(h)->size * 3, in, double)); }
 void tdlbo_get_nu(void* h, double* out) { DISPATCH(h, COPY_OUT(LAT32(h), Nu, LAT32(h)->size, out), COPY_OUT(LAT64(h), Nu, LAT64(h)->size, out)); }
 void tdlbo_set_nu_field(void* h, const double* in) { DISPATCH(h, COPY_IN(LAT32(h), Nu, LAT32(h)->size, in, float), COPY_IN(LAT64(h), Nu, LAT64(h)->size, in, double)); }
+/* The spread sums (sum of w*(j + F/2) minus rho_sum*u, 3 per marker) of the
+ * last forcing() call, in marker order. */
+void tdlbo_get_forcing_sums(void* h, double* out, long n) {
+    DISPATCH(h, memcpy(out, LAT32(h)->sums, sizeof(double) * 3 * (size_t)n), memcpy(out, LAT64(h)->sums, sizeof(double) * 3 * (size_t)n));
+}
+
 void tdlbo_get_o(void* h, uint8_t* out) {
     DISPATCH(h, memcpy(out, LAT32(h)->Olast, LAT32(h)->size), memcpy(out, LAT64(h)->Olast, LAT64(h)->size));
 }

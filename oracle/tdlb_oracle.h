@@ -63,6 +63,7 @@ void tdlbo_set_nu_field(void* h, const double* in);
 void tdlbo_get_o(void* h, uint8_t* out);
 void tdlbo_get_moments(void* h, double* out);
 void tdlbo_transport(void* h);
+void tdlbo_get_forcing_sums(void* h, double* out, long n);
 
 /* Integer-coded transport known-answer tests, same contract as the
  * tdlbref_kat_* entry points of oracle/_ref. Values are exact in uint64. */

@@ -59,7 +59,7 @@ struct tdlb_lattice {
     bool holds_moments = true;   // state is in moment form (after initialise)
     bool even = true;            // Esotwist parity (ComputeUnit.hpp:116)
     int pass = 0;                // forcing passes so far; mask[pass & 1] is current
-    int vec = 4;                 // cells per thread of the step kernels
+    int vec = 4;                 // cells per thread of the step kernels (set per scheme in build())
     bool initialised = false;
 
     // markers: the resident list and its two-segment schedule
@@ -164,6 +164,10 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
     try {
         h->cfg = c;
         h->device = device;
+        // measured on B200 at 400^3: Simple is fastest with one cell per
+        // thread (direct loads), Esotwist with four (float4 + shuffles)
+        h->vec = c.streaming == TDLB_STREAMING_SIMPLE ? 1 : 4;
+        h->err.reserve(512);
         TDLB_CK(cudaSetDevice(device));
         TDLB_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         Dims& g = h->g;

@@ -318,3 +318,64 @@ def test_marker_positions_bit_exact_on_device(gpu):
             want[(mk["i"] + i1) % e, mk["j"], (mk["k"] + k1) % e] = 1
     np.testing.assert_array_equal(cu.read_touched(), want)
     cu.close()
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_impeller_load_matches_oracle(gpu, port_oracle, streaming):
+    """FP64 force and torque on the attached impeller (rotating-non-updating +
+    rotating markers) against the oracle's per-marker spread sums."""
+    tb, po = gpu, port_oracle
+    e = 40
+    rt = tb.RushtonTurbine(e, e, e, tip_speed=0.1)
+    d = rt.increment(1)
+    nu = tb.nu_from_reynolds(7300.0, 0.1, rt.blade_outer_radius())
+    cu = tb.ComputeUnit(x=e, y=e, z=e, nu=nu, cs0=0.1, useLES=1,
+                        streaming=tb.STREAMING_SIMPLE if streaming == "Simple" else tb.STREAMING_ESOTWIST)
+    lat = po.CpuLattice("port", e, e, e, po.Flow(nu=nu, useLES=True), streaming, 4)
+    cu.attach_rushton(rt, d, 0.0, d)
+    mk = cu.read_markers()
+    n_fixed = len(rt.fixed())
+    cu.initialise(1.0)
+    lat.initialise(1.0)
+    angle = 0.0
+    cu.forcing_resident(ALPHA, BETA)
+    lat.forcing(mk, ALPHA, BETA)
+    for _ in range(3):
+        angle += d
+        cu.rotate_impeller(angle, d)
+        mk = cu.read_markers()
+        cu.collision()
+        cu.forcing_resident(ALPHA, BETA)
+        lat.step(mk, ALPHA, BETA)
+    load = cu.impeller_load()
+    sums = lat.get_forcing_sums(len(mk))[n_fixed:]
+    imp = mk[n_fixed:]
+    ci = ck = (e - 1) / 2.0
+    di = imp["i"] + imp["iCartFraction"].astype(np.float64) - ci
+    dk = imp["k"] + imp["kCartFraction"].astype(np.float64) - ck
+    f = -BETA * sums
+    want = np.array([f[:, 0].sum(), f[:, 1].sum(), f[:, 2].sum(), (dk * f[:, 0] - di * f[:, 2]).sum(), len(imp)])
+    assert load[4] == len(imp)
+    scale = np.abs(f).sum()
+    np.testing.assert_allclose(load[:3], want[:3], rtol=0, atol=2e-5 * scale)
+    torque_scale = (np.abs(dk * f[:, 0]) + np.abs(di * f[:, 2])).sum()
+    assert abs(load[3] - want[3]) <= 2e-5 * torque_scale
+    cu.close()
+
+
+def test_device_rotation_matches_host_generator(gpu):
+    """Blade markers moved on the device are bit-identical to the host
+    generator's markers at the same angle."""
+    tb = gpu
+    e = 48
+    rt = tb.RushtonTurbine(e, e, e, tip_speed=0.1)
+    d = rt.increment(1)
+    cu = tb.ComputeUnit(x=e, y=e, z=e, nu=1e-3)
+    cu.attach_rushton(rt, d, 0.0, d)
+    n_rot = len(rt.rotating(0.0, d))
+    for angle in (0.0, 0.1234, 1.0, 2.5, 6.1):
+        cu.rotate_impeller(angle, d)
+        dev = cu.read_markers()[-n_rot:]
+        host = rt.rotating(angle, d)
+        np.testing.assert_array_equal(dev.view(np.uint8), host.view(np.uint8))
+    cu.close()
