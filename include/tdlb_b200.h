@@ -220,6 +220,18 @@ int tdlb_set_rotating_markers(tdlb_handle h, const tdlb_marker* markers, size_t 
  * summed. A project-defined diagnostic: the reference computes none. */
 int tdlb_impeller_load(tdlb_handle h, double* out5);
 
+/* The same FP64 impeller load for callers that may not allocate device
+ * memory while they run (inside CUDA graph capture, under their own memory
+ * pool, or in a loop that must not allocate): it calls no cudaMalloc,
+ * cudaFree or other allocating routine, and writes the 5 doubles to the
+ * caller's DEVICE buffer d_out5 on h's stream (nothing is synchronised).
+ * No counterpart in the reference. Its scratch is a fixed 40 KiB array
+ * compiled into the library, so lists of more than 1,048,576 markers are
+ * rejected (TDLB_EINVAL). The first call on each device looks that array up
+ * (cudaGetSymbolAddress): make it before any stream capture. All calls on a
+ * device share the array; calls that overlap on the GPU race. */
+int tdlb_impeller_load_noalloc(tdlb_handle h, double* d_out5);
+
 /* Copy of the resident marker list as the device holds it (list order). */
 int tdlb_read_markers(tdlb_handle h, tdlb_marker* out, size_t cap, size_t* n);
 

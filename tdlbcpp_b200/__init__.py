@@ -140,6 +140,7 @@ def load_library() -> ctypes.CDLL:
         "tdlb_read_markers": (i32, [H, vp, sz, ctypes.POINTER(sz)]),
         "tdlb_set_rotating_markers": (i32, [H, vp, sz]),
         "tdlb_impeller_load": (i32, [H, vp]),
+        "tdlb_impeller_load_noalloc": (i32, [H, vp]),
         "tdlb_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "tdlb_set_cells_per_thread": (i32, [H, i32]),
     }
@@ -289,6 +290,11 @@ class ComputeUnit:
     def set_cells_per_thread(self, v: int):
         """Step-kernel variant (1, 2 or 4 cells per thread); results are identical."""
         self._check(self.lib.tdlb_set_cells_per_thread(self.h, v))
+
+    def impeller_load_noalloc(self, device_ptr: int):
+        """Allocation-free impeller load into a caller-owned device buffer of
+        5 doubles (queued on this unit's stream; not synchronised)."""
+        self._check(self.lib.tdlb_impeller_load_noalloc(self.h, ctypes.c_void_p(device_ptr)))
 
     @property
     def stream(self) -> int:

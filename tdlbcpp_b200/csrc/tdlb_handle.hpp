@@ -1,0 +1,88 @@
+// The handle behind tdlb_handle (include/tdlb_b200.h): one lattice on one
+// GPU with its device buffers, resident markers and state bookkeeping.
+// Shared by the C-ABI translation units.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "tdlb_b200.h"
+#include "tdlb_kernels.cuh"
+#include "tdlb_runtime.hpp"
+
+using tdlb::Dims;
+using tdlb::Planes;
+
+struct tdlb_lattice {
+    tdlb_config cfg{};
+    Dims g{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    tdlb::CollideParams cp{};
+
+    float* bufA = nullptr;       // 18 planes
+    float* bufB = nullptr;       // 18 planes (Simple only)
+    float* Nu = nullptr;
+    float* F = nullptr;          // 3 planes: Fx, Fy, Fz
+    uint32_t* mask = nullptr;    // 2 x (rows * kw) words
+    long long mask_words = 0;
+
+    // state
+    int cur = 0;                 // Simple: which buffer holds the state (0 A, 1 B)
+    bool holds_moments = true;   // state is in moment form (after initialise)
+    bool even = true;            // Esotwist parity (ComputeUnit.hpp:116)
+    int pass = 0;                // forcing passes so far; mask[pass & 1] is current
+    int vec = 4;                 // cells per thread of the step kernels (set per scheme in build())
+    bool initialised = false;
+
+    // markers: the resident list and its two-segment schedule
+    tdlb::Marker* d_markers = nullptr;
+    int* d_sched = nullptr;
+    int* d_level_ptr = nullptr;
+    int* d_plane_lv0 = nullptr;
+    int* d_plane_lv1 = nullptr;
+    // first-segment cell lists and per-pass IBM buffers
+    tdlb::CellList cells;
+    int* d_cell_e = nullptr;
+    int* d_plane_cell = nullptr;
+    float* d_prep = nullptr;      // PF_COUNT * n0
+    float* d_cell_m = nullptr;    // 4 * C0
+    float* d_cell_F = nullptr;    // 3 * C0
+    float* d_tail = nullptr;      // TF_COUNT * tail_cap
+    long long tail_cap = 0;
+    float* d_sums = nullptr;      // 3 * marker_cap
+    int smem_cells = 0;
+    long long marker_cap = 0;
+    long long level_cap = 0;
+    int n_markers = 0;      // list length
+    int n0 = 0;             // markers of the first segment (the rest rotate)
+    std::vector<tdlb_marker> h_markers;   // host copy of the resident list
+    tdlb::MarkerSchedule seg0, seg1;
+    bool markers_set = false;
+    float last_beta = 0.f;        // beta of the last forcing pass (for the load)
+    // resident impeller: markers [n0, n_markers) are blades
+    double* d_rot_xz = nullptr;   // their impeller-frame offsets (device rotation)
+    bool rot_device = false;
+    double rot_ci = 0, rot_ck = 0;
+    int impeller_begin = -1;      // first marker of the impeller (-1: none)
+    double* d_load = nullptr;     // kLoadBlocks*5 partials + 5 results
+    tdlb_marker* h_stage = nullptr;   // pinned staging of the blade upload
+    size_t stage_cap = 0;
+
+    std::string err = "no error";
+
+    Planes planes(float* base) const {
+        Planes p;
+        for (int d = 0; d < tdlb::NQ; d++) p.p[d] = base + (size_t)d * (size_t)g.plane;
+        return p;
+    }
+    float* state_buf() const { return cfg.streaming == TDLB_STREAMING_SIMPLE && cur == 1 ? bufB : bufA; }
+    float* other_buf() const { return cur == 1 ? bufA : bufB; }
+    uint32_t* mask_cur() const { return mask + (size_t)(pass & 1) * mask_words; }
+    uint32_t* mask_next() const { return mask + (size_t)((pass + 1) & 1) * mask_words; }
+    int state_mode() const {
+        if (cfg.streaming == TDLB_STREAMING_SIMPLE) return holds_moments ? 1 : 0;
+        return holds_moments ? 3 : 2;
+    }
+};
+
