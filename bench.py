@@ -238,6 +238,154 @@ def run_ours(args, rank, world, device):
     return result
 
 
+# ---------------------------------------------------------------- batched form
+
+BATCH_EDGES = (32, 48, 64, 96, 128)
+BATCH_SEED = 20261203
+BATCH_TANKS = 64
+
+
+def draw_batched_tanks(n=BATCH_TANKS, seed=BATCH_SEED):
+    """Tank list of the batched workload: per tank, in this order, the edge
+    uniform over BATCH_EDGES, tip speed U[0.05, 0.12], Re log-uniform on
+    [1e3, 2e4], all from numpy's default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        edge = int(rng.choice(BATCH_EDGES))
+        tip = float(rng.uniform(0.05, 0.12))
+        re = float(np.exp(rng.uniform(np.log(1e3), np.log(2e4))))
+        out.append((edge, tip, re))
+    return out
+
+
+def batched_configs(tb, tanks, storage="fp32"):
+    rts, cfgs = [], []
+    for edge, tip, re in tanks:
+        rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=tip, startup_steps=0)
+        nu = tb.nu_from_reynolds(re, tip, rt.blade_outer_radius())
+        rts.append(rt)
+        cfgs.append(dict(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0,
+                         streaming="Simple", storage=storage))
+    return rts, cfgs
+
+
+def prepare_tank(cu, rt):
+    d = rt.increment(1)
+    cu.attach_rushton(rt, d, d, d)
+    cu.initialise(1.0)
+    cu.forcing_resident(ALPHA, BETA)          # main.cpp:305
+
+
+def run_batched(args, rank, world, device):
+    """The batched form: 64 tanks in one batch, timed over K batched steps;
+    beside it the same tanks stepped one after another in the plain form."""
+    import torch
+    import tdlbcpp_b200 as tb
+
+    torch.cuda.set_device(device)
+    tanks = draw_batched_tanks()
+    rts, cfgs = batched_configs(tb, tanks)
+    cells = sum(e ** 3 for e, _, _ in tanks)
+    b = tb.Batch(cfgs, device=device)
+    stream = torch.cuda.ExternalStream(b.stream(), device=device)
+    for cu, rt in zip(b.tanks, rts):
+        prepare_tank(cu, rt)
+    b.run(4, ALPHA, BETA)
+    fused_ms = b.autotune(trials=5)
+    shape = b.shape()
+    for cu, rt in zip(b.tanks, rts):              # autotuning changed the fields
+        prepare_tank(cu, rt)
+    b.run(args.warmup, ALPHA, BETA)
+    b.synchronize()
+
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.kernel_launches()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clk:
+        t0.record(stream)
+        b.run(args.steps, ALPHA, BETA)
+        t1.record(stream)
+        b.synchronize()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(t0.elapsed_time(t1), world)
+    launches = b.kernel_launches() - l0
+
+    # fused batched launch alone, timed on the batch stream after the run
+    fused = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run(1, ALPHA, BETA)
+        e1.record(stream)
+        b.synchronize()
+        fused.append(e0.elapsed_time(e1))
+
+    # e2e: public API with host buffers -- chunks of 10 steps, then every
+    # tank's FP64 impeller load read back to pinned host memory
+    chunk = 10
+    n_chunks = max(1, args.steps // (5 * chunk))
+    load = np.zeros((len(tanks), 5))
+    b.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(n_chunks):
+        b.run(chunk, ALPHA, BETA)
+        for t, cu in enumerate(b.tanks):
+            cu.impeller_load(load[t])
+    b.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - w0, world)
+    b.close()
+
+    # the same tanks in the plain form, one after another
+    seq_ms = 0.0
+    k_seq = max(5, min(20, args.steps // 10))
+    for (edge, tip, re), rt, cfg in zip(tanks, rts, cfgs):
+        cu = tb.ComputeUnit(device=device, **cfg)
+        prepare_tank(cu, rt)
+        st = torch.cuda.ExternalStream(cu.stream, device=device)
+        angle, s = rt.increment(1), 1
+
+        def plain_step():
+            nonlocal angle, s
+            s += 1
+            d = rt.increment(s)
+            angle += d
+            cu.rotate_impeller(angle, d)
+            cu.collision()
+            cu.forcing_resident(ALPHA, BETA)
+
+        for _ in range(3):
+            plain_step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        cu.synchronize()
+        e0.record(st)
+        for _ in range(k_seq):
+            plain_step()
+        e1.record(st)
+        cu.synchronize()
+        seq_ms += e0.elapsed_time(e1) / k_seq
+        cu.close()
+
+    return {
+        "value_mlups": world * cells * args.steps / (ms / 1e3) / 1e6,
+        "ms_per_step": ms / args.steps,
+        "kernel_ms": fused_ms,
+        "step_ms_single": statistics.median(fused),
+        "e2e_mlups": world * cells * chunk * n_chunks / e2e_s / 1e6,
+        "e2e_steps": chunk * n_chunks,
+        "d2h": len(tanks) * 5 * 8 / chunk,
+        "seq_mlups": world * cells / (seq_ms / 1e3) / 1e6,
+        "seq_steps": k_seq,
+        "cells": cells,
+        "shape": shape,
+        "launches": launches,
+        "clocks": clk.summary(),
+        "tanks": len(tanks),
+    }
+
+
 # ---------------------------------------------------------------- reference arm
 
 def slab_markers(tb, rt, j0, height, angle, dth):
@@ -335,22 +483,62 @@ def max_over_ranks(x, world):
     return float(x)
 
 
+def report_batched(args, rank, world, local, config):
+    res = run_batched(args, rank, world, local)
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peak()
+    bpc = 152
+    achieved = bpc * res["cells"] / (res["kernel_ms"] / 1e3) / 1e9
+    v, nt, bps = res["shape"]
+    config = dict(config, shape={"cells_per_thread": v, "threads": nt, "blocks_per_sm": bps},
+                  sequential_plain_mlups=res["seq_mlups"], sequential_steps_per_tank=res["seq_steps"],
+                  single_step_ms=res["step_ms_single"])
+    line = {
+        "metric": "MLUPS", "value": res["value_mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": config,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "kernel": "k_batch_step", "bytes_per_cell": bpc,
+                     "kernel_ms": res["kernel_ms"], "traffic": None},
+        "e2e": {"value": res["e2e_mlups"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": res["d2h"], "steps": res["e2e_steps"]},
+        "gpu_launches": res["launches"],
+        "clocks": res["clocks"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        r = reference_sample(1, 0, host_threads())
+        line["cpu_baseline"] = {"value": r["value"], "unit": "MLUPS", "cores": r["cores"], "kind": "reference",
+                                "sample": r["sample"] + " (per-cell rate of the same step)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["simple", "esotwist"], default="simple")
+    ap.add_argument("--workload", choices=["simple", "esotwist", "batched"], default="simple")
     ap.add_argument("--edge", type=int, default=EDGE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3   # timing rule: at least 3 warm-up steps
-    workload = f"rushton-{args.edge}^3-{args.workload}-fp32-les"
-    config = {"workload": workload, "grid": [args.edge] * 3, "streaming": args.workload.capitalize(),
-              "collision": "EgglesSomers+LES(cs0=0.1)", "re": RE, "tip_speed": TIP, "ibm": "Rushton turbine, rotating",
-              "l2": "lattice > L2 every step (no flush needed)"}
+    if args.workload == "batched":
+        tanks = draw_batched_tanks()
+        workload = f"batched-{len(tanks)}-tanks-simple-fp32-les"
+        config = {"workload": workload, "tanks": len(tanks), "edges": [t[0] for t in tanks],
+                  "cells": sum(t[0] ** 3 for t in tanks), "seed": BATCH_SEED,
+                  "draw": "edge U{32,48,64,96,128}, tip U[0.05,0.12], Re log-U[1e3,2e4] per tank, in that order",
+                  "streaming": "Simple", "collision": "EgglesSomers+LES(cs0=0.1)", "ibm": "Rushton turbine, rotating",
+                  "l2": "lattices > L2 every step (no flush needed)"}
+    else:
+        workload = f"rushton-{args.edge}^3-{args.workload}-fp32-les"
+        config = {"workload": workload, "grid": [args.edge] * 3, "streaming": args.workload.capitalize(),
+                  "collision": "EgglesSomers+LES(cs0=0.1)", "re": RE, "tip_speed": TIP,
+                  "ibm": "Rushton turbine, rotating", "l2": "lattice > L2 every step (no flush needed)"}
 
     rank, world, local = init_dist(args)
 
@@ -369,6 +557,9 @@ def main():
                 "e2e": {"value": r["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
+
+    if args.workload == "batched":
+        return report_batched(args, rank, world, local, config)
 
     res = run_ours(args, rank, world, local)
     if rank != 0:

@@ -42,8 +42,12 @@ extern "C" {
 #define TDLB_STREAMING_SIMPLE 0
 #define TDLB_STREAMING_ESOTWIST 1
 
-/* population storage precision */
+/* population storage precision: FP32 populations, or 16-bit deviations
+ * f_i - w_i*rho0 from the rest weights (w = 1/12 faces, 1/24 edges;
+ * rho0 = initialRho) with all arithmetic in FP32 */
 #define TDLB_STORAGE_FP32 0
+#define TDLB_STORAGE_FP16 1
+#define TDLB_STORAGE_BF16 2
 
 typedef struct tdlb_lattice* tdlb_handle;
 
@@ -151,6 +155,11 @@ int tdlb_read_touched(tdlb_handle h, uint8_t* flags);
 int tdlb_get_dims(tdlb_handle h, int64_t* x, int64_t* y, int64_t* z);
 int tdlb_get_even_step(tdlb_handle h, int* even);
 
+/* FP64 sums over all interior cells (a project-defined diagnostic; the
+ * reference has none): out[0] = mass (sum of rho), out[1..3] = momentum
+ * (sum of j + F/2). Deterministic: fixed launch shape and summation order. */
+int tdlb_reduce_fp64(tdlb_handle h, double* out4);
+
 /* Make all queued device work complete. */
 int tdlb_synchronize(tdlb_handle h);
 
@@ -240,6 +249,44 @@ int tdlb_read_markers(tdlb_handle h, tdlb_marker* out, size_t cap, size_t* n);
  * of levels in one plane. Markers of one level share no stencil cell. */
 int tdlb_schedule_levels(const tdlb_marker* markers, size_t n, int64_t x, int64_t y, int64_t z,
                          int32_t* level_out, int32_t* max_levels_per_plane);
+
+/* ---- batched form: many independent tanks on one GPU ----
+ * No counterpart in the reference (it runs one lattice per process,
+ * main.cpp:336-454). A batch owns its tanks; every tank is an ordinary
+ * handle (tdlb_batch_tank) for initialise, attach_rushton, set_markers and
+ * the read functions, and all tanks share the batch's stream. All tanks of a
+ * batch use one streaming scheme and one storage precision; sizes, nu, LES
+ * and markers differ freely. */
+typedef struct tdlb_batch_s* tdlb_batch;
+
+int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* out);
+int tdlb_batch_destroy(tdlb_batch b);
+/* Last error of b; of the calling thread's last failed create if b is NULL. */
+const char* tdlb_batch_last_error(tdlb_batch b);
+int tdlb_batch_size(tdlb_batch b, int* n);
+int tdlb_batch_tank(tdlb_batch b, int t, tdlb_handle* out);
+/* Shape of the fused batched launch: cells per thread (1, 2, 4; 16-bit
+ * storage 1 or 4), threads per block (128 or 256), resident blocks per SM
+ * (1..16; the grid is min(work items, SMs x blocks_per_sm)). */
+int tdlb_batch_set_shape(tdlb_batch b, int cells_per_thread, int threads, int blocks_per_sm);
+int tdlb_batch_get_shape(tdlb_batch b, int* cells_per_thread, int* threads, int* blocks_per_sm);
+/* Times every shape on the initialised batch and keeps the fastest
+ * (best_ms: its fused-launch time, may be NULL). The timed launches change
+ * the fields: initialise the tanks again afterwards. */
+int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms);
+/* `steps` time steps of every tank, the reference's main-loop step each
+ * (main.cpp:409-454): impeller rotation (tanks with tdlb_attach_rushton, the
+ * angle advanced by tdlb_rushton_impeller_increment of the step), fused
+ * collision + streaming, immersed-boundary forcing (tanks with markers) with
+ * alpha, beta. Pairs of steps replay one captured CUDA graph. */
+int tdlb_batch_run(tdlb_batch b, int steps, float alpha, float beta);
+/* Same steps, every launch issued eagerly (no graph). */
+int tdlb_batch_run_eager(tdlb_batch b, int steps, float alpha, float beta);
+/* Kernels the batch's runs have launched since it was created (graph
+ * replays counted per kernel node). */
+int tdlb_batch_kernel_launches(tdlb_batch b, long long* n);
+int tdlb_batch_synchronize(tdlb_batch b);
+int tdlb_batch_get_stream(tdlb_batch b, void** stream);
 
 /* ---- known-answer-test support (integer-coded transport) ----
  * Raw population state: for Simple the current buffer, for Esotwist the

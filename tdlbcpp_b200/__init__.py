@@ -19,7 +19,7 @@ from typing import Optional
 import numpy as np
 
 __all__ = [
-    "ComputeUnit", "TdlbError", "MARKER_DTYPE", "library_path", "load_library",
+    "ComputeUnit", "Batch", "TdlbError", "MARKER_DTYPE", "library_path", "load_library", "make_config",
     "STREAMING_SIMPLE", "STREAMING_ESOTWIST",
 ]
 
@@ -29,6 +29,9 @@ _LIB_NAME = "libtdlb_b200.so"
 
 STREAMING_SIMPLE = 0
 STREAMING_ESOTWIST = 1
+STORAGE_FP32 = 0
+STORAGE_FP16 = 1
+STORAGE_BF16 = 2
 
 # Lattice vectors of population slots Q01..Q18 (tdlbcpp/src/Header.h:70-100);
 # opposite(d) = d ^ 1.
@@ -84,6 +87,23 @@ class Rushton(ctypes.Structure):
         ("baffle_width", ctypes.c_double), ("wall_inset", ctypes.c_double), ("tip_speed", ctypes.c_double),
         ("startup_steps", ctypes.c_int64),
     ]
+
+
+def make_config(**fields) -> Config:
+    """A tdlb_config from keyword fields. Unnamed fields: cs0 0.12, g3 0.8,
+    alpha 0.97, beta 1.9, useLES off (the reference's FlowParams defaults,
+    FlowParams.hpp:32-59) and initialRho 1 (the reference's is 8). ``streaming``
+    may be "Simple" or "Esotwist", ``storage`` "fp32", "fp16" or "bf16"."""
+    cfg = Config()
+    cfg.streaming = STREAMING_SIMPLE
+    cfg.initialRho, cfg.cs0, cfg.g3, cfg.alpha, cfg.beta, cfg.useLES = 1.0, 0.12, 0.8, 0.97, 1.9, 0
+    for key, val in fields.items():
+        if key == "streaming" and isinstance(val, str):
+            val = STREAMING_SIMPLE if val == "Simple" else STREAMING_ESOTWIST
+        if key == "storage" and isinstance(val, str):
+            val = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16}[val.lower()]
+        setattr(cfg, key, val)
+    return cfg
 
 
 def library_path() -> str:
@@ -143,6 +163,20 @@ def load_library() -> ctypes.CDLL:
         "tdlb_impeller_load_noalloc": (i32, [H, vp]),
         "tdlb_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "tdlb_set_cells_per_thread": (i32, [H, i32]),
+        "tdlb_reduce_fp64": (i32, [H, vp]),
+        "tdlb_batch_create": (i32, [ctypes.POINTER(Config), i32, i32, ctypes.POINTER(H)]),
+        "tdlb_batch_destroy": (i32, [H]),
+        "tdlb_batch_last_error": (ctypes.c_char_p, [H]),
+        "tdlb_batch_size": (i32, [H, ctypes.POINTER(i32)]),
+        "tdlb_batch_tank": (i32, [H, i32, ctypes.POINTER(H)]),
+        "tdlb_batch_set_shape": (i32, [H, i32, i32, i32]),
+        "tdlb_batch_get_shape": (i32, [H, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+        "tdlb_batch_autotune": (i32, [H, i32, ctypes.POINTER(ctypes.c_double)]),
+        "tdlb_batch_run": (i32, [H, i32, f32, f32]),
+        "tdlb_batch_run_eager": (i32, [H, i32, f32, f32]),
+        "tdlb_batch_synchronize": (i32, [H]),
+        "tdlb_batch_kernel_launches": (i32, [H, ctypes.POINTER(ctypes.c_longlong)]),
+        "tdlb_batch_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -189,17 +223,22 @@ class ComputeUnit:
                     text = f.read()
             rc = self.lib.tdlb_create(text.encode(), device, ctypes.byref(h))
         else:
-            cfg = Config()
-            cfg.streaming = STREAMING_SIMPLE
-            cfg.initialRho, cfg.cs0, cfg.g3, cfg.alpha, cfg.beta, cfg.useLES = 1.0, 0.12, 0.8, 0.97, 1.9, 0
-            for key, val in config.items():
-                if key == "streaming" and isinstance(val, str):
-                    val = STREAMING_SIMPLE if val == "Simple" else STREAMING_ESOTWIST
-                setattr(cfg, key, val)
-            rc = self.lib.tdlb_create_config(ctypes.byref(cfg), device, ctypes.byref(h))
+            rc = self.lib.tdlb_create_config(ctypes.byref(make_config(**config)), device, ctypes.byref(h))
         if rc != 0:
             raise TdlbError(rc, self.lib.tdlb_last_error(None).decode())
+        self._attach(h, owned=True)
+
+    @classmethod
+    def _borrowed(cls, lib: ctypes.CDLL, h: ctypes.c_void_p) -> "ComputeUnit":
+        """A view of a tank that a Batch owns (closing it does nothing)."""
+        cu = cls.__new__(cls)
+        cu.lib = lib
+        cu._attach(h, owned=False)
+        return cu
+
+    def _attach(self, h: ctypes.c_void_p, owned: bool):
         self.h = h
+        self._owned = owned
         x, y, z = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         self._check(self.lib.tdlb_get_dims(self.h, ctypes.byref(x), ctypes.byref(y), ctypes.byref(z)))
         self.x, self.y, self.z = x.value, y.value, z.value
@@ -211,7 +250,8 @@ class ComputeUnit:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.tdlb_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.lib.tdlb_destroy(self.h)
             self.h = None
 
     def __enter__(self):
@@ -287,6 +327,12 @@ class ComputeUnit:
         self._check(self.lib.tdlb_impeller_load(self.h, _p(out)))
         return out
 
+    def reduce_fp64(self) -> np.ndarray:
+        """FP64 (mass, momentum x, y, z) over all interior cells."""
+        out = np.zeros(4, np.float64)
+        self._check(self.lib.tdlb_reduce_fp64(self.h, _p(out)))
+        return out
+
     def set_cells_per_thread(self, v: int):
         """Step-kernel variant (1, 2 or 4 cells per thread); results are identical."""
         self._check(self.lib.tdlb_set_cells_per_thread(self.h, v))
@@ -354,6 +400,95 @@ class ComputeUnit:
 # Rushton-turbine geometry (host only), mirroring the calls main.cpp makes on
 # RushtonTurbinePolarCPP (main.cpp:274-303, :409-426).
 # ---------------------------------------------------------------------------
+class Batch:
+    """Many independent tanks on one GPU (``tdlb_batch_*``): one persistent
+    fused launch steps every tank, then each tank's immersed-boundary pass;
+    pairs of steps replay a captured CUDA graph.
+
+    ``configs`` is a list of ``make_config`` keyword dicts (or Config
+    structs), one per tank; all share one streaming scheme and one storage
+    precision. ``tanks[t]`` is a ComputeUnit view of tank t for initialise,
+    attach_rushton, set_markers and the read functions.
+    """
+
+    def __init__(self, configs, device: int = 0):
+        self.lib = load_library()
+        n = len(configs)
+        arr = (Config * n)()
+        for t, c in enumerate(configs):
+            arr[t] = c if isinstance(c, Config) else make_config(**c)
+        h = ctypes.c_void_p()
+        rc = self.lib.tdlb_batch_create(arr, n, device, ctypes.byref(h))
+        if rc != 0:
+            raise TdlbError(rc, self.lib.tdlb_batch_last_error(None).decode())
+        self.h = h
+        self.tanks = []
+        for t in range(n):
+            th = ctypes.c_void_p()
+            self._check(self.lib.tdlb_batch_tank(self.h, t, ctypes.byref(th)))
+            self.tanks.append(ComputeUnit._borrowed(self.lib, th))
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise TdlbError(rc, self.lib.tdlb_batch_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            for cu in self.tanks:
+                cu.h = None
+            self.lib.tdlb_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        return len(self.tanks)
+
+    @property
+    def ncell(self) -> int:
+        return sum(cu.ncell for cu in self.tanks)
+
+    def set_shape(self, cells_per_thread: int, threads: int, blocks_per_sm: int):
+        self._check(self.lib.tdlb_batch_set_shape(self.h, cells_per_thread, threads, blocks_per_sm))
+
+    def shape(self):
+        v, t, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.tdlb_batch_get_shape(self.h, ctypes.byref(v), ctypes.byref(t), ctypes.byref(b)))
+        return v.value, t.value, b.value
+
+    def autotune(self, trials: int = 3) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.tdlb_batch_autotune(self.h, trials, ctypes.byref(ms)))
+        return ms.value
+
+    def run(self, steps: int, alpha: float, beta: float, graph: bool = True):
+        fn = self.lib.tdlb_batch_run if graph else self.lib.tdlb_batch_run_eager
+        self._check(fn(self.h, steps, alpha, beta))
+
+    def synchronize(self):
+        self._check(self.lib.tdlb_batch_synchronize(self.h))
+
+    def kernel_launches(self) -> int:
+        n = ctypes.c_longlong()
+        self._check(self.lib.tdlb_batch_kernel_launches(self.h, ctypes.byref(n)))
+        return n.value
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.tdlb_batch_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+
 class RushtonTurbine:
     """Marker lists of the project's stirred-tank geometry for an x*y*z lattice."""
 

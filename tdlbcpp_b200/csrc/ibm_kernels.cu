@@ -46,13 +46,20 @@ __device__ __forceinline__ float calc_weight(float x) {
 
 __device__ __forceinline__ int wrap_i(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
 
+template <typename S>
+__device__ __forceinline__ float ld_state(const float* plane, long long e) {
+    if constexpr (sizeof(S) == 4) return plane[e];
+    else return Storage<S>::dec(reinterpret_cast<const S*>(plane)[e]);
+}
+
 // rho and momentum of the state at interior cell (i, j, k).
+template <typename S>
 __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int even, const Dims& g, int i, int j, int k,
-                                              float* m4) {
+                                              const CollideParams& p, float* m4) {
     if (mode == 1) {
         const long long e = ((long long)i * g.ny + j) * g.kp + k;
 #pragma unroll
-        for (int s = 0; s < 4; s++) m4[s] = A.p[s][e];
+        for (int s = 0; s < 4; s++) m4[s] = ld_state<S>(A.p[s], e);
         return;
     }
     float q[NQ];
@@ -62,7 +69,7 @@ __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int eve
             const int si = i - cx_of(d), sj = j - cy_of(d), sk = k - cz_of(d);
             const bool in = (unsigned)si < (unsigned)g.nx && (unsigned)sj < (unsigned)g.ny && (unsigned)sk < (unsigned)g.nz;
             const long long src = in ? ((long long)si * g.ny + sj) * g.kp + sk : ((long long)i * g.ny + j) * g.kp + k;
-            q[d] = A.p[d][src];
+            q[d] = ld_state<S>(A.p[d], src) + (Storage<S>::deviation ? (is_face(d) ? p.wface : p.wedge) : 0.f);
         }
         moments4_of(q, m4);
         return;
@@ -75,7 +82,8 @@ __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int eve
         const int s = even ? d : (d ^ 1);
         const int sg = even ? -1 : 1;
         const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
-        q[d] = A.p[s][((long long)(oi ? i1 : i) * g.ny + (oj ? j1 : j)) * g.kp + (ok ? k1 : k)];
+        q[d] = ld_state<S>(A.p[s], ((long long)(oi ? i1 : i) * g.ny + (oj ? j1 : j)) * g.kp + (ok ? k1 : k)) +
+               (mode == 2 && Storage<S>::deviation ? (is_face(d) ? p.wface : p.wedge) : 0.f);
     }
     if (mode == 3) {
 #pragma unroll
@@ -107,6 +115,7 @@ __global__ void k_ibm_prepare(IbmArgs a, float* __restrict__ prep) {
 // segment (cells sorted by row, so neighbouring threads pull neighbouring
 // cells), and the F each cell starts the pass with (zero unless the previous
 // pass touched it, Forcing.hpp:162-174).
+template <typename S>
 __global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.ncell) return;
@@ -117,7 +126,7 @@ __global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a) {
     const int i = row / g.ny;
     const int j = row - i * g.ny;
     float m4[4];
-    cell_moments4(a.A, a.state_mode, a.even, g, i, j, k, m4);
+    cell_moments4<S>(a.A, a.state_mode, a.even, g, i, j, k, a.p, m4);
     const long long C = a.ncell;
 #pragma unroll
     for (int s = 0; s < 4; s++) a.cell_m[s * C + c] = m4[s];
@@ -129,6 +138,7 @@ __global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a) {
 
 // Second segment (the blades): weights and the moments of the 9 stencil
 // cells of every blade marker.
+template <typename S>
 __global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.n - a.n0) return;
@@ -142,7 +152,7 @@ __global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
             const float w = calc_weight(-mk.iCartFraction + (float)i1) * calc_weight(-mk.kCartFraction + (float)k1);
             const int i2 = wrap_i(i + i1, a.g.nx), k2 = wrap_i(k + k1, a.g.nz);
             float m4[4];
-            cell_moments4(a.A, a.state_mode, a.even, a.g, i2, j, k2, m4);
+            cell_moments4<S>(a.A, a.state_mode, a.even, a.g, i2, j, k2, a.p, m4);
             s[(TF_W + c) * cap + t] = w;
             s[(TF_RHO + c) * cap + t] = m4[0];
             s[(TF_MX + c) * cap + t] = m4[1];
@@ -157,34 +167,34 @@ __global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
 }
 
 // One CTA per j-plane: the plane's first-segment levels on an F tile in
-// shared memory, then write-back and flags, then the blade levels on the
-// dense F, then the plane's touched flags.
-__global__ void __launch_bounds__(512) k_ibm_spread(IbmArgs a) {
-    extern __shared__ uint32_t smem[];
+// shared memory (planes with more cells than the tile holds work on cell_F
+// in place), write-back to F, then the blade levels on the dense F. The
+// touched flags of the first segment never change, so each pass starts
+// mask_new as a copy of them (mask_static) and the blade walk adds its cells.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes,
+                                                                       int tile_cells) {
+    extern __shared__ float tile[];                             // [3][tile_cells]
     const Dims g = a.g;
-    const int j = blockIdx.x;
-    const int nwords = g.nx * g.kw;
-    uint32_t* touched = smem;                                   // [nx][kw]
-    float* tile = reinterpret_cast<float*>(smem + nwords);      // [3][smem_cells]
+    const int j = planes[blockIdx.x];
     const int c0 = a.plane_cell[j], nc = a.plane_cell[j + 1] - c0;
     const long long C = a.ncell;
+    const bool in_smem = nc <= tile_cells;
     float *fx, *fy, *fz;
-    if (a.smem_cells > 0) {
-        fx = tile; fy = tile + a.smem_cells; fz = tile + 2 * a.smem_cells;
-    } else {
-        fx = a.cell_F + c0; fy = a.cell_F + C + c0; fz = a.cell_F + 2 * C + c0;
-    }
-    for (int w = threadIdx.x; w < nwords; w += blockDim.x) touched[w] = 0u;
-    if (a.smem_cells > 0)
+    if (in_smem) {
+        fx = tile; fy = tile + tile_cells; fz = tile + 2 * tile_cells;
         for (int t = threadIdx.x; t < nc; t += blockDim.x) {
             fx[t] = a.cell_F[c0 + t];
             fy[t] = a.cell_F[C + c0 + t];
             fz[t] = a.cell_F[2 * C + c0 + t];
         }
+    } else {
+        fx = a.cell_F + c0; fy = a.cell_F + C + c0; fz = a.cell_F + 2 * C + c0;
+    }
     __syncthreads();
 
-    // ---- first segment: F lives in the tile; each marker in list order
-    //      relative to every marker it shares a cell with (level walk)
+    // ---- first segment: each marker in list order relative to every marker
+    //      it shares a cell with (level walk)
     const long long n0 = a.n0;
     const float* rho = a.cell_m + c0;
     const float* mx = a.cell_m + C + c0;
@@ -193,17 +203,15 @@ __global__ void __launch_bounds__(512) k_ibm_spread(IbmArgs a) {
     for (int lv = a.plane_lv0[j]; lv < a.plane_lv0[j + 1]; lv++) {
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
         for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-            float w[9];
-            int li[9];
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                w[c] = a.prep[(PF_W + c) * n0 + p];
-                li[c] = __float_as_int(a.prep[(PF_CELL + c) * n0 + p]);
-                rhoSum = fmaf(w[c], rho[li[c]], rhoSum);
-                xSum = fmaf(w[c], fmaf(0.5f, fx[li[c]], mx[li[c]]), xSum);
-                ySum = fmaf(w[c], fmaf(0.5f, fy[li[c]], my[li[c]]), ySum);
-                zSum = fmaf(w[c], fmaf(0.5f, fz[li[c]], mz[li[c]]), zSum);
+                const float w = a.prep[(PF_W + c) * n0 + p];
+                const int li = __float_as_int(a.prep[(PF_CELL + c) * n0 + p]);
+                rhoSum = fmaf(w, rho[li], rhoSum);
+                xSum = fmaf(w, fmaf(0.5f, fx[li], mx[li]), xSum);
+                ySum = fmaf(w, fmaf(0.5f, fy[li], my[li]), ySum);
+                zSum = fmaf(w, fmaf(0.5f, fz[li], mz[li]), zSum);
             }
             xSum = fmaf(-rhoSum, a.prep[PF_U * n0 + p], xSum);
             ySum = fmaf(-rhoSum, a.prep[PF_V * n0 + p], ySum);
@@ -213,54 +221,51 @@ __global__ void __launch_bounds__(512) k_ibm_spread(IbmArgs a) {
             a.sums[2 * a.n + p] = zSum;
 #pragma unroll
             for (int c = 0; c < 9; c++) {   // sequential: a wrapped stencil sees its own update
-                const float bw = a.beta * w[c];
-                fx[li[c]] = fmaf(a.alpha, fx[li[c]], -bw * xSum);
-                fy[li[c]] = fmaf(a.alpha, fy[li[c]], -bw * ySum);
-                fz[li[c]] = fmaf(a.alpha, fz[li[c]], -bw * zSum);
+                const float bw = a.beta * a.prep[(PF_W + c) * n0 + p];
+                const int li = __float_as_int(a.prep[(PF_CELL + c) * n0 + p]);
+                fx[li] = fmaf(a.alpha, fx[li], -bw * xSum);
+                fy[li] = fmaf(a.alpha, fy[li], -bw * ySum);
+                fz[li] = fmaf(a.alpha, fz[li], -bw * zSum);
             }
         }
         __syncthreads();
     }
-    // ---- write the tile back to F and flag the plane's cells
+    // ---- write the plane's cells back to F
     for (int t = threadIdx.x; t < nc; t += blockDim.x) {
         const int e = a.cell_e[c0 + t];
         a.Fx[e] = fx[t];
         a.Fy[e] = fy[t];
         a.Fz[e] = fz[t];
-        const int row = e / g.kp, k = e - row * g.kp, i = row / g.ny;
-        atomicOr(&touched[i * g.kw + (k >> 5)], 1u << (k & 31));
     }
     __syncthreads();
 
-    // ---- second segment (blades): dense F, touched flags of this pass
+    // ---- second segment (blades): dense F; mask_new holds this pass's
+    //      touched cells (the first segment's, plus blade cells so far)
     const float* s = a.tail;
     const long long cap = a.tail_cap;
     for (int lv = a.plane_lv1[j]; lv < a.plane_lv1[j + 1]; lv++) {
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
         for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
             const int t = p - a.n0;
-            float w[9];
-            long long e[9];
-            int sw[9];
-            uint32_t bit[9];
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                w[c] = s[(TF_W + c) * cap + t];
+                const float w = s[(TF_W + c) * cap + t];
                 const int packed = __float_as_int(s[(TF_CELL + c) * cap + t]);
                 const int i2 = packed >> 16, k2 = packed & 0xffff;
                 const long long row = (long long)i2 * g.ny + j;
-                e[c] = row * g.kp + k2;
-                sw[c] = i2 * g.kw + (k2 >> 5);
-                bit[c] = 1u << (k2 & 31);
-                const bool live = (touched[sw[c]] & bit[c]) || (a.mask_old[row * g.kw + (k2 >> 5)] & bit[c]);
-                const float vx = live ? a.Fx[e[c]] : 0.f;
-                const float vy = live ? a.Fy[e[c]] : 0.f;
-                const float vz = live ? a.Fz[e[c]] : 0.f;
-                rhoSum = fmaf(w[c], s[(TF_RHO + c) * cap + t], rhoSum);
-                xSum = fmaf(w[c], fmaf(0.5f, vx, s[(TF_MX + c) * cap + t]), xSum);
-                ySum = fmaf(w[c], fmaf(0.5f, vy, s[(TF_MY + c) * cap + t]), ySum);
-                zSum = fmaf(w[c], fmaf(0.5f, vz, s[(TF_MZ + c) * cap + t]), zSum);
+                const long long e = row * g.kp + k2;
+                const long long wd = row * g.kw + (k2 >> 5);
+                const uint32_t bit = 1u << (k2 & 31);
+                // L2 reads: flags and F written by this CTA's earlier levels
+                const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
+                const float vx = live ? __ldcg(a.Fx + e) : 0.f;
+                const float vy = live ? __ldcg(a.Fy + e) : 0.f;
+                const float vz = live ? __ldcg(a.Fz + e) : 0.f;
+                rhoSum = fmaf(w, s[(TF_RHO + c) * cap + t], rhoSum);
+                xSum = fmaf(w, fmaf(0.5f, vx, s[(TF_MX + c) * cap + t]), xSum);
+                ySum = fmaf(w, fmaf(0.5f, vy, s[(TF_MY + c) * cap + t]), ySum);
+                zSum = fmaf(w, fmaf(0.5f, vz, s[(TF_MZ + c) * cap + t]), zSum);
             }
             xSum = fmaf(-rhoSum, s[TF_U * cap + t], xSum);
             ySum = fmaf(-rhoSum, s[TF_V * cap + t], ySum);
@@ -270,25 +275,25 @@ __global__ void __launch_bounds__(512) k_ibm_spread(IbmArgs a) {
             a.sums[2 * a.n + p] = zSum;
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                const long long row = e[c] / g.kp;
-                const int k2 = (int)(e[c] - row * g.kp);
-                const bool live = (touched[sw[c]] & bit[c]) || (a.mask_old[row * g.kw + (k2 >> 5)] & bit[c]);
-                const float vx = live ? a.Fx[e[c]] : 0.f;
-                const float vy = live ? a.Fy[e[c]] : 0.f;
-                const float vz = live ? a.Fz[e[c]] : 0.f;
-                const float bw = a.beta * w[c];
-                a.Fx[e[c]] = fmaf(a.alpha, vx, -bw * xSum);
-                a.Fy[e[c]] = fmaf(a.alpha, vy, -bw * ySum);
-                a.Fz[e[c]] = fmaf(a.alpha, vz, -bw * zSum);
-                atomicOr(&touched[sw[c]], bit[c]);
+                const int packed = __float_as_int(s[(TF_CELL + c) * cap + t]);
+                const int i2 = packed >> 16, k2 = packed & 0xffff;
+                const long long row = (long long)i2 * g.ny + j;
+                const long long e = row * g.kp + k2;
+                const long long wd = row * g.kw + (k2 >> 5);
+                const uint32_t bit = 1u << (k2 & 31);
+                // L2 reads: flags and F written by this CTA's earlier levels
+                const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
+                const float vx = live ? __ldcg(a.Fx + e) : 0.f;
+                const float vy = live ? __ldcg(a.Fy + e) : 0.f;
+                const float vz = live ? __ldcg(a.Fz + e) : 0.f;
+                const float bw = a.beta * s[(TF_W + c) * cap + t];
+                a.Fx[e] = fmaf(a.alpha, vx, -bw * xSum);
+                a.Fy[e] = fmaf(a.alpha, vy, -bw * ySum);
+                a.Fz[e] = fmaf(a.alpha, vz, -bw * zSum);
+                atomicOr(&a.mask_new[wd], bit);
             }
         }
         __syncthreads();
-    }
-    // ---- publish this plane's touched flags (planes without markers publish zeros)
-    for (int w = threadIdx.x; w < nwords; w += blockDim.x) {
-        const int i = w / g.kw, wk = w - i * g.kw;
-        a.mask_new[((long long)i * g.ny + j) * g.kw + wk] = touched[w];
     }
 }
 
@@ -364,12 +369,85 @@ cudaError_t launch_marker_load(const IbmArgs& a, int begin, double ci, double ck
     return cudaGetLastError();
 }
 
+// FP64 mass and momentum over all interior cells, deterministic: a fixed
+// grid of kReduceBlocks blocks, a fixed per-thread stride, a fixed tree,
+// then one thread sums the block partials in order.
+template <typename S>
+__global__ void __launch_bounds__(256) k_reduce_fp64(IbmArgs a, const uint32_t* __restrict__ mask, double* partial) {
+    __shared__ double red[4][256];
+    const Dims g = a.g;
+    const long long total = g.rows() * g.nz;
+    double acc[4] = {0, 0, 0, 0};
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % g.nz);
+        const long long row = t / g.nz;
+        const int j = (int)(row % g.ny), i = (int)(row / g.ny);
+        float m4[4];
+        cell_moments4<S>(a.A, a.state_mode, a.even, g, i, j, k, a.p, m4);
+        const long long e = row * g.kp + k;
+        const bool on = (mask[row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
+        acc[0] += m4[0];
+        acc[1] += (double)m4[1] + (on ? 0.5 * (double)a.Fx[e] : 0.0);
+        acc[2] += (double)m4[2] + (on ? 0.5 * (double)a.Fy[e] : 0.0);
+        acc[3] += (double)m4[3] + (on ? 0.5 * (double)a.Fz[e] : 0.0);
+    }
+    for (int c = 0; c < 4; c++) red[c][threadIdx.x] = acc[c];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int c = 0; c < 4; c++) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 4; c++) partial[blockIdx.x * 4 + c] = red[c][0];
+}
+
+__global__ void k_reduce_fp64_final(const double* partial, int nblocks, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double acc[4] = {0, 0, 0, 0};
+    for (int b = 0; b < nblocks; b++)
+        for (int c = 0; c < 4; c++) acc[c] += partial[b * 4 + c];
+    for (int c = 0; c < 4; c++) out[c] = acc[c];
+}
+
+cudaError_t launch_reduce_fp64(const IbmArgs& a, const uint32_t* mask, double* partial, double* out, cudaStream_t st) {
+    if (a.storage == STORE_F16) k_reduce_fp64<__half><<<kReduceBlocks, 256, 0, st>>>(a, mask, partial);
+    else if (a.storage == STORE_BF16) k_reduce_fp64<__nv_bfloat16><<<kReduceBlocks, 256, 0, st>>>(a, mask, partial);
+    else k_reduce_fp64<float><<<kReduceBlocks, 256, 0, st>>>(a, mask, partial);
+    k_reduce_fp64_final<<<1, 32, 0, st>>>(partial, kReduceBlocks, out);
+    return cudaGetLastError();
+}
+
+// Rest state of the 16-bit storage at density rho: every population
+// w_d * rho, stored as its deviation from w_d * rho0.
+template <typename S>
+__global__ void k_fill_rest(Planes Q, long long plane, float rho_ratio_m1, CollideParams p) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= plane) return;
+#pragma unroll
+    for (int d = 0; d < NQ; d++)
+        reinterpret_cast<S*>(Q.p[d])[t] = Storage<S>::enc(rho_ratio_m1 * (is_face(d) ? p.wface : p.wedge));
+}
+
+cudaError_t launch_fill_rest(Planes Q, long long plane, float rho, float rho0, int storage, const CollideParams& p,
+                             cudaStream_t st) {
+    const unsigned b = (unsigned)((plane + 255) / 256);
+    const float r = rho / rho0 - 1.f;
+    if (storage == STORE_F16) k_fill_rest<__half><<<b, 256, 0, st>>>(Q, plane, r, p);
+    else k_fill_rest<__nv_bfloat16><<<b, 256, 0, st>>>(Q, plane, r, p);
+    return cudaGetLastError();
+}
+
 size_t ibm_smem_bytes(const Dims& g, int cells) {
-    return (size_t)g.nx * g.kw * sizeof(uint32_t) + (size_t)3 * cells * sizeof(float);
+    (void)g;
+    return (size_t)3 * cells * sizeof(float);
 }
 
 cudaError_t ibm_prepare_smem(size_t bytes) {
-    return cudaFuncSetAttribute(k_ibm_spread, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_ibm_spread<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_ibm_spread<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, cudaStream_t st) {
@@ -381,18 +459,44 @@ cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, 
 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
     if (a.ncell > 0) {
-        k_ibm_cells<<<(a.ncell + 255) / 256, 256, 0, st>>>(a);
+        const unsigned b = (a.ncell + 255) / 256;
+        if (a.storage == STORE_F16) k_ibm_cells<__half><<<b, 256, 0, st>>>(a);
+        else if (a.storage == STORE_BF16) k_ibm_cells<__nv_bfloat16><<<b, 256, 0, st>>>(a);
+        else k_ibm_cells<float><<<b, 256, 0, st>>>(a);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }
     if (a.n > a.n0) {
-        k_ibm_gather_tail<<<(a.n - a.n0 + 127) / 128, 128, 0, st>>>(a);
+        const unsigned b = (a.n - a.n0 + 127) / 128;
+        if (a.storage == STORE_F16) k_ibm_gather_tail<__half><<<b, 128, 0, st>>>(a);
+        else if (a.storage == STORE_BF16) k_ibm_gather_tail<__nv_bfloat16><<<b, 128, 0, st>>>(a);
+        else k_ibm_gather_tail<float><<<b, 128, 0, st>>>(a);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }
-    const size_t smem = ibm_smem_bytes(a.g, a.smem_cells);
-    k_ibm_spread<<<a.g.ny, 512, smem, st>>>(a);
-    return cudaGetLastError();
+    // mask_new starts as the first segment's (static) touched cells
+    cudaError_t err = cudaMemcpyAsync(a.mask_new, a.mask_static, a.mask_bytes, cudaMemcpyDeviceToDevice, st);
+    if (err != cudaSuccess) return err;
+    // planes with many cells (an impeller disk) run on a side stream with a
+    // full-size tile and 512 threads, concurrently with the other planes
+    if (a.n_big > 0) {
+        err = cudaEventRecord(a.ev_fork, st);
+        if (err != cudaSuccess) return err;
+        err = cudaStreamWaitEvent(a.side, a.ev_fork, 0);
+        if (err != cudaSuccess) return err;
+        k_ibm_spread<512><<<a.n_big, 512, ibm_smem_bytes(a.g, a.big_tile_cells), a.side>>>(a, a.plane_list + a.n_small,
+                                                                                           a.big_tile_cells);
+        err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
+        err = cudaEventRecord(a.ev_join, a.side);
+        if (err != cudaSuccess) return err;
+    }
+    if (a.n_small > 0)
+        k_ibm_spread<256><<<a.n_small, 256, ibm_smem_bytes(a.g, a.smem_cells), st>>>(a, a.plane_list, a.smem_cells);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    if (a.n_big > 0) return cudaStreamWaitEvent(st, a.ev_join, 0);
+    return cudaSuccess;
 }
 
 }  // namespace tdlb

@@ -1,0 +1,490 @@
+// Step-kernel templates (Simple pull and Esotwist in place), generic in the
+// population storage type S (float, __half, __nv_bfloat16) and in V, the
+// cells per thread. Instantiated by step_kernels.cu (FP32 storage) and
+// step_kernels_h16.cu (16-bit deviation storage). See step_kernels.cu for
+// the streaming semantics.
+#pragma once
+#include <cstring>
+
+#include "tdlb_kernels.cuh"
+
+namespace tdlb {
+
+// ---------------------------------------------------------------------------
+// Thread mapping shared by both schemes: V consecutive cells of one row per
+// thread ("quad"), quads numbered row-major over (row, kq); a warp covers 32
+// consecutive quads, so neighbouring lanes hold neighbouring cells of the
+// same row except at row ends (where the wall rule or the periodic wrap
+// applies anyway). V in {1, 2, 4}; populations move as float/float2/float4.
+// ---------------------------------------------------------------------------
+constexpr unsigned FULL = 0xffffffffu;
+
+// FP32 vector helpers (F, Nu and FP32 populations)
+template <int V>
+__device__ __forceinline__ void vload(const float* __restrict__ p, float (&v)[V]) {
+    if constexpr (V == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (V == 2) {
+        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = __ldg(p);
+    }
+}
+template <int V>
+__device__ __forceinline__ void vstore(float* p, const float (&v)[V]) {
+    if constexpr (V == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    else if constexpr (V == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    else *p = v[0];
+}
+
+// Population plane access in storage type S: V elements from element e,
+// decoded to FP32 (RO: read-only, non-coherent path).
+template <typename S, int V, bool RO>
+__device__ __forceinline__ void pload(const float* plane, int e, float (&v)[V]) {
+    if constexpr (sizeof(S) == 4) {
+        const float* p = plane + e;
+        if constexpr (V == 4) {
+            const float4 t = RO ? __ldg(reinterpret_cast<const float4*>(p)) : *reinterpret_cast<const float4*>(p);
+            v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+        } else if constexpr (V == 2) {
+            const float2 t = RO ? __ldg(reinterpret_cast<const float2*>(p)) : *reinterpret_cast<const float2*>(p);
+            v[0] = t.x; v[1] = t.y;
+        } else {
+            v[0] = RO ? __ldg(p) : *p;
+        }
+    } else {
+        const S* p = reinterpret_cast<const S*>(plane) + e;
+        if constexpr (V == 4) {
+            const uint2 t = RO ? __ldg(reinterpret_cast<const uint2*>(p)) : *reinterpret_cast<const uint2*>(p);
+            S s4[4];
+            memcpy(s4, &t, sizeof t);
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[k] = Storage<S>::dec(s4[k]);
+        } else if constexpr (V == 2) {
+            const unsigned t = RO ? __ldg(reinterpret_cast<const unsigned*>(p)) : *reinterpret_cast<const unsigned*>(p);
+            S s2[2];
+            memcpy(s2, &t, sizeof t);
+            v[0] = Storage<S>::dec(s2[0]);
+            v[1] = Storage<S>::dec(s2[1]);
+        } else {
+            const unsigned short t = RO ? __ldg(reinterpret_cast<const unsigned short*>(p))
+                                        : *reinterpret_cast<const unsigned short*>(p);
+            S s1;
+            memcpy(&s1, &t, sizeof t);
+            v[0] = Storage<S>::dec(s1);
+        }
+    }
+}
+template <typename S, bool RO>
+__device__ __forceinline__ float pload1(const float* plane, int e) {
+    float v[1];
+    pload<S, 1, RO>(plane, e, v);
+    return v[0];
+}
+template <typename S, int V>
+__device__ __forceinline__ void pstore(float* plane, int e, const float (&v)[V]) {
+    if constexpr (sizeof(S) == 4) {
+        vstore<V>(plane + e, v);
+    } else {
+        S* p = reinterpret_cast<S*>(plane) + e;
+        if constexpr (V == 4) {
+            S s4[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) s4[k] = Storage<S>::enc(v[k]);
+            uint2 t;
+            memcpy(&t, s4, sizeof t);
+            *reinterpret_cast<uint2*>(p) = t;
+        } else if constexpr (V == 2) {
+            S s2[2] = {Storage<S>::enc(v[0]), Storage<S>::enc(v[1])};
+            unsigned t;
+            memcpy(&t, s2, sizeof t);
+            *reinterpret_cast<unsigned*>(p) = t;
+        } else {
+            *p = Storage<S>::enc(v[0]);
+        }
+    }
+}
+template <typename S>
+__device__ __forceinline__ void pstore1(float* plane, int e, float v) {
+    const float a[1] = {v};
+    pstore<S, 1>(plane, e, a);
+}
+// rest-population offset of direction/slot d in the deviation storage
+template <typename S>
+__device__ __forceinline__ float rest_of(int d, const CollideParams& p) {
+    return Storage<S>::deviation ? (is_face(d) ? p.wface : p.wedge) : 0.f;
+}
+
+struct Quad {
+    int i, j, k0;     // cell (i, j, k0 .. k0+V-1)
+    int row;          // i*ny + j
+    int e0;           // element index of (row, k0)
+    bool active;      // k0 < nz (the quad holds at least one cell)
+};
+
+template <int V>
+__device__ __forceinline__ Quad quad_of(const Dims& g, int nq, unsigned t) {
+    Quad q;
+    const unsigned total = (unsigned)g.nx * (unsigned)g.ny * (unsigned)nq;
+    const unsigned tc = t < total ? t : total - 1;   // keep spare lanes on a valid quad
+    const unsigned row = tc / (unsigned)nq;
+    const int kq = (int)(tc - row * (unsigned)nq);
+    q.row = (int)row;
+    q.i = (int)(row / (unsigned)g.ny);
+    q.j = (int)row - q.i * g.ny;
+    q.k0 = kq * V;
+    q.e0 = (int)row * g.kp + q.k0;
+    q.active = t < total && q.k0 < g.nz;
+    return q;
+}
+
+template <int V, bool LES, bool COLLIDE>
+__device__ __forceinline__ void collide_quad(float (&f)[NQ][V], const Quad& q, float* __restrict__ Nu,
+                                             const float* __restrict__ Fx, const float* __restrict__ Fy,
+                                             const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+                                             const Dims& g, const CollideParams& p, bool from_moments, float (&nu)[V]) {
+    if (!COLLIDE) return;
+    float fx[V], fy[V], fz[V];
+    const uint32_t bits = (__ldg(mask + (size_t)q.row * g.kw + (q.k0 >> 5)) >> (q.k0 & 31)) & ((1u << V) - 1u);
+    if (bits) {
+        vload<V>(Fx + q.e0, fx);
+        vload<V>(Fy + q.e0, fy);
+        vload<V>(Fz + q.e0, fz);
+#pragma unroll
+        for (int e = 0; e < V; e++)
+            if (!((bits >> e) & 1u)) fx[e] = fy[e] = fz[e] = 0.f;
+    } else {
+#pragma unroll
+        for (int e = 0; e < V; e++) fx[e] = fy[e] = fz[e] = 0.f;
+    }
+    if (LES) vload<V>(Nu + q.e0, nu);
+#pragma unroll
+    for (int e = 0; e < V; e++) {
+        float qv[NQ], m[NQ];
+#pragma unroll
+        for (int d = 0; d < NQ; d++) qv[d] = f[d][e];
+        if (from_moments) {
+#pragma unroll
+            for (int d = 0; d < NQ; d++) m[d] = qv[d];
+        } else {
+            moments_of(qv, m);
+        }
+        float n = LES ? nu[e] : 0.f;
+        collide<LES>(m, fx[e], fy[e], fz[e], n, p, qv);
+        if (LES) nu[e] = n;
+#pragma unroll
+        for (int d = 0; d < NQ; d++) f[d][e] = qv[d];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Simple (A/B, pull).
+//
+// All loads of a thread are issued as one straight-line batch (no branch
+// between them), so the 18 population fetches of a quad are in flight
+// together. V = 1 pulls every population directly from x - c_d. V > 1 loads
+// aligned vectors of the upstream rows and moves k-shifted values between
+// lanes with shuffles; the values a lane cannot get from a neighbour (warp
+// edges) and the own values the wall rule needs at row ends come from
+// scalar loads issued in the same batch (in bounds for every lane; the ones
+// a lane does not need hit L1).
+// ---------------------------------------------------------------------------
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE>
+__device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, float* __restrict__ Nu,
+                                            const float* __restrict__ Fx, const float* __restrict__ Fy,
+                                            const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+                                            const Dims& g, const CollideParams& p, unsigned t) {
+    const int nq = g.kp / V;
+    const Quad q = quad_of<V>(g, nq, t);
+    const int lane = threadIdx.x & 31;
+    const int rs = g.ny * g.kp;   // elements per i step
+    const bool i_lo = q.i == 0, i_hi = q.i == g.nx - 1, j_lo = q.j == 0, j_hi = q.j == g.ny - 1;
+    const bool k_first = q.k0 == 0, k_last = q.k0 + V >= g.nz;
+    float f[NQ][V];
+    if (FROM_MOMENTS) {
+#pragma unroll
+        for (int d = 0; d < NQ; d++) pload<S, V, true>(A.p[d], q.e0, f[d]);
+    } else if (V == 1) {
+#pragma unroll
+        for (int d = 0; d < NQ; d++) {
+            const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+            // upstream cell x - c_d; off the lattice -> the cell keeps its own value
+            const bool in = !((cx > 0 && i_lo) || (cx < 0 && i_hi) || (cy > 0 && j_lo) || (cy < 0 && j_hi) ||
+                              (cz > 0 && k_first) || (cz < 0 && k_last));
+            const int off = in ? -(cx * rs + cy * g.kp + cz) : 0;
+            f[d][0] = pload1<S, true>(A.p[d], q.e0 + off);
+        }
+    } else {
+        float hal[NQ], own[NQ];
+        // batch 1: every load
+#pragma unroll
+        for (int d = 0; d < NQ; d++) {
+            const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+            const bool row_ok = !((cx > 0 && i_lo) || (cx < 0 && i_hi) || (cy > 0 && j_lo) || (cy < 0 && j_hi));
+            const int soff = row_ok ? -(cx * rs + cy * g.kp) : 0;
+            const int src = q.e0 + soff;
+            pload<S, V, true>(A.p[d], src, f[d]);
+            if (cz > 0) {
+                hal[d] = pload1<S, true>(A.p[d], (lane == 0 && !k_first) ? src - 1 : src);
+                own[d] = (cx != 0 || cy != 0) ? pload1<S, true>(A.p[d], q.e0) : 0.f;
+            } else if (cz < 0) {
+                hal[d] = pload1<S, true>(A.p[d], (lane == 31 && !k_last) ? src + V : src);
+                int le = g.nz - 1 - q.k0;
+                le = le < 0 ? 0 : (le > V - 1 ? V - 1 : le);
+                own[d] = (cx != 0 || cy != 0) ? pload1<S, true>(A.p[d], q.e0 + le) : 0.f;
+            }
+        }
+        // batch 2: shift along k
+#pragma unroll
+        for (int d = 0; d < NQ; d++) {
+            const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+            const bool row_ok = !((cx > 0 && i_lo) || (cx < 0 && i_hi) || (cy > 0 && j_lo) || (cy < 0 && j_hi));
+            if (cz > 0) {                          // source k - 1
+                float left = __shfl_up_sync(FULL, f[d][V - 1], 1);
+                if (lane == 0) left = hal[d];
+                const float own0 = (cx != 0 || cy != 0) ? own[d] : f[d][0];
+                if (row_ok) {
+#pragma unroll
+                    for (int e = V - 1; e > 0; e--) f[d][e] = f[d][e - 1];
+                    f[d][0] = k_first ? own0 : left;
+                }
+            } else if (cz < 0) {                   // source k + 1
+                float right = __shfl_down_sync(FULL, f[d][0], 1);
+                if (lane == 31) right = hal[d];
+                const int le = g.nz - 1 - q.k0;   // element of the row's last cell when k_last
+                float ownl = own[d];
+                if (cx == 0 && cy == 0) {
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if (e == le) ownl = f[d][e];
+                }
+                if (row_ok) {
+#pragma unroll
+                    for (int e = 0; e < V - 1; e++) f[d][e] = f[d][e + 1];
+                    f[d][V - 1] = right;
+                    if (k_last) {
+#pragma unroll
+                        for (int e = 0; e < V; e++)
+                            if (e == le) f[d][e] = ownl;
+                    }
+                }
+            }
+        }
+    }
+    if (Storage<S>::deviation) {
+#pragma unroll
+        for (int d = 0; d < NQ; d++)
+#pragma unroll
+            for (int e = 0; e < V; e++) f[d][e] += rest_of<S>(d, p);
+    }
+    float nu[V];
+    collide_quad<V, LES, COLLIDE>(f, q, Nu, Fx, Fy, Fz, mask, g, p, FROM_MOMENTS, nu);
+    if (!q.active) return;
+#pragma unroll
+    for (int d = 0; d < NQ; d++) {
+        if (Storage<S>::deviation) {
+#pragma unroll
+            for (int e = 0; e < V; e++) f[d][e] -= rest_of<S>(d, p);
+        }
+        pstore<S, V>(B.p[d], q.e0, f[d]);
+    }
+    if (COLLIDE && LES) vstore<V>(Nu + q.e0, nu);
+}
+
+// ---------------------------------------------------------------------------
+// Esotwist (single buffer, in place).
+//
+// Slot s of cell x lives at x + o_s, o_s = max(-c_s, 0) (even) or
+// max(+c_s, 0) (odd), +1 wrapping to 0; a cell reads and writes the same 18
+// locations. V = 1 addresses them directly. For V > 1, where o_s has a k
+// component the V locations of a quad are k0+1 .. k0+V: loads take the
+// aligned vector at k0 and the next lane's first element; stores write the
+// aligned vector at k0 holding the previous lane's last value, and the lane
+// that owns the last cell of a warp (or of a row, where the location wraps to
+// k = 0) stores that one value alone. A __syncwarp() separates every lane's
+// loads from any lane's stores, so a location is always read by its owner
+// before a neighbour overwrites it.
+// ---------------------------------------------------------------------------
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN>
+__device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict__ Nu, const float* __restrict__ Fx,
+                                              const float* __restrict__ Fy, const float* __restrict__ Fz,
+                                              const uint32_t* __restrict__ mask, const Dims& g, const CollideParams& p,
+                                              unsigned t) {
+    const int nq = g.kp / V;
+    const Quad q = quad_of<V>(g, nq, t);
+    const int lane = threadIdx.x & 31;
+    const int i1 = q.i + 1 == g.nx ? 0 : q.i + 1;
+    const int j1 = q.j + 1 == g.ny ? 0 : q.j + 1;
+    const bool k_last = q.k0 + V >= g.nz;
+    const int last_e = g.nz - 1 - q.k0;   // element holding the row's last cell (if < V)
+    float f[NQ][V];
+    if (V == 1) {
+        const int k1 = q.k0 + 1 == g.nz ? 0 : q.k0 + 1;
+#pragma unroll
+        for (int s = 0; s < NQ; s++) {
+            const int sg = EVEN ? -1 : 1;
+            const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
+            const int d = EVEN ? s : (s ^ 1);
+            f[d][0] = pload1<S, false>(Q.p[s], ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp + (ok ? k1 : q.k0));
+        }
+    } else {
+        float hal[NQ], wrap[NQ];
+#pragma unroll
+        for (int s = 0; s < NQ; s++) {
+            const int sg = EVEN ? -1 : 1;
+            const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
+            const int d = EVEN ? s : (s ^ 1);
+            const int base = ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp;
+            pload<S, V, false>(Q.p[s], base + q.k0, f[d]);
+            if (ok) {
+                hal[s] = pload1<S, false>(Q.p[s], base + ((lane == 31 && !k_last) ? q.k0 + V : q.k0));
+                wrap[s] = pload1<S, false>(Q.p[s], base);
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < NQ; s++) {
+            const int sg = EVEN ? -1 : 1;
+            const bool ok = sg * cz_of(s) > 0;
+            const int d = EVEN ? s : (s ^ 1);
+            if (!ok) continue;
+            float right = __shfl_down_sync(FULL, f[d][0], 1);
+            if (lane == 31) right = hal[s];
+#pragma unroll
+            for (int e = 0; e < V - 1; e++) f[d][e] = f[d][e + 1];
+            f[d][V - 1] = right;
+            if (k_last) {                          // k = nz-1 wraps to 0
+#pragma unroll
+                for (int e = 0; e < V; e++)
+                    if (e == last_e) f[d][e] = wrap[s];
+            }
+        }
+    }
+    __syncwarp();
+    if (Storage<S>::deviation) {
+#pragma unroll
+        for (int d = 0; d < NQ; d++)
+#pragma unroll
+            for (int e = 0; e < V; e++) f[d][e] += rest_of<S>(d, p);
+    }
+    float nu[V];
+    collide_quad<V, LES, COLLIDE>(f, q, Nu, Fx, Fy, Fz, mask, g, p, FROM_MOMENTS, nu);
+    if (Storage<S>::deviation) {
+#pragma unroll
+        for (int d = 0; d < NQ; d++)
+#pragma unroll
+            for (int e = 0; e < V; e++) f[d][e] -= rest_of<S>(d, p);
+    }
+    if (V == 1) {
+        if (!q.active) return;
+        const int k1 = q.k0 + 1 == g.nz ? 0 : q.k0 + 1;
+#pragma unroll
+        for (int s = 0; s < NQ; s++) {
+            const int sg = EVEN ? -1 : 1;
+            const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
+            const int d = EVEN ? (s ^ 1) : s;
+            pstore1<S>(Q.p[s], ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp + (ok ? k1 : q.k0), f[d][0]);
+        }
+        if (COLLIDE && LES) Nu[q.e0] = nu[0];
+        return;
+    }
+    const bool k_first = q.k0 == 0;
+#pragma unroll
+    for (int s = 0; s < NQ; s++) {
+        const int sg = EVEN ? -1 : 1;
+        const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
+        const int d = EVEN ? (s ^ 1) : s;      // direction written to slot s
+        const int base = ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp;
+        if (!ok) {
+            if (q.active) pstore<S, V>(Q.p[s], base + q.k0, f[d]);
+            continue;
+        }
+        float w[V];
+        const float prev = __shfl_up_sync(FULL, f[d][V - 1], 1);
+        w[0] = prev;
+#pragma unroll
+        for (int e = 1; e < V; e++) w[e] = f[d][e - 1];
+        if (!q.active) continue;
+        if (lane != 0 && !k_first) {
+            pstore<S, V>(Q.p[s], base + q.k0, w);
+        } else {
+#pragma unroll
+            for (int e = 1; e < V; e++) pstore1<S>(Q.p[s], base + q.k0 + e, w[e]);
+        }
+        if (k_last) {                          // the wrap location of k = nz-1
+#pragma unroll
+            for (int e = 0; e < V; e++)
+                if (e == last_e) pstore1<S>(Q.p[s], base, f[d][e]);
+        } else if (lane == 31) {
+            pstore1<S>(Q.p[s], base + q.k0 + V, f[d][V - 1]);
+        }
+    }
+    if (COLLIDE && LES && q.active) vstore<V>(Nu + q.e0, nu);
+}
+
+
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE>
+__global__ void __launch_bounds__(128, 4) k_step_simple(Planes A, Planes B, float* __restrict__ Nu,
+                                                       const float* __restrict__ Fx, const float* __restrict__ Fy,
+                                                       const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+                                                       Dims g, CollideParams p) {
+    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE>(A, B, Nu, Fx, Fy, Fz, mask, g, p, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN>
+__global__ void __launch_bounds__(128, 4) k_step_esotwist(Planes Q, float* __restrict__ Nu,
+                                                         const float* __restrict__ Fx, const float* __restrict__ Fy,
+                                                         const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+                                                         Dims g, CollideParams p) {
+    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN>(Q, Nu, Fx, Fy, Fz, mask, g, p,
+                                                           blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Moments of the current state at every interior cell (what the reference's
+// Q holds after moments()), written to 18 FP32 output planes of the same
+// layout. mode: 0 = Simple populations (pull), 1 = moments (own cell),
+// 2 = Esotwist populations (read map, parity `even`), 3 = Esotwist moments.
+template <typename S>
+__global__ void __launch_bounds__(256) k_state_moments(Planes A, Planes M, Dims g, int mode, int even, CollideParams p) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = g.rows() * g.nz;
+    if (t >= total) return;
+    const int k = (int)(t % g.nz);
+    const long long row = t / g.nz;
+    const int j = (int)(row % g.ny);
+    const int i = (int)(row / g.ny);
+    const int e = (int)(row * g.kp + k);
+    float q[NQ], m[NQ];
+    if (mode <= 1) {
+#pragma unroll
+        for (int d = 0; d < NQ; d++) {
+            int src = e;
+            if (mode == 0) {
+                const int si = i - cx_of(d), sj = j - cy_of(d), sk = k - cz_of(d);
+                const bool in = (unsigned)si < (unsigned)g.nx && (unsigned)sj < (unsigned)g.ny && (unsigned)sk < (unsigned)g.nz;
+                if (in) src = (si * g.ny + sj) * g.kp + sk;
+            }
+            q[d] = pload1<S, false>(A.p[d], src) + (mode == 0 ? rest_of<S>(d, p) : 0.f);
+        }
+    } else {
+        const int i1 = i + 1 == g.nx ? 0 : i + 1, j1 = j + 1 == g.ny ? 0 : j + 1, k1 = k + 1 == g.nz ? 0 : k + 1;
+#pragma unroll
+        for (int d = 0; d < NQ; d++) {
+            const int s = even ? d : (d ^ 1);
+            const int sg = even ? -1 : 1;
+            const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
+            q[d] = pload1<S, false>(A.p[s], ((oi ? i1 : i) * g.ny + (oj ? j1 : j)) * g.kp + (ok ? k1 : k)) +
+                   (mode == 2 ? rest_of<S>(d, p) : 0.f);
+        }
+    }
+    if (mode == 0 || mode == 2) moments_of(q, m);
+    else {
+#pragma unroll
+        for (int d = 0; d < NQ; d++) m[d] = q[d];
+    }
+#pragma unroll
+    for (int d = 0; d < NQ; d++) M.p[d][e] = m[d];
+}
+
+}  // namespace tdlb

@@ -64,10 +64,17 @@ void release(tdlb_lattice* h) {
     cudaFree(h->d_cell_F);
     cudaFree(h->d_tail);
     cudaFree(h->d_sums);
+    cudaFree(h->d_mask_static);
+    cudaFree(h->d_plane_list);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    cudaFree(h->d_red);
     cudaFree(h->d_rot_xz);
     cudaFree(h->d_load);
     cudaFreeHost(h->h_stage);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    else if (h->stream) cudaStreamDestroy(h->stream);
 }
 
 void validate_config(const tdlb_config& c) {
@@ -75,7 +82,10 @@ void validate_config(const tdlb_config& c) {
     if (c.x > 32767 || c.y > 32767 || c.z > 32767) throw Fail{TDLB_EINVAL, "grid extent above 32767"};
     if (c.streaming != TDLB_STREAMING_SIMPLE && c.streaming != TDLB_STREAMING_ESOTWIST)
         throw Fail{TDLB_EINVAL, "streaming must be Simple (0) or Esotwist (1)"};
-    if (c.storage != TDLB_STORAGE_FP32) throw Fail{TDLB_EINVAL, "unsupported storage precision"};
+    if (c.storage != TDLB_STORAGE_FP32 && c.storage != TDLB_STORAGE_FP16 && c.storage != TDLB_STORAGE_BF16)
+        throw Fail{TDLB_EINVAL, "storage must be FP32 (0), FP16 (1) or BF16 (2)"};
+    if (c.storage != TDLB_STORAGE_FP32 && !(c.initialRho > 0.0))
+        throw Fail{TDLB_EINVAL, "16-bit storage needs initialRho > 0 (deviations are taken from it)"};
     if (!(c.nu >= 0.0) || !std::isfinite(c.nu)) throw Fail{TDLB_EINVAL, "nu must be finite and >= 0"};
 }
 
@@ -99,6 +109,9 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
         h->err.reserve(512);
         TDLB_CK(cudaSetDevice(device));
         TDLB_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        TDLB_CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        TDLB_CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+        TDLB_CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
         Dims& g = h->g;
         g.nx = (int)c.x; g.ny = (int)c.y; g.nz = (int)c.z;
         g.kp = (int)round_up(c.z, 16);
@@ -110,8 +123,10 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
         if (tdlb::ibm_smem_bytes(g, 0) > 200 * 1024)
             throw Fail{TDLB_EINVAL, "x * ceil(z/32) too large for the per-plane IBM flag tile"};
         h->cp = tdlb::make_collide_params(c.nu, c.cs0, c.g3);
+        h->cp.wface = (float)(c.initialRho / 12.0);
+        h->cp.wedge = (float)(c.initialRho / 24.0);
 
-        const size_t pop_bytes = (size_t)tdlb::NQ * g.plane * sizeof(float);
+        const size_t pop_bytes = (size_t)tdlb::NQ * g.plane * h->esz();
         size_t free_b = 0, total_b = 0;
         TDLB_CK(cudaMemGetInfo(&free_b, &total_b));
         const size_t need = pop_bytes * (c.streaming == TDLB_STREAMING_SIMPLE ? 2 : 1) +
@@ -220,6 +235,7 @@ tdlb::StepArgs step_args(tdlb_lattice* h, bool collide) {
     a.collide = collide ? 1 : 0;
     a.even = h->even ? 1 : 0;
     a.vec = h->vec;
+    a.storage = h->cfg.storage;
     return a;
 }
 
@@ -317,11 +333,37 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
     }
     if (n0) TDLB_CK(cudaMalloc(&h->d_prep, (size_t)tdlb::PF_COUNT * n0 * sizeof(float)));
     {
-        const size_t fit = 220 * 1024;
-        const int mc = h->cells.max_plane_cells;
-        h->smem_cells = tdlb::ibm_smem_bytes(g, mc) <= fit ? mc : 0;
-        const size_t bytes = tdlb::ibm_smem_bytes(g, h->smem_cells);
+        // F tiles: 4608 cells (3 CTAs of 256 threads per SM) for typical
+        // planes; planes with more cells (an impeller disk) go to a second
+        // launch with a tile for the largest of them (global memory beyond
+        // the 227 KB shared-memory limit)
+        const int small_cap = 4608;
+        std::vector<int> small, big;
+        int big_max = 0;
+        for (int j = 0; j < g.ny; j++) {
+            const int nc = h->cells.plane_cell[(size_t)j + 1] - h->cells.plane_cell[(size_t)j];
+            if (nc > small_cap) { big.push_back(j); big_max = std::max(big_max, nc); }
+            else small.push_back(j);
+        }
+        h->smem_cells = small_cap;
+        h->n_small = (int)small.size();
+        h->n_big = (int)big.size();
+        h->big_tile_cells = tdlb::ibm_smem_bytes(g, big_max) <= 220 * 1024 ? big_max : 0;
+        const size_t bytes = std::max(tdlb::ibm_smem_bytes(g, h->smem_cells), tdlb::ibm_smem_bytes(g, h->big_tile_cells));
         if (bytes > 48 * 1024) TDLB_CK(tdlb::ibm_prepare_smem(bytes));
+        small.insert(small.end(), big.begin(), big.end());
+        if (!h->d_plane_list) TDLB_CK(cudaMalloc(&h->d_plane_list, (size_t)g.ny * sizeof(int)));
+        TDLB_CK(cudaMemcpy(h->d_plane_list, small.data(), (size_t)g.ny * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    // static touched flags of the first segment
+    {
+        std::vector<uint32_t> ms((size_t)h->mask_words, 0u);
+        for (int e : h->cells.cell_e) {
+            const int row = e / g.kp, k = e - row * g.kp;
+            ms[(size_t)row * g.kw + (k >> 5)] |= 1u << (k & 31);
+        }
+        if (!h->d_mask_static) TDLB_CK(cudaMalloc(&h->d_mask_static, (size_t)h->mask_words * sizeof(uint32_t)));
+        TDLB_CK(cudaMemcpy(h->d_mask_static, ms.data(), ms.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     }
     if (!h->d_plane_lv0) {
         TDLB_CK(cudaMalloc(&h->d_plane_lv0, (size_t)(g.ny + 1) * sizeof(int)));
@@ -369,6 +411,13 @@ tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     a.tail_cap = h->tail_cap;
     a.sums = h->d_sums;
     a.smem_cells = h->smem_cells;
+    a.plane_list = h->d_plane_list;
+    a.n_small = h->n_small;
+    a.n_big = h->n_big;
+    a.big_tile_cells = h->big_tile_cells;
+    a.side = h->side;
+    a.ev_fork = h->ev_fork;
+    a.ev_join = h->ev_join;
     a.A = h->planes(h->state_buf());
     a.state_mode = h->state_mode();
     a.even = h->even ? 1 : 0;
@@ -377,9 +426,13 @@ tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     a.Fz = h->F + 2 * h->g.plane;
     a.mask_old = h->mask_cur();
     a.mask_new = h->mask_next();
+    a.mask_static = h->d_mask_static;
+    a.mask_bytes = (size_t)h->mask_words * sizeof(uint32_t);
     a.g = h->g;
     a.alpha = alpha;
     a.beta = beta;
+    a.storage = h->cfg.storage;
+    a.p = h->cp;
     return a;
 }
 
@@ -424,8 +477,8 @@ void host_aos_to_planes(tdlb_lattice* h, const float* in, int npl, float* dev) {
 float* state_moments(tdlb_lattice* h) {
     float* M = nullptr;
     TDLB_CK(cudaMalloc(&M, (size_t)tdlb::NQ * h->g.plane * sizeof(float)));
-    cudaError_t e = tdlb::launch_state_moments(h->planes(h->state_buf()), h->planes(M), h->g, h->state_mode(),
-                                               h->even ? 1 : 0, h->stream);
+    cudaError_t e = tdlb::launch_state_moments(h->planes(h->state_buf()), h->planes32(M), h->g, h->state_mode(),
+                                               h->even ? 1 : 0, h->stream, h->cfg.storage, h->cp);
     if (e != cudaSuccess) {
         cudaFree(M);
         throw Fail{TDLB_ECUDA, std::string("state moments: ") + cudaGetErrorString(e)};
@@ -495,7 +548,15 @@ int tdlb_initialise(tdlb_handle h, float rho) {
         h->even = true;
         h->holds_moments = true;
         h->pass = 0;
-        TDLB_CK(tdlb::launch_fill_uniform_moments(h->planes(h->bufA), g, rho, h->stream));
+        if (h->cfg.storage == TDLB_STORAGE_FP32) {
+            TDLB_CK(tdlb::launch_fill_uniform_moments(h->planes(h->bufA), g, rho, h->stream));
+        } else {
+            // 16-bit storage holds populations only: the rest populations of
+            // rho have the same moments (rho, 0, ..., 0) as the reference's Q
+            TDLB_CK(tdlb::launch_fill_rest(h->planes(h->bufA), g.plane, rho, (float)h->cfg.initialRho, h->cfg.storage,
+                                           h->cp, h->stream));
+            h->holds_moments = false;
+        }
         TDLB_CK(cudaMemsetAsync(h->Nu, 0, (size_t)g.plane * sizeof(float), h->stream));
         TDLB_CK(cudaMemsetAsync(h->F, 0, (size_t)3 * g.plane * sizeof(float), h->stream));
         TDLB_CK(cudaMemsetAsync(h->mask, 0, (size_t)2 * h->mask_words * sizeof(uint32_t), h->stream));
@@ -641,6 +702,19 @@ int tdlb_set_cells_per_thread(tdlb_handle h, int v) {
     });
 }
 
+int tdlb_reduce_fp64(tdlb_handle h, double* out4) {
+    return guarded(h, [&] {
+        require_init(h);
+        if (!out4) throw Fail{TDLB_EINVAL, "out is NULL"};
+        if (!h->d_red) TDLB_CK(cudaMalloc(&h->d_red, (size_t)(tdlb::kReduceBlocks * 4 + 4) * sizeof(double)));
+        tdlb::IbmArgs a = ibm_args(h, 0.f, 0.f);
+        TDLB_CK(tdlb::launch_reduce_fp64(a, h->mask_cur(), h->d_red, h->d_red + tdlb::kReduceBlocks * 4, h->stream));
+        TDLB_CK(cudaMemcpyAsync(out4, h->d_red + tdlb::kReduceBlocks * 4, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                                h->stream));
+        TDLB_CK(cudaStreamSynchronize(h->stream));
+    });
+}
+
 int tdlb_get_stream(tdlb_handle h, void** stream) {
     return guarded(h, [&] {
         if (!stream) throw Fail{TDLB_EINVAL, "out is NULL"};
@@ -687,6 +761,9 @@ int tdlb_attach_rushton(tdlb_handle h, const tdlb_rushton* spec, double nonupdat
         h->rot_ci = G.ci;
         h->rot_ck = G.ck;
         h->impeller_begin = n_fixed;
+        h->rspec = *spec;
+        h->angle = angle;
+        h->rstep = 1;
     });
 }
 
@@ -696,6 +773,7 @@ int tdlb_rotate_impeller(tdlb_handle h, double angle, double delta_angle) {
         TDLB_CK(tdlb::launch_rotate_markers(h->d_rot_xz, h->d_markers + h->n0, h->n_markers - h->n0, std::cos(angle),
                                             std::sin(angle), delta_angle, h->rot_ci, h->rot_ck, h->g.nx, h->g.nz,
                                             h->stream));
+        h->angle = angle;
     });
 }
 
@@ -773,6 +851,7 @@ int tdlb_schedule_levels(const tdlb_marker* markers, size_t n, int64_t x, int64_
 int tdlb_debug_get_state(tdlb_handle h, float* out) {
     return guarded(h, [&] {
         if (!out) throw Fail{TDLB_EINVAL, "out is NULL"};
+        if (h->cfg.storage != TDLB_STORAGE_FP32) throw Fail{TDLB_EINVAL, "raw state access needs FP32 storage"};
         planes_to_host_aos(h, h->state_buf(), tdlb::NQ, out);
     });
 }
@@ -780,6 +859,7 @@ int tdlb_debug_get_state(tdlb_handle h, float* out) {
 int tdlb_debug_set_state(tdlb_handle h, const float* in, int holds_moments) {
     return guarded(h, [&] {
         if (!in) throw Fail{TDLB_EINVAL, "in is NULL"};
+        if (h->cfg.storage != TDLB_STORAGE_FP32) throw Fail{TDLB_EINVAL, "raw state access needs FP32 storage"};
         host_aos_to_planes(h, in, tdlb::NQ, h->state_buf());
         h->holds_moments = holds_moments != 0;
         h->initialised = true;
@@ -789,8 +869,18 @@ int tdlb_debug_set_state(tdlb_handle h, const float* in, int holds_moments) {
 int tdlb_debug_transport(tdlb_handle h) {
     return guarded(h, [&] {
         require_init(h);
+        if (h->cfg.storage != TDLB_STORAGE_FP32) throw Fail{TDLB_EINVAL, "transport-only steps need FP32 storage"};
         run_step(h, false);
     });
 }
 
 }  // extern "C"
+
+namespace tdlb_rt {
+tdlb::StepArgs step_args(tdlb_lattice* h, bool collide) { return ::step_args(h, collide); }
+tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) { return ::ibm_args(h, alpha, beta); }
+void borrow_stream(tdlb_lattice* h, cudaStream_t s) {
+    if (!h->own_stream) h->own_stream = h->stream;
+    h->stream = s;
+}
+}  // namespace tdlb_rt

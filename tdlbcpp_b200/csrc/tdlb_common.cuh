@@ -15,6 +15,8 @@
 //     flags as one bit per cell: word r*kw + k/32, bit k%32.
 #pragma once
 #include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace tdlb {
@@ -43,10 +45,41 @@ struct Dims {
     __host__ __device__ long long rows() const { return (long long)nx * ny; }
 };
 
-// 18 plane base pointers of one population buffer.
+// 18 plane base pointers of one population buffer. With 16-bit storage the
+// pointers address __half / __nv_bfloat16 elements (kernels cast them).
 struct Planes {
     float* p[NQ];
 };
+
+// Population storage. FP32 stores f itself; the 16-bit forms store the
+// deviation f - w_d * rho0 from the rest weight of the direction's class
+// (w = 1/12 for faces, 1/24 for edges: the populations the Eggels-Somers
+// inverse filter gives at rest), and all arithmetic stays FP32.
+enum StorageKind { STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2 };
+
+template <typename S>
+struct Storage;
+template <>
+struct Storage<float> {
+    static constexpr bool deviation = false;
+    __device__ __forceinline__ static float dec(float x) { return x; }
+    __device__ __forceinline__ static float enc(float x) { return x; }
+};
+template <>
+struct Storage<__half> {
+    static constexpr bool deviation = true;
+    __device__ __forceinline__ static float dec(__half x) { return __half2float(x); }
+    __device__ __forceinline__ static __half enc(float x) { return __float2half_rn(x); }
+};
+template <>
+struct Storage<__nv_bfloat16> {
+    static constexpr bool deviation = true;
+    __device__ __forceinline__ static float dec(__nv_bfloat16 x) { return __bfloat162float(x); }
+    __device__ __forceinline__ static __nv_bfloat16 enc(float x) { return __float2bfloat16_rn(x); }
+};
+
+// rest population of slot/direction d for the deviation storage
+__host__ __device__ constexpr bool is_face(int d) { return d < 6; }
 
 // Collision constants (FlowParams fields the step reads).
 struct CollideParams {
@@ -54,6 +87,8 @@ struct CollideParams {
     float b0, c0;   // 1/(1+6 nu), 1-6 nu  (CollisionEgglesSomers.hpp:31-32)
     float cs0sq;    // Smagorinsky cs0^2
     float g3;       // third-order relaxation
+    float wface;    // rest populations rho0/12 and rho0/24 (16-bit storage offsets)
+    float wedge;
 };
 
 __host__ inline CollideParams make_collide_params(double nu, double cs0, double g3) {
@@ -63,6 +98,8 @@ __host__ inline CollideParams make_collide_params(double nu, double cs0, double 
     p.c0 = (float)(1.0 - 6.0 * (double)(float)nu);
     p.cs0sq = (float)cs0 * (float)cs0;
     p.g3 = (float)g3;
+    p.wface = 1.f / 12.f;
+    p.wedge = 1.f / 24.f;
     return p;
 }
 

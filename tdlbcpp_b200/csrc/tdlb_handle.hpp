@@ -17,7 +17,8 @@ struct tdlb_lattice {
     tdlb_config cfg{};
     Dims g{};
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;       // all of the handle's work is queued here
+    cudaStream_t own_stream = nullptr;   // set when `stream` is borrowed from a batch
     tdlb::CollideParams cp{};
 
     float* bufA = nullptr;       // 18 planes
@@ -52,6 +53,12 @@ struct tdlb_lattice {
     long long tail_cap = 0;
     float* d_sums = nullptr;      // 3 * marker_cap
     int smem_cells = 0;
+    int* d_plane_list = nullptr;  // small planes, then big planes
+    int n_small = 0, n_big = 0, big_tile_cells = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    uint32_t* d_mask_static = nullptr;   // first segment's touched cells
+    double* d_red = nullptr;             // FP64 reduction partials + result
     long long marker_cap = 0;
     long long level_cap = 0;
     int n_markers = 0;      // list length
@@ -65,13 +72,24 @@ struct tdlb_lattice {
     bool rot_device = false;
     double rot_ci = 0, rot_ck = 0;
     int impeller_begin = -1;      // first marker of the impeller (-1: none)
+    tdlb_rushton rspec{};         // the attached impeller's spec
+    double angle = 0.0;           // impeller angle of the last rotation
+    unsigned long long rstep = 1; // main-loop step the angle belongs to (main.cpp:336 starts at 1)
     double* d_load = nullptr;     // kLoadBlocks*5 partials + 5 results
     tdlb_marker* h_stage = nullptr;   // pinned staging of the blade upload
     size_t stage_cap = 0;
 
     std::string err = "no error";
 
+    size_t esz() const { return cfg.storage == TDLB_STORAGE_FP32 ? 4 : 2; }   // bytes per population
     Planes planes(float* base) const {
+        Planes p;
+        for (int d = 0; d < tdlb::NQ; d++)
+            p.p[d] = reinterpret_cast<float*>(reinterpret_cast<char*>(base) + (size_t)d * (size_t)g.plane * esz());
+        return p;
+    }
+    // FP32 planes of a moment buffer (always FP32)
+    Planes planes32(float* base) const {
         Planes p;
         for (int d = 0; d < tdlb::NQ; d++) p.p[d] = base + (size_t)d * (size_t)g.plane;
         return p;
@@ -86,3 +104,11 @@ struct tdlb_lattice {
     }
 };
 
+
+// Runtime helpers shared by the C-ABI translation units (tdlb_capi.cu).
+namespace tdlb_rt {
+tdlb::StepArgs step_args(tdlb_lattice* h, bool collide);
+tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta);
+// Queue h's work on `s` instead of its own stream (batches share one).
+void borrow_stream(tdlb_lattice* h, cudaStream_t s);
+}  // namespace tdlb_rt

@@ -20,12 +20,16 @@ struct StepArgs {
     int collide;            // 0: transport only (identity collision; known-answer tests)
     int even;               // Esotwist parity (evenStep)
     int vec;                // cells per thread: 1, 2 or 4 (float, float2, float4 traffic)
+    int storage;            // StorageKind of the population planes
 };
 
 cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_esotwist(const StepArgs& a, cudaStream_t st);
+cudaError_t launch_step_simple_h16(const StepArgs& a, cudaStream_t st);
+cudaError_t launch_step_esotwist_h16(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_fill_uniform_moments(Planes Q, const Dims& g, float rho, cudaStream_t st);
-cudaError_t launch_state_moments(Planes A, Planes M, const Dims& g, int mode, int even, cudaStream_t st);
+cudaError_t launch_state_moments(Planes A, Planes M, const Dims& g, int mode, int even, cudaStream_t st, int storage,
+                                 const CollideParams& p);
 
 // ---- immersed boundary ----
 
@@ -74,15 +78,24 @@ struct IbmArgs {
     float* tail;                // TF_COUNT * ntail_cap
     long long tail_cap;
     float* sums;                // 3 * n: each slot's spread sums (for the impeller load)
-    int smem_cells;             // F tile capacity per plane in shared memory (0: use cell_F in place)
+    int smem_cells;             // F tile capacity of the small-plane launch
+    const int* plane_list;      // [ny] small planes first, then the big ones
+    int n_small, n_big;         // planes in each launch
+    int big_tile_cells;         // F tile capacity of the big-plane launch
+    cudaStream_t side;          // stream of the big-plane launch
+    cudaEvent_t ev_fork, ev_join;
     Planes A;                   // current state
     int state_mode;             // 0 Simple pops, 1 moments, 2 Esotwist pops, 3 Esotwist moments
     int even;                   // Esotwist parity of the state's read map
     float* Fx; float* Fy; float* Fz;
     const uint32_t* mask_old;   // touched flags of the previous forcing pass
     uint32_t* mask_new;         // touched flags of this pass (fully written)
+    const uint32_t* mask_static;   // touched flags of the first segment (every pass)
+    size_t mask_bytes;
     Dims g;
     float alpha, beta;
+    int storage;                // StorageKind of the state planes
+    CollideParams p;            // rest offsets of the 16-bit storage
 };
 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st);
@@ -98,6 +111,13 @@ cudaError_t ibm_prepare_smem(size_t bytes);
 // the tank axis (ci, ck), out[4] = number of markers summed. `partial` holds
 // kLoadBlocks * 5 doubles.
 constexpr int kLoadBlocks = 128;
+// FP64 mass/momentum reduction: out[0] = sum rho, out[1..3] = sum (j + F/2).
+// `partial` holds kReduceBlocks * 4 doubles.
+constexpr int kReduceBlocks = 592;
+cudaError_t launch_reduce_fp64(const IbmArgs& a, const uint32_t* mask, double* partial, double* out, cudaStream_t st);
+// Rest state at density rho for the 16-bit storage.
+cudaError_t launch_fill_rest(Planes Q, long long plane, float rho, float rho0, int storage, const CollideParams& p,
+                             cudaStream_t st);
 cudaError_t launch_marker_load(const IbmArgs& a, int begin, double ci, double ck, double* partial, double* out,
                                cudaStream_t st);
 // Recompute n rotating markers (offsets xz[2n]) for cos/sin (ca, sa).
