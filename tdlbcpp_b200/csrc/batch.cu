@@ -1,22 +1,27 @@
 // Batched form: many independent tanks of uneven sizes on one GPU.
 //
-// All tanks' fused steps run as ONE persistent launch (k_batch_step): a grid
-// of a few blocks per SM loops over work items, each 128..256 consecutive
-// quads of one tank, with that tank's step view staged in shared memory; so
-// small tanks no longer leave most of the GPU idle. Per step the batch then
-// runs every tank's immersed-boundary pass (on a pool of streams, so the
-// tanks' passes overlap) and moves every attached impeller on the device
-// from a per-step cos/sin table. Two consecutive steps (one A/B and parity
-// cycle) are captured into a CUDA graph and replayed. The kernel shape --
-// cells per thread, threads per block, resident blocks per SM -- is chosen
-// by a small autotuner that times every candidate on the batch itself.
+// One batched step is seven launches whatever the number of tanks:
+//   1. k_rotate_batch   every attached impeller's blades at the step's angle,
+//                       read from a per-step (cos, sin, delta) table indexed
+//                       by a device step counter;
+//   2. k_batch_step     all tanks' fused collision + streaming: a persistent
+//                       grid of a few blocks per SM loops over work items,
+//                       each 128 or 256 consecutive quads of one tank, with
+//                       that tank's step view staged in shared memory (block
+//                       0 also advances the step counter);
+//   3-7. the immersed-boundary passes of all tanks (launch_ibm_batch): cells,
+//                       blade gathers, touched-flag copies, small-plane and
+//                       large-plane spreads, each one launch over all tanks.
+// Two consecutive steps (one A/B and parity cycle) are captured into a CUDA
+// graph and replayed. The fused launch's shape -- cells per thread, threads
+// per block, resident blocks per SM -- is chosen by an autotuner that times
+// every candidate on the batch itself.
 #include "tdlb_handle.hpp"
 #include "tdlb_geometry.hpp"
 #include "tdlb_rotate.hpp"
 #include "step_kernels.cuh"
 
 #include <algorithm>
-#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -35,6 +40,15 @@ struct TankStep {
     Dims g;
     CollideParams p;
     int les, from_moments, even, pad;
+};
+
+// One tank's impeller for the rotation launch.
+struct TankRotor {
+    const double* xz;            // blade offsets in the impeller frame
+    Marker* out;                 // the blades of the resident marker list
+    const double* table;         // [steps][3] cos a, sin a, delta a
+    double ci, ck;
+    int n, nx, nz, pad;
 };
 
 template <int NT>
@@ -57,12 +71,14 @@ __device__ __forceinline__ void tank_quad(const TankStep& ts, unsigned t) {
 // Persistent batched step: block b takes work items b, b + grid, ...; an
 // item is `NT` consecutive quads of one tank, whose step view is staged in
 // shared memory. 16-bit storage never holds moments, so its from-moments
-// bodies are not built.
+// bodies are not built. `counter` (may be NULL) is advanced once: this
+// launch runs after the step's rotation, which reads it.
 template <typename S, int V, int NT, bool ESO>
 __global__ void __launch_bounds__(NT) k_batch_step(const TankStep* __restrict__ tanks, const int2* __restrict__ work,
-                                                   int nwork) {
+                                                   int nwork, int* counter) {
     constexpr bool kFM = sizeof(S) == 4;
     __shared__ TankStep ts;
+    if (counter && blockIdx.x == 0 && threadIdx.x == 0) *counter += 1;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const int2 wk = work[w];
         __syncthreads();
@@ -79,30 +95,26 @@ __global__ void __launch_bounds__(NT) k_batch_step(const TankStep* __restrict__ 
     }
 }
 
-// Blade rotation from a per-step table (cos a, sin a, delta a) indexed by
-// the device step counter, so a captured graph can replay many steps.
-__global__ void k_rotate_tab(const double* __restrict__ xz, Marker* __restrict__ out, int n,
-                             const double* __restrict__ table, const int* __restrict__ step, double ci, double ck, int nx,
-                             int nz) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
-    const double* tb = table + 3 * (size_t)(*step);
-    const RotatedMarker r = rotate_marker(xz[2 * q], xz[2 * q + 1], tb[0], tb[1], tb[2], ci, ck, nx, nz);
-    Marker& m = out[q];
-    m.i = r.i;
-    m.k = r.k;
-    m.iCartFraction = r.iCartFraction;
-    m.kCartFraction = r.kCartFraction;
-    m.uDelta = r.uDelta;
-    m.vDelta = 0.f;
-    m.wDelta = r.wDelta;
+// Blade rotation of every tank: work item = (tank, first of 256 blades).
+__global__ void __launch_bounds__(256) k_rotate_batch(const TankRotor* __restrict__ rotors, const int2* __restrict__ work,
+                                                      const int* __restrict__ step) {
+    const int2 w = work[blockIdx.x];
+    const TankRotor& r = rotors[w.x];
+    const int q = w.y + threadIdx.x;
+    if (q >= r.n) return;
+    const double* tb = r.table + 3 * (size_t)(*step);
+    const RotatedMarker m = rotate_marker(r.xz[2 * q], r.xz[2 * q + 1], tb[0], tb[1], tb[2], r.ci, r.ck, r.nx, r.nz);
+    Marker& o = r.out[q];
+    o.i = m.i;
+    o.k = m.k;
+    o.iCartFraction = m.iCartFraction;
+    o.kCartFraction = m.kCartFraction;
+    o.uDelta = m.uDelta;
+    o.vDelta = 0.f;
+    o.wDelta = m.wDelta;
 }
 
-__global__ void k_counter_inc(int* step) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
-}
-
-using BatchFn = void (*)(const TankStep*, const int2*, int);
+using BatchFn = void (*)(const TankStep*, const int2*, int, int*);
 
 template <typename S, bool ESO>
 BatchFn pick(int v, int nt) {
@@ -120,23 +132,39 @@ BatchFn batch_kernel(int storage, bool eso, int v, int nt) {
 
 }  // namespace tdlb
 
+using tdlb::TankRotor;
 using tdlb::TankStep;
+
+namespace {
+
+// A device array of int2 work items, regrown as needed.
+struct WorkList {
+    int2* d = nullptr;
+    int n = 0, cap = 0;
+};
+
+}  // namespace
 
 struct tdlb_batch_s {
     int device = 0;
     std::vector<tdlb_lattice*> tanks;
     cudaStream_t stream = nullptr;
-    std::vector<cudaStream_t> pool;   // per-tank IBM passes run spread over these
-    std::vector<cudaEvent_t> ev;      // fork/join events
-    TankStep* d_steps = nullptr;      // [2][n]: views of an even and an odd step of a run
-    int2* d_work = nullptr;
-    int nwork = 0;
-    int* d_step = nullptr;            // device step counter of a run
-    std::vector<double*> d_table;     // per tank: [steps][3] cos, sin, delta
+    cudaStream_t side = nullptr;       // large-plane spreads
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    TankStep* d_steps = nullptr;       // [2][n]: views of an even and an odd step of a run
+    tdlb::IbmArgs* d_ibm = nullptr;    // [2][n]: forcing passes of the same two steps
+    WorkList work;                     // fused-step items (tank, first quad)
+    int* d_step = nullptr;             // device step counter of a run
+    std::vector<double*> d_table;      // per tank: [steps][3] cos, sin, delta
     std::vector<int> table_cap;
-    int vec = 1, threads = 128, bps = 4;   // kernel shape
+    TankRotor* d_rotors = nullptr;     // [n]
+    WorkList rot_work;                 // (tank, first blade)
+    WorkList cells, tails, copies, small, big;   // immersed-boundary items
+    int small_tile = 0, big_tile = 0;
+    std::vector<unsigned> ibm_gen;     // marker generation the IBM lists were built for
+    int vec = 1, threads = 128, bps = 4;   // fused-launch shape
     int grid = 0;
-    long long launches = 0;           // kernels run by tdlb_batch_run* so far
+    long long launches = 0;            // kernels run by tdlb_batch_run* so far
     std::string err = "no error";
 };
 
@@ -174,7 +202,25 @@ int bguard(tdlb_batch_s* b, F&& fn) {
 int storage_of(const tdlb_batch_s* b) { return b->tanks[0]->cfg.storage; }
 bool eso_of(const tdlb_batch_s* b) { return b->tanks[0]->cfg.streaming == TDLB_STREAMING_ESOTWIST; }
 
-// Work list for the current kernel shape: (tank, first quad) per item.
+// Upload `items` into `w` (the stream is idle: callers synchronise first).
+void put(WorkList& w, const std::vector<int2>& items) {
+    if ((int)items.size() > w.cap) {
+        cudaFree(w.d);
+        w.d = nullptr;
+        w.cap = 0;
+        TDLB_BCK(cudaMalloc(&w.d, std::max<size_t>(items.size(), 1) * sizeof(int2)));
+        w.cap = (int)items.size();
+    }
+    if (!items.empty()) TDLB_BCK(cudaMemcpy(w.d, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    w.n = (int)items.size();
+}
+
+void drop(WorkList& w) {
+    cudaFree(w.d);
+    w = WorkList{};
+}
+
+// Fused-step work list for the current shape: (tank, first quad) per item.
 void build_work(tdlb_batch_s* b) {
     std::vector<int2> w;
     for (int t = 0; t < (int)b->tanks.size(); t++) {
@@ -183,14 +229,41 @@ void build_work(tdlb_batch_s* b) {
         for (long long q = 0; q < nq; q += b->threads) w.push_back(make_int2(t, (int)q));
     }
     TDLB_BCK(cudaStreamSynchronize(b->stream));   // queued launches may still read the old list
-    cudaFree(b->d_work);
-    b->d_work = nullptr;
-    TDLB_BCK(cudaMalloc(&b->d_work, w.size() * sizeof(int2)));
-    TDLB_BCK(cudaMemcpy(b->d_work, w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice));
-    b->nwork = (int)w.size();
+    put(b->work, w);
     int sms = 0;
     TDLB_BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-    b->grid = std::min(b->nwork, sms * b->bps);
+    b->grid = std::min(b->work.n, sms * b->bps);
+}
+
+// Immersed-boundary work lists; rebuilt when a tank's markers changed.
+void build_ibm_work(tdlb_batch_s* b) {
+    bool same = true;
+    for (size_t t = 0; t < b->tanks.size(); t++) same = same && b->ibm_gen[t] == b->tanks[t]->marker_gen;
+    if (same) return;
+    std::vector<int2> cells, tails, copies, small, big;
+    int small_tile = 0, big_tile = 0;
+    for (int t = 0; t < (int)b->tanks.size(); t++) {
+        const tdlb_lattice* h = b->tanks[(size_t)t];
+        if (!h->markers_set) continue;
+        const int ncell = (int)h->cells.cell_e.size();
+        for (int c = 0; c < ncell; c += 256) cells.push_back(make_int2(t, c));
+        for (int q = 0; q < h->n_markers - h->n0; q += 128) tails.push_back(make_int2(t, q));
+        for (long long wd = 0; wd < h->mask_words; wd += tdlb::kMaskCopyWords) copies.push_back(make_int2(t, (int)wd));
+        for (int s = 0; s < h->n_small; s++) small.push_back(make_int2(t, h->h_plane_list[(size_t)s]));
+        for (int s = 0; s < h->n_big; s++) big.push_back(make_int2(t, h->h_plane_list[(size_t)(h->n_small + s)]));
+        small_tile = std::max(small_tile, h->smem_cells);
+        if (h->n_big) big_tile = std::max(big_tile, h->big_tile_cells);
+    }
+    TDLB_BCK(cudaStreamSynchronize(b->stream));
+    put(b->cells, cells);
+    put(b->tails, tails);
+    put(b->copies, copies);
+    put(b->small, small);
+    put(b->big, big);
+    b->small_tile = small_tile;
+    b->big_tile = big_tile;
+    TDLB_BCK(tdlb::ibm_batch_prepare_smem(tdlb::ibm_smem_bytes(Dims{}, small_tile), tdlb::ibm_smem_bytes(Dims{}, big_tile)));
+    for (size_t t = 0; t < b->tanks.size(); t++) b->ibm_gen[t] = b->tanks[t]->marker_gen;
 }
 
 TankStep view_of(tdlb_lattice* h) {
@@ -211,76 +284,61 @@ TankStep view_of(tdlb_lattice* h) {
     return s;
 }
 
-// Advance every tank's host bookkeeping by one fused step.
+// Advance a tank's host bookkeeping over one fused step.
 void advance_step_state(tdlb_lattice* h) {
     if (h->cfg.streaming == TDLB_STREAMING_SIMPLE) h->cur ^= 1;
     else h->even = !h->even;
     h->holds_moments = false;
 }
 
-void launch_fused(tdlb_batch_s* b, const TankStep* d_views, cudaStream_t st) {
+void launch_fused(tdlb_batch_s* b, const TankStep* d_views, int* counter, cudaStream_t st) {
     const tdlb::BatchFn fn = tdlb::batch_kernel(storage_of(b), eso_of(b), b->vec, b->threads);
-    fn<<<b->grid, b->threads, 0, st>>>(d_views, b->d_work, b->nwork);
+    fn<<<b->grid, b->threads, 0, st>>>(d_views, b->work.d, b->work.n, counter);
     TDLB_BCK(cudaGetLastError());
 }
 
-// Kernels one immersed-boundary pass launches (tdlb::launch_ibm).
-int ibm_kernels(const tdlb::IbmArgs& a) {
-    return (a.ncell > 0) + (a.n > a.n0) + (a.n_big > 0) + (a.n_small > 0);
-}
-
-// One batched step as launches on b->stream (also used inside capture):
-// rotate impellers, fused step (views = d_views), IBM pass per tank.
-// Returns the number of kernels it queued.
-int queue_step(tdlb_batch_s* b, const TankStep* d_views, float alpha, float beta, bool use_table) {
+// One batched step on b->stream (also used inside capture). `k` selects the
+// uploaded views (0: first step of the pair, 1: second). Returns the number
+// of kernels it queued.
+int queue_step(tdlb_batch_s* b, int k) {
     const size_t n = b->tanks.size();
-    const size_t P = b->pool.size();
-    int kernels = 1;
-    if (use_table) {
-        for (size_t t = 0; t < n; t++) {
-            tdlb_lattice* h = b->tanks[t];
-            if (!h->rot_device || h->n_markers == h->n0) continue;
-            const int nr = h->n_markers - h->n0;
-            tdlb::k_rotate_tab<<<(nr + 255) / 256, 256, 0, b->stream>>>(h->d_rot_xz, h->d_markers + h->n0, nr,
-                                                                         b->d_table[t], b->d_step, h->rot_ci, h->rot_ck,
-                                                                         h->g.nx, h->g.nz);
-            kernels++;
-        }
-        TDLB_BCK(cudaGetLastError());
-    }
-    launch_fused(b, d_views, b->stream);
-    for (size_t t = 0; t < n; t++) advance_step_state(b->tanks[t]);
-    // the tanks' IBM passes, spread over the stream pool
-    TDLB_BCK(cudaEventRecord(b->ev[0], b->stream));
-    for (size_t k = 0; k < P; k++) TDLB_BCK(cudaStreamWaitEvent(b->pool[k], b->ev[0], 0));
-    for (size_t t = 0; t < n; t++) {
-        tdlb_lattice* h = b->tanks[t];
-        if (!h->markers_set) continue;
-        cudaStream_t s = b->pool[t % P];
-        const tdlb::IbmArgs ia = tdlb_rt::ibm_args(h, alpha, beta);
-        TDLB_BCK(tdlb::launch_ibm(ia, s));
-        kernels += ibm_kernels(ia);
-        h->pass++;
-        h->last_beta = beta;
-    }
-    for (size_t k = 0; k < P; k++) {
-        TDLB_BCK(cudaEventRecord(b->ev[1 + k], b->pool[k]));
-        TDLB_BCK(cudaStreamWaitEvent(b->stream, b->ev[1 + k], 0));
-    }
-    if (use_table) {
-        tdlb::k_counter_inc<<<1, 32, 0, b->stream>>>(b->d_step);
+    int kernels = 0;
+    if (b->rot_work.n) {
+        tdlb::k_rotate_batch<<<b->rot_work.n, 256, 0, b->stream>>>(b->d_rotors, b->rot_work.d, b->d_step);
         TDLB_BCK(cudaGetLastError());
         kernels++;
+    }
+    launch_fused(b, b->d_steps + (size_t)k * n, b->d_step, b->stream);
+    kernels++;
+    for (tdlb_lattice* h : b->tanks) advance_step_state(h);
+    tdlb::IbmBatch ib{};
+    ib.args = b->d_ibm + (size_t)k * n;
+    ib.cells = b->cells.d; ib.n_cells = b->cells.n;
+    ib.tails = b->tails.d; ib.n_tails = b->tails.n;
+    ib.copies = b->copies.d; ib.n_copies = b->copies.n;
+    ib.small = b->small.d; ib.n_small = b->small.n;
+    ib.big = b->big.d; ib.n_big = b->big.n;
+    ib.small_tile = b->small_tile;
+    ib.big_tile = b->big_tile;
+    ib.storage = storage_of(b);
+    TDLB_BCK(tdlb::launch_ibm_batch(ib, b->stream, b->side, b->ev_fork, b->ev_join));
+    kernels += (ib.n_cells > 0) + (ib.n_tails > 0) + (ib.n_copies > 0) + (ib.n_small > 0) + (ib.n_big > 0);
+    for (tdlb_lattice* h : b->tanks) {
+        if (!h->markers_set) continue;
+        h->pass++;
     }
     return kernels;
 }
 
-void upload_views(tdlb_batch_s* b) {
-    // views of the next two steps (the host state is restored afterwards)
+// Views and forcing arguments of the next two steps, uploaded in stream
+// order (launches already queued read the previous ones). The host state is
+// left as it was.
+void upload_views(tdlb_batch_s* b, float alpha, float beta) {
     const size_t n = b->tanks.size();
     std::vector<TankStep> v(2 * n);
+    std::vector<tdlb::IbmArgs> ia(2 * n);
     std::vector<int> cur(n), pass(n);
-    std::vector<bool> even(n), hm(n);
+    std::vector<char> even(n), hm(n);
     for (size_t t = 0; t < n; t++) {
         tdlb_lattice* h = b->tanks[t];
         cur[t] = h->cur; pass[t] = h->pass; even[t] = h->even; hm[t] = h->holds_moments;
@@ -290,24 +348,30 @@ void upload_views(tdlb_batch_s* b) {
             tdlb_lattice* h = b->tanks[t];
             v[(size_t)k * n + t] = view_of(h);
             advance_step_state(h);
-            h->pass++;
+            ia[(size_t)k * n + t] = tdlb_rt::ibm_args(h, alpha, beta);
+            if (h->markers_set) h->pass++;
         }
     for (size_t t = 0; t < n; t++) {
         tdlb_lattice* h = b->tanks[t];
         h->cur = cur[t]; h->pass = pass[t]; h->even = even[t]; h->holds_moments = hm[t];
     }
-    // stream-ordered: launches already queued read the previous views
     TDLB_BCK(cudaMemcpyAsync(b->d_steps, v.data(), v.size() * sizeof(TankStep), cudaMemcpyHostToDevice, b->stream));
+    TDLB_BCK(cudaMemcpyAsync(b->d_ibm, ia.data(), ia.size() * sizeof(tdlb::IbmArgs), cudaMemcpyHostToDevice, b->stream));
 }
 
-// Per-step (cos, sin, delta) of every attached impeller for `steps` steps.
+// Per-step (cos, sin, delta) of every attached impeller for `steps` steps,
+// and the rotation launch's tank table.
 void build_tables(tdlb_batch_s* b, int steps) {
+    std::vector<TankRotor> rot(b->tanks.size());
+    std::vector<int2> items;
     for (size_t t = 0; t < b->tanks.size(); t++) {
         tdlb_lattice* h = b->tanks[t];
-        if (!h->rot_device) continue;
+        rot[t] = TankRotor{};
+        if (!h->rot_device || h->n_markers == h->n0) continue;
         if (b->table_cap[t] < steps) {
             cudaFree(b->d_table[t]);
             b->d_table[t] = nullptr;
+            b->table_cap[t] = 0;
             TDLB_BCK(cudaMalloc(&b->d_table[t], (size_t)3 * steps * sizeof(double)));
             b->table_cap[t] = steps;
         }
@@ -324,7 +388,12 @@ void build_tables(tdlb_batch_s* b, int steps) {
             tab[(size_t)3 * s + 2] = d;
         }
         TDLB_BCK(cudaMemcpy(b->d_table[t], tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        const int nr = h->n_markers - h->n0;
+        rot[t] = TankRotor{h->d_rot_xz, h->d_markers + h->n0, b->d_table[t], h->rot_ci, h->rot_ck, nr, h->g.nx, h->g.nz, 0};
+        for (int q = 0; q < nr; q += 256) items.push_back(make_int2((int)t, q));
     }
+    TDLB_BCK(cudaMemcpy(b->d_rotors, rot.data(), rot.size() * sizeof(TankRotor), cudaMemcpyHostToDevice));
+    put(b->rot_work, items);
 }
 
 void finish_tables(tdlb_batch_s* b, int steps) {
@@ -343,30 +412,32 @@ void check_ready(tdlb_batch_s* b) {
         if (!h->initialised) throw BFail{TDLB_ESTATE, "every tank must be initialised first"};
 }
 
-// Steps, eager or graph-replayed: the first step of a tank that still holds
-// moments (right after initialise) always runs eagerly.
+// `steps` steps, eager or graph-replayed. A step whose state still holds
+// moments (right after initialise) runs eagerly: its views differ from the
+// repeating pair's.
 void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
     check_ready(b);
-    TDLB_BCK(cudaStreamSynchronize(b->stream));   // the previous run may still read the tables
+    TDLB_BCK(cudaStreamSynchronize(b->stream));   // the previous run may still read the tables and lists
+    build_ibm_work(b);
     build_tables(b, steps);
     TDLB_BCK(cudaMemsetAsync(b->d_step, 0, sizeof(int), b->stream));
     int done = 0;
     bool any_moments = false;
     for (tdlb_lattice* h : b->tanks) any_moments = any_moments || h->holds_moments;
     while (done < steps && (any_moments || !graph || steps - done < 2)) {
-        upload_views(b);
-        b->launches += queue_step(b, b->d_steps, alpha, beta, true);
+        upload_views(b, alpha, beta);
+        b->launches += queue_step(b, 0);
         done++;
         any_moments = false;
     }
     if (done < steps) {
-        upload_views(b);
+        upload_views(b, alpha, beta);
         cudaGraph_t g = nullptr;
         int per_pair = 0;
         TDLB_BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            per_pair += queue_step(b, b->d_steps, alpha, beta, true);
-            per_pair += queue_step(b, b->d_steps + b->tanks.size(), alpha, beta, true);
+            per_pair += queue_step(b, 0);
+            per_pair += queue_step(b, 1);
         } catch (...) {
             cudaStreamEndCapture(b->stream, &g);
             if (g) cudaGraphDestroy(g);
@@ -377,9 +448,10 @@ void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
         const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
         cudaGraphDestroy(g);
         TDLB_BCK(ie);
-        // the capture advanced the host state by two steps; each replay is two steps
+        // the capture advanced the host state by the pair; the replays run it
         const int pairs = (steps - done) / 2;
-        for (tdlb_lattice* h : b->tanks) h->pass -= 2;
+        for (tdlb_lattice* h : b->tanks)
+            if (h->markers_set) h->pass -= 2;
         for (int r = 0; r < pairs; r++) {
             const cudaError_t le = cudaGraphLaunch(ge, b->stream);
             if (le != cudaSuccess) {
@@ -388,28 +460,34 @@ void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
             }
         }
         cudaGraphExecDestroy(ge);
-        for (tdlb_lattice* h : b->tanks) h->pass += 2 * pairs;
+        for (tdlb_lattice* h : b->tanks)
+            if (h->markers_set) h->pass += 2 * pairs;
         b->launches += (long long)per_pair * pairs;
         done += 2 * pairs;
         if (done < steps) {   // an odd step left
-            upload_views(b);
-            b->launches += queue_step(b, b->d_steps, alpha, beta, true);
+            upload_views(b, alpha, beta);
+            b->launches += queue_step(b, 0);
             done++;
         }
     }
     finish_tables(b, steps);
+    for (tdlb_lattice* h : b->tanks)
+        if (h->markers_set) h->last_beta = beta;   // for tdlb_impeller_load
 }
 
 void release(tdlb_batch_s* b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (tdlb_lattice* h : b->tanks) tdlb_destroy(h);
-    for (cudaStream_t s : b->pool) cudaStreamDestroy(s);
-    for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
     for (double* p : b->d_table) cudaFree(p);
+    for (WorkList* w : {&b->work, &b->rot_work, &b->cells, &b->tails, &b->copies, &b->small, &b->big}) drop(*w);
     cudaFree(b->d_steps);
-    cudaFree(b->d_work);
+    cudaFree(b->d_ibm);
+    cudaFree(b->d_rotors);
     cudaFree(b->d_step);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->side) cudaStreamDestroy(b->side);
     if (b->stream) cudaStreamDestroy(b->stream);
 }
 
@@ -436,16 +514,17 @@ int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* ou
         }
         TDLB_BCK(cudaSetDevice(device));
         TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        TDLB_BCK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+        TDLB_BCK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        TDLB_BCK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
         for (tdlb_lattice* h : b->tanks) tdlb_rt::borrow_stream(h, b->stream);
-        const int P = std::min(n, 16);
-        b->pool.resize((size_t)P);
-        for (auto& s : b->pool) TDLB_BCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-        b->ev.resize((size_t)P + 1);
-        for (auto& e : b->ev) TDLB_BCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         TDLB_BCK(cudaMalloc(&b->d_steps, (size_t)2 * n * sizeof(TankStep)));
+        TDLB_BCK(cudaMalloc(&b->d_ibm, (size_t)2 * n * sizeof(tdlb::IbmArgs)));
+        TDLB_BCK(cudaMalloc(&b->d_rotors, (size_t)n * sizeof(TankRotor)));
         TDLB_BCK(cudaMalloc(&b->d_step, sizeof(int)));
         b->d_table.assign((size_t)n, nullptr);
         b->table_cap.assign((size_t)n, 0);
+        b->ibm_gen.assign((size_t)n, ~0u);
         b->vec = cfgs[0].streaming == TDLB_STREAMING_SIMPLE ? 1 : 4;
         build_work(b);
     } catch (const BFail& f) {
@@ -506,9 +585,8 @@ int tdlb_batch_get_shape(tdlb_batch b, int* cells_per_thread, int* threads, int*
 }
 
 // Times the fused batched launch for every candidate shape on the batch's
-// own (initialised) tanks and keeps the fastest. The timed launches write
-// the populations the next step would overwrite anyway, but they also
-// update the LES eddy viscosity; callers re-initialise afterwards.
+// own (initialised) tanks and keeps the fastest. The timed launches repeat
+// the next step's view, so they change the fields; callers initialise again.
 int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms) {
     return bguard(b, [&] {
         check_ready(b);
@@ -524,24 +602,31 @@ int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms) {
                     cands.push_back({v, nt, bps});
                 }
         }
-        upload_views(b);
+        TDLB_BCK(cudaStreamSynchronize(b->stream));
+        upload_views(b, 0.f, 0.f);
         cudaEvent_t e0, e1;
         TDLB_BCK(cudaEventCreate(&e0));
         TDLB_BCK(cudaEventCreate(&e1));
         float best = 1e30f;
         Cand win = cands[0];
-        for (const Cand& c : cands) {
-            b->vec = c.v; b->threads = c.nt; b->bps = c.bps;
-            build_work(b);
-            launch_fused(b, b->d_steps, b->stream);   // warm-up
-            TDLB_BCK(cudaEventRecord(e0, b->stream));
-            for (int r = 0; r < trials; r++) launch_fused(b, b->d_steps, b->stream);
-            TDLB_BCK(cudaEventRecord(e1, b->stream));
-            TDLB_BCK(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            TDLB_BCK(cudaEventElapsedTime(&ms, e0, e1));
-            ms /= trials;
-            if (ms < best) { best = ms; win = c; }
+        try {
+            for (const Cand& c : cands) {
+                b->vec = c.v; b->threads = c.nt; b->bps = c.bps;
+                build_work(b);
+                launch_fused(b, b->d_steps, nullptr, b->stream);   // warm-up
+                TDLB_BCK(cudaEventRecord(e0, b->stream));
+                for (int r = 0; r < trials; r++) launch_fused(b, b->d_steps, nullptr, b->stream);
+                TDLB_BCK(cudaEventRecord(e1, b->stream));
+                TDLB_BCK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                TDLB_BCK(cudaEventElapsedTime(&ms, e0, e1));
+                ms /= trials;
+                if (ms < best) { best = ms; win = c; }
+            }
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

@@ -28,20 +28,34 @@
 #include "tdlb_kernels.cuh"
 #include "tdlb_rotate.hpp"
 
+#include <algorithm>
+
 namespace tdlb {
 
-// 3-point smoothed delta (Forcing.hpp:18-35).
-__device__ __forceinline__ float calc_weight(float x) {
-    x = fabsf(x);
-    float w = 0.f;
-    if (x <= 1.5f) {
-        if (x <= 0.5f) w = (1.f / 3.f) * (1.f + sqrtf(fmaf(-3.f * x, x, 1.f)));
-        else {
-            const float y = 1.f - x;
-            w = (1.f / 6.f) * (5.f - 3.f * x - sqrtf(fmaf(-3.f * y, y, 1.f)));
-        }
+// 3-point smoothed delta (Forcing.hpp:18-35). The reference evaluates it
+// in double (its literals promote the float argument) and rounds the result
+// to float; every operation here is an explicitly rounded double operation
+// in the reference's order, so no kernel can contract it differently and
+// the weights equal the reference's bit for bit.
+__device__ __forceinline__ float calc_weight(float xf) {
+    const double x = (double)fabsf(xf);
+    if (x > 1.5) return 0.f;
+    double w;
+    if (x <= 0.5) {
+        const double r = __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(-3.0, x), x), 1.0));
+        w = __dmul_rn(1.0 / 3.0, __dadd_rn(1.0, r));
+    } else {
+        const double y = __dsub_rn(1.0, x);
+        const double r = __dsqrt_rn(__dadd_rn(__dmul_rn(-3.0, __dmul_rn(y, y)), 1.0));
+        w = __dmul_rn(1.0 / 6.0, __dsub_rn(__dsub_rn(5.0, __dmul_rn(3.0, x)), r));
     }
-    return w;
+    return __double2float_rn(w);
+}
+
+// Weight of stencil offset (i1, k1) for a marker at fractions (icf, kcf):
+// the product of the two 1-D weights, rounded to float (Forcing.hpp:37-48).
+__device__ __forceinline__ float stencil_weight(float icf, float kcf, int i1, int k1) {
+    return __fmul_rn(calc_weight(__fadd_rn(-icf, (float)i1)), calc_weight(__fadd_rn(-kcf, (float)k1)));
 }
 
 __device__ __forceinline__ int wrap_i(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
@@ -105,7 +119,7 @@ __global__ void k_ibm_prepare(IbmArgs a, float* __restrict__ prep) {
     for (int k1 = -1; k1 <= 1; k1++)
         for (int i1 = -1; i1 <= 1; i1++, c++)
             prep[(PF_W + c) * n0 + p] =
-                calc_weight(-mk.iCartFraction + (float)i1) * calc_weight(-mk.kCartFraction + (float)k1);
+                stencil_weight(mk.iCartFraction, mk.kCartFraction, i1, k1);
     prep[PF_U * n0 + p] = mk.uDelta;
     prep[PF_V * n0 + p] = mk.vDelta;
     prep[PF_WV * n0 + p] = mk.wDelta;
@@ -116,9 +130,7 @@ __global__ void k_ibm_prepare(IbmArgs a, float* __restrict__ prep) {
 // cells), and the F each cell starts the pass with (zero unless the previous
 // pass touched it, Forcing.hpp:162-174).
 template <typename S>
-__global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.ncell) return;
+__device__ __forceinline__ void ibm_cell(const IbmArgs& a, int c) {
     const Dims& g = a.g;
     const int e = a.cell_e[c];
     const int row = e / g.kp;
@@ -136,12 +148,16 @@ __global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a) {
     a.cell_F[2 * C + c] = live ? a.Fz[e] : 0.f;
 }
 
+template <typename S>
+__global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < a.ncell) ibm_cell<S>(a, c);
+}
+
 // Second segment (the blades): weights and the moments of the 9 stencil
 // cells of every blade marker.
 template <typename S>
-__global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n - a.n0) return;
+__device__ __forceinline__ void ibm_tail_marker(const IbmArgs& a, int t) {
     const Marker mk = a.markers[a.sched[a.n0 + t]];
     const int i = (int)mk.i, j = (int)mk.j, k = (int)mk.k;
     float* s = a.tail;
@@ -149,7 +165,7 @@ __global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
     int c = 0;
     for (int k1 = -1; k1 <= 1; k1++) {
         for (int i1 = -1; i1 <= 1; i1++, c++) {
-            const float w = calc_weight(-mk.iCartFraction + (float)i1) * calc_weight(-mk.kCartFraction + (float)k1);
+            const float w = stencil_weight(mk.iCartFraction, mk.kCartFraction, i1, k1);
             const int i2 = wrap_i(i + i1, a.g.nx), k2 = wrap_i(k + k1, a.g.nz);
             float m4[4];
             cell_moments4<S>(a.A, a.state_mode, a.even, a.g, i2, j, k2, a.p, m4);
@@ -166,17 +182,20 @@ __global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
     s[TF_WV * cap + t] = mk.wDelta;
 }
 
+template <typename S>
+__global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < a.n - a.n0) ibm_tail_marker<S>(a, t);
+}
+
 // One CTA per j-plane: the plane's first-segment levels on an F tile in
 // shared memory (planes with more cells than the tile holds work on cell_F
 // in place), write-back to F, then the blade levels on the dense F. The
 // touched flags of the first segment never change, so each pass starts
 // mask_new as a copy of them (mask_static) and the blade walk adds its cells.
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes,
-                                                                       int tile_cells) {
-    extern __shared__ float tile[];                             // [3][tile_cells]
+__device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int tile_cells, float* tile) {
     const Dims g = a.g;
-    const int j = planes[blockIdx.x];
     const int c0 = a.plane_cell[j], nc = a.plane_cell[j + 1] - c0;
     const long long C = a.ncell;
     const bool in_smem = nc <= tile_cells;
@@ -295,6 +314,13 @@ __global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread(
         }
         __syncthreads();
     }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes,
+                                                                       int tile_cells) {
+    extern __shared__ float tile[];                             // [3][tile_cells]
+    ibm_spread_plane<THREADS>(a, planes[blockIdx.x], tile_cells, tile);
 }
 
 // Impeller rotation on the device: recomputes the blade markers of the
@@ -496,6 +522,104 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     if (a.n_big > 0) return cudaStreamWaitEvent(st, a.ev_join, 0);
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// Batched passes: the immersed-boundary passes of many lattices in one set of
+// launches. Every block takes one work item (lattice, first index); the
+// lattice's IbmArgs is staged in shared memory and the single-lattice body
+// runs on it, so each lattice's result equals its own launch_ibm.
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void stage_args(IbmArgs& dst, const IbmArgs* src) {
+    static_assert(sizeof(IbmArgs) % 8 == 0, "IbmArgs words");
+    constexpr int words = sizeof(IbmArgs) / 8;
+    for (int w = threadIdx.x; w < words; w += NT)
+        reinterpret_cast<unsigned long long*>(&dst)[w] = reinterpret_cast<const unsigned long long*>(src)[w];
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_ibm_cells_batch(const IbmArgs* __restrict__ args, const int2* __restrict__ work) {
+    __shared__ IbmArgs sa;
+    const int2 w = work[blockIdx.x];
+    stage_args<256>(sa, args + w.x);
+    __syncthreads();
+    const int c = w.y + threadIdx.x;
+    if (c < sa.ncell) ibm_cell<S>(sa, c);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(128) k_ibm_tail_batch(const IbmArgs* __restrict__ args, const int2* __restrict__ work) {
+    __shared__ IbmArgs sa;
+    const int2 w = work[blockIdx.x];
+    stage_args<128>(sa, args + w.x);
+    __syncthreads();
+    const int t = w.y + threadIdx.x;
+    if (t < sa.n - sa.n0) ibm_tail_marker<S>(sa, t);
+}
+
+// mask_new = mask_static, kMaskCopyWords words per work item
+__global__ void __launch_bounds__(256) k_mask_copy_batch(const IbmArgs* __restrict__ args, const int2* __restrict__ work) {
+    const int2 w = work[blockIdx.x];
+    const IbmArgs& a = args[w.x];
+    const long long words = (long long)(a.mask_bytes / sizeof(uint32_t));
+    uint32_t* dst = a.mask_new;
+    const uint32_t* src = a.mask_static;
+    for (int q = threadIdx.x; q < kMaskCopyWords; q += 256) {
+        const long long e = (long long)w.y + q;
+        if (e < words) dst[e] = src[e];
+    }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread_batch(const IbmArgs* __restrict__ args,
+                                                                             const int2* __restrict__ work, int big) {
+    extern __shared__ float tile[];
+    __shared__ IbmArgs sa;
+    const int2 w = work[blockIdx.x];
+    stage_args<THREADS>(sa, args + w.x);
+    __syncthreads();
+    ibm_spread_plane<THREADS>(sa, w.y, big ? sa.big_tile_cells : sa.smem_cells, tile);
+}
+
+cudaError_t ibm_batch_prepare_smem(size_t small_bytes, size_t big_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(k_ibm_spread_batch<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)std::max<size_t>(small_bytes, 1));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_ibm_spread_batch<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)std::max<size_t>(big_bytes, 1));
+}
+
+cudaError_t launch_ibm_batch(const IbmBatch& b, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
+    if (b.n_cells > 0) {
+        if (b.storage == STORE_F16) k_ibm_cells_batch<__half><<<b.n_cells, 256, 0, st>>>(b.args, b.cells);
+        else if (b.storage == STORE_BF16) k_ibm_cells_batch<__nv_bfloat16><<<b.n_cells, 256, 0, st>>>(b.args, b.cells);
+        else k_ibm_cells_batch<float><<<b.n_cells, 256, 0, st>>>(b.args, b.cells);
+    }
+    if (b.n_tails > 0) {
+        if (b.storage == STORE_F16) k_ibm_tail_batch<__half><<<b.n_tails, 128, 0, st>>>(b.args, b.tails);
+        else if (b.storage == STORE_BF16) k_ibm_tail_batch<__nv_bfloat16><<<b.n_tails, 128, 0, st>>>(b.args, b.tails);
+        else k_ibm_tail_batch<float><<<b.n_tails, 128, 0, st>>>(b.args, b.tails);
+    }
+    if (b.n_copies > 0) k_mask_copy_batch<<<b.n_copies, 256, 0, st>>>(b.args, b.copies);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    if (b.n_big > 0) {
+        err = cudaEventRecord(fork, st);
+        if (err != cudaSuccess) return err;
+        err = cudaStreamWaitEvent(side, fork, 0);
+        if (err != cudaSuccess) return err;
+        k_ibm_spread_batch<512><<<b.n_big, 512, ibm_smem_bytes(Dims{}, b.big_tile), side>>>(b.args, b.big, 1);
+        err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
+        err = cudaEventRecord(join, side);
+        if (err != cudaSuccess) return err;
+    }
+    if (b.n_small > 0) k_ibm_spread_batch<256><<<b.n_small, 256, ibm_smem_bytes(Dims{}, b.small_tile), st>>>(b.args, b.small, 0);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    if (b.n_big > 0) return cudaStreamWaitEvent(st, join, 0);
     return cudaSuccess;
 }
 

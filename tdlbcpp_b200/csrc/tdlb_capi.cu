@@ -354,6 +354,7 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
         small.insert(small.end(), big.begin(), big.end());
         if (!h->d_plane_list) TDLB_CK(cudaMalloc(&h->d_plane_list, (size_t)g.ny * sizeof(int)));
         TDLB_CK(cudaMemcpy(h->d_plane_list, small.data(), (size_t)g.ny * sizeof(int), cudaMemcpyHostToDevice));
+        h->h_plane_list = small;
     }
     // static touched flags of the first segment
     {
@@ -390,6 +391,7 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
     h->markers_set = true;
     h->rot_device = false;
     h->impeller_begin = -1;
+    h->marker_gen++;
 }
 
 tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {

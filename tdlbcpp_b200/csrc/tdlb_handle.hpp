@@ -54,6 +54,8 @@ struct tdlb_lattice {
     float* d_sums = nullptr;      // 3 * marker_cap
     int smem_cells = 0;
     int* d_plane_list = nullptr;  // small planes, then big planes
+    std::vector<int> h_plane_list;   // host copy of d_plane_list
+    unsigned marker_gen = 0;      // bumped by every marker upload
     int n_small = 0, n_big = 0, big_tile_cells = 0;
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;

@@ -99,6 +99,24 @@ struct IbmArgs {
 };
 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st);
+
+// Immersed-boundary passes of many lattices in one set of launches: device
+// IbmArgs per lattice and work lists of (lattice, first index) items --
+// cells: 256 first-segment cells; tails: 128 blade markers; copies: 1024
+// touched-flag words; small / big: one j-plane (256 / 512 threads).
+struct IbmBatch {
+    const IbmArgs* args;
+    const int2* cells; int n_cells;
+    const int2* tails; int n_tails;
+    const int2* copies; int n_copies;
+    const int2* small; int n_small;
+    const int2* big; int n_big;
+    int small_tile, big_tile;   // dynamic F tiles (cells) of the two spread launches
+    int storage;
+};
+constexpr int kMaskCopyWords = 1024;
+cudaError_t launch_ibm_batch(const IbmBatch& b, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join);
+cudaError_t ibm_batch_prepare_smem(size_t small_bytes, size_t big_bytes);
 // Per-upload preparation of the first segment (weights, velocities).
 cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, cudaStream_t st);
 // Shared memory the spread kernel needs: the plane's touched-flag tile plus
