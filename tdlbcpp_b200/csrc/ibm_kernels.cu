@@ -22,9 +22,12 @@
 // only where the bit is set, and the next pass treats F as zero where neither
 // the previous pass (mask_old) nor the current one has touched the cell.
 //
-// Two launches: k_ibm_gather (all markers in parallel: weights and the
-// moments of the 9 stencil cells, which no marker changes) and k_ibm_spread
-// (per plane, per level: the order-dependent F updates).
+// Per pass (launch_ibm): k_ibm_cells (moments and starting F of every unique
+// stencil cell of the static markers), k_ibm_gather_tail (weights and
+// stencil moments of every blade marker, which no marker changes), a copy of
+// the static touched flags into mask_new, then k_ibm_spread, one CTA per
+// j-plane: the static markers' levels on an F tile in shared memory, then
+// the blade levels on a shared-memory hash table of the plane's blade cells.
 #include "tdlb_kernels.cuh"
 #include "tdlb_rotate.hpp"
 
@@ -188,14 +191,175 @@ __global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
     if (t < a.n - a.n0) ibm_tail_marker<S>(a, t);
 }
 
+// Blade levels of plane j on global memory: F and the touched flags are
+// read back from L2 (__ldcg), since earlier levels of this CTA wrote them.
+// Used when the plane's blade stencils do not fit the shared-memory table.
+__device__ __forceinline__ void blade_levels_global(const IbmArgs& a, int j) {
+    const Dims g = a.g;
+    const float* s = a.tail;
+    const long long cap = a.tail_cap;
+    for (int lv = a.plane_lv1[j]; lv < a.plane_lv1[j + 1]; lv++) {
+        const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
+        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            const int t = p - a.n0;
+            float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                const float w = s[(TF_W + c) * cap + t];
+                const int packed = __float_as_int(s[(TF_CELL + c) * cap + t]);
+                const int i2 = packed >> 16, k2 = packed & 0xffff;
+                const long long row = (long long)i2 * g.ny + j;
+                const long long e = row * g.kp + k2;
+                const long long wd = row * g.kw + (k2 >> 5);
+                const uint32_t bit = 1u << (k2 & 31);
+                const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
+                const float vx = live ? __ldcg(a.Fx + e) : 0.f;
+                const float vy = live ? __ldcg(a.Fy + e) : 0.f;
+                const float vz = live ? __ldcg(a.Fz + e) : 0.f;
+                rhoSum = fmaf(w, s[(TF_RHO + c) * cap + t], rhoSum);
+                xSum = fmaf(w, fmaf(0.5f, vx, s[(TF_MX + c) * cap + t]), xSum);
+                ySum = fmaf(w, fmaf(0.5f, vy, s[(TF_MY + c) * cap + t]), ySum);
+                zSum = fmaf(w, fmaf(0.5f, vz, s[(TF_MZ + c) * cap + t]), zSum);
+            }
+            xSum = fmaf(-rhoSum, s[TF_U * cap + t], xSum);
+            ySum = fmaf(-rhoSum, s[TF_V * cap + t], ySum);
+            zSum = fmaf(-rhoSum, s[TF_WV * cap + t], zSum);
+            a.sums[p] = xSum;
+            a.sums[a.n + p] = ySum;
+            a.sums[2 * a.n + p] = zSum;
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                const int packed = __float_as_int(s[(TF_CELL + c) * cap + t]);
+                const int i2 = packed >> 16, k2 = packed & 0xffff;
+                const long long row = (long long)i2 * g.ny + j;
+                const long long e = row * g.kp + k2;
+                const long long wd = row * g.kw + (k2 >> 5);
+                const uint32_t bit = 1u << (k2 & 31);
+                const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
+                const float vx = live ? __ldcg(a.Fx + e) : 0.f;
+                const float vy = live ? __ldcg(a.Fy + e) : 0.f;
+                const float vz = live ? __ldcg(a.Fz + e) : 0.f;
+                const float bw = a.beta * s[(TF_W + c) * cap + t];
+                a.Fx[e] = fmaf(a.alpha, vx, -bw * xSum);
+                a.Fy[e] = fmaf(a.alpha, vy, -bw * ySum);
+                a.Fz[e] = fmaf(a.alpha, vz, -bw * zSum);
+                atomicOr(&a.mask_new[wd], bit);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Blade levels of plane j on a shared-memory table. The plane's 9 x nb
+// stencil references (nb blade markers) go into an open-addressing hash
+// table keyed by the packed cell (i << 16 | k), H >= 9 nb entries of (key,
+// Fx, Fy, Fz), so every insert ends within H probes. Each cell's F is loaded
+// once -- zero unless this pass (mask_new: the first segment's cells) or the
+// previous one touched it -- the levels run on the table, and the cells go
+// back to F with their touched flags. The walk reads and writes the same
+// values in the same order as blade_levels_global; only the L2 round trips
+// between levels go. Needs 4 H + 9 nb words of `tile`; returns false, having
+// done nothing, when they do not fit.
+template <int THREADS>
+__device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float* tile, int tile_words) {
+    const int lv0 = a.plane_lv1[j], lv1 = a.plane_lv1[j + 1];
+    const int q0 = a.level_ptr[lv0], q1 = a.level_ptr[lv1];
+    const int nref = 9 * (q1 - q0);
+    int lg = 5;
+    while ((1 << lg) < nref) lg++;
+    const int H = 1 << lg;
+    if (4LL * H + nref > (long long)tile_words) return false;
+    int* keys = reinterpret_cast<int*>(tile);
+    float* hx = tile + H;
+    float* hy = tile + 2 * H;
+    float* hz = tile + 3 * H;
+    int* ref = reinterpret_cast<int*>(tile + 4 * H);
+    const Dims g = a.g;
+    const float* s = a.tail;
+    const long long cap = a.tail_cap;
+
+    for (int h = threadIdx.x; h < H; h += THREADS) keys[h] = -1;
+    __syncthreads();
+    for (int r = threadIdx.x; r < nref; r += THREADS) {
+        const int m = r / 9, c = r - 9 * m;
+        const int key = __float_as_int(s[(TF_CELL + c) * cap + (q0 + m - a.n0)]);
+        unsigned h = ((unsigned)key * 2654435761u) >> (32 - lg);
+        for (int probe = 0; probe < H; probe++) {
+            const int prev = atomicCAS(&keys[h], -1, key);
+            if (prev == -1 || prev == key) break;
+            h = (h + 1) & (unsigned)(H - 1);
+        }
+        ref[r] = (int)h;
+    }
+    __syncthreads();
+    for (int h = threadIdx.x; h < H; h += THREADS) {
+        const int key = keys[h];
+        if (key < 0) continue;
+        const int i2 = key >> 16, k2 = key & 0xffff;
+        const long long row = (long long)i2 * g.ny + j;
+        const long long e = row * g.kp + k2;
+        const long long wd = row * g.kw + (k2 >> 5);
+        const uint32_t bit = 1u << (k2 & 31);
+        const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
+        hx[h] = live ? __ldcg(a.Fx + e) : 0.f;
+        hy[h] = live ? __ldcg(a.Fy + e) : 0.f;
+        hz[h] = live ? __ldcg(a.Fz + e) : 0.f;
+    }
+    __syncthreads();
+    for (int lv = lv0; lv < lv1; lv++) {
+        const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
+        for (int p = p0 + threadIdx.x; p < p1; p += THREADS) {
+            const int t = p - a.n0;
+            const int* rf = ref + 9 * (p - q0);
+            float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                const float w = s[(TF_W + c) * cap + t];
+                const int h = rf[c];
+                rhoSum = fmaf(w, s[(TF_RHO + c) * cap + t], rhoSum);
+                xSum = fmaf(w, fmaf(0.5f, hx[h], s[(TF_MX + c) * cap + t]), xSum);
+                ySum = fmaf(w, fmaf(0.5f, hy[h], s[(TF_MY + c) * cap + t]), ySum);
+                zSum = fmaf(w, fmaf(0.5f, hz[h], s[(TF_MZ + c) * cap + t]), zSum);
+            }
+            xSum = fmaf(-rhoSum, s[TF_U * cap + t], xSum);
+            ySum = fmaf(-rhoSum, s[TF_V * cap + t], ySum);
+            zSum = fmaf(-rhoSum, s[TF_WV * cap + t], zSum);
+            a.sums[p] = xSum;
+            a.sums[a.n + p] = ySum;
+            a.sums[2 * a.n + p] = zSum;
+#pragma unroll
+            for (int c = 0; c < 9; c++) {   // sequential: a wrapped stencil sees its own update
+                const int h = rf[c];
+                const float bw = a.beta * s[(TF_W + c) * cap + t];
+                hx[h] = fmaf(a.alpha, hx[h], -bw * xSum);
+                hy[h] = fmaf(a.alpha, hy[h], -bw * ySum);
+                hz[h] = fmaf(a.alpha, hz[h], -bw * zSum);
+            }
+        }
+        __syncthreads();
+    }
+    for (int h = threadIdx.x; h < H; h += THREADS) {
+        const int key = keys[h];
+        if (key < 0) continue;
+        const int i2 = key >> 16, k2 = key & 0xffff;
+        const long long row = (long long)i2 * g.ny + j;
+        const long long e = row * g.kp + k2;
+        a.Fx[e] = hx[h];
+        a.Fy[e] = hy[h];
+        a.Fz[e] = hz[h];
+        atomicOr(&a.mask_new[row * g.kw + (k2 >> 5)], 1u << (k2 & 31));
+    }
+    return true;
+}
+
 // One CTA per j-plane: the plane's first-segment levels on an F tile in
 // shared memory (planes with more cells than the tile holds work on cell_F
-// in place), write-back to F, then the blade levels on the dense F. The
-// touched flags of the first segment never change, so each pass starts
-// mask_new as a copy of them (mask_static) and the blade walk adds its cells.
+// in place), write-back to F, then the blade levels, on a shared-memory
+// table when they fit the tile, else on global F. The touched flags of the
+// first segment never change, so each pass starts mask_new as a copy of them
+// (mask_static) and the blade walk adds its cells.
 template <int THREADS>
 __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int tile_cells, float* tile) {
-    const Dims g = a.g;
     const int c0 = a.plane_cell[j], nc = a.plane_cell[j + 1] - c0;
     const long long C = a.ncell;
     const bool in_smem = nc <= tile_cells;
@@ -258,62 +422,9 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
     }
     __syncthreads();
 
-    // ---- second segment (blades): dense F; mask_new holds this pass's
-    //      touched cells (the first segment's, plus blade cells so far)
-    const float* s = a.tail;
-    const long long cap = a.tail_cap;
-    for (int lv = a.plane_lv1[j]; lv < a.plane_lv1[j + 1]; lv++) {
-        const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
-        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-            const int t = p - a.n0;
-            float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
-#pragma unroll
-            for (int c = 0; c < 9; c++) {
-                const float w = s[(TF_W + c) * cap + t];
-                const int packed = __float_as_int(s[(TF_CELL + c) * cap + t]);
-                const int i2 = packed >> 16, k2 = packed & 0xffff;
-                const long long row = (long long)i2 * g.ny + j;
-                const long long e = row * g.kp + k2;
-                const long long wd = row * g.kw + (k2 >> 5);
-                const uint32_t bit = 1u << (k2 & 31);
-                // L2 reads: flags and F written by this CTA's earlier levels
-                const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
-                const float vx = live ? __ldcg(a.Fx + e) : 0.f;
-                const float vy = live ? __ldcg(a.Fy + e) : 0.f;
-                const float vz = live ? __ldcg(a.Fz + e) : 0.f;
-                rhoSum = fmaf(w, s[(TF_RHO + c) * cap + t], rhoSum);
-                xSum = fmaf(w, fmaf(0.5f, vx, s[(TF_MX + c) * cap + t]), xSum);
-                ySum = fmaf(w, fmaf(0.5f, vy, s[(TF_MY + c) * cap + t]), ySum);
-                zSum = fmaf(w, fmaf(0.5f, vz, s[(TF_MZ + c) * cap + t]), zSum);
-            }
-            xSum = fmaf(-rhoSum, s[TF_U * cap + t], xSum);
-            ySum = fmaf(-rhoSum, s[TF_V * cap + t], ySum);
-            zSum = fmaf(-rhoSum, s[TF_WV * cap + t], zSum);
-            a.sums[p] = xSum;
-            a.sums[a.n + p] = ySum;
-            a.sums[2 * a.n + p] = zSum;
-#pragma unroll
-            for (int c = 0; c < 9; c++) {
-                const int packed = __float_as_int(s[(TF_CELL + c) * cap + t]);
-                const int i2 = packed >> 16, k2 = packed & 0xffff;
-                const long long row = (long long)i2 * g.ny + j;
-                const long long e = row * g.kp + k2;
-                const long long wd = row * g.kw + (k2 >> 5);
-                const uint32_t bit = 1u << (k2 & 31);
-                // L2 reads: flags and F written by this CTA's earlier levels
-                const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
-                const float vx = live ? __ldcg(a.Fx + e) : 0.f;
-                const float vy = live ? __ldcg(a.Fy + e) : 0.f;
-                const float vz = live ? __ldcg(a.Fz + e) : 0.f;
-                const float bw = a.beta * s[(TF_W + c) * cap + t];
-                a.Fx[e] = fmaf(a.alpha, vx, -bw * xSum);
-                a.Fy[e] = fmaf(a.alpha, vy, -bw * ySum);
-                a.Fz[e] = fmaf(a.alpha, vz, -bw * zSum);
-                atomicOr(&a.mask_new[wd], bit);
-            }
-        }
-        __syncthreads();
-    }
+    // ---- second segment (blades)
+    if (a.plane_lv1[j] == a.plane_lv1[j + 1]) return;
+    if (!blade_levels_tile<THREADS>(a, j, tile, 3 * tile_cells)) blade_levels_global(a, j);
 }
 
 template <int THREADS>
