@@ -163,6 +163,31 @@ int tdlb_reduce_fp64(tdlb_handle h, double* out4);
 /* Make all queued device work complete. */
 int tdlb_synchronize(tdlb_handle h);
 
+/* Replaces: ComputeUnitBase::checkpoint_write(unit_name, RunningParams)
+ * (ComputeUnit.hpp:389-439) with the directory given instead of derived
+ * (DiskOutputTree.h:560-570). Writes, in the reference's layout and names
+ * (DiskOutputTree.h:572-589), <dir>/checkpoint_grid.<id>.<unit>.{Q,F,Nu}
+ * over the ghosted grid (Q: the 18 moments as the reference's Q holds them
+ * between steps -- at the cell for Simple, in the writeMoments places for
+ * Esotwist; ghost cells zero) and <dir>/AllParams.<id>.<unit>.json. <id> is
+ * idi.idj.idk of params_json's ComputeUnitParams (default 0.0.0).
+ * params_json (may be NULL) holds the run's params sections (RunningParams
+ * with the step and angle, ...); missing sections are filled from the
+ * handle. Extension: "StreamingState": {"evenStep"} records the Esotwist
+ * parity, which the reference's checkpoint drops. <dir> is created if
+ * missing (one level). Any storage precision. */
+int tdlb_checkpoint_write(tdlb_handle h, const char* dir, const char* unit_name, const char* params_json);
+
+/* Replaces: ComputeUnitBase::checkpoint_read(dirname, unit_name)
+ * (ComputeUnit.hpp:318-386): reads <dir>/AllParams.0.0.0.<unit>.json and
+ * the Q, F and Nu files. The lattice size must match the handle; the flow
+ * params (nu, cs0, g3, alpha, beta, useLES, initialRho) are taken from the
+ * file as the reference does (:341). Afterwards the state holds moments,
+ * as after tdlb_initialise; Esotwist parity from "StreamingState.evenStep"
+ * (true when absent). A missing or short file is TDLB_EIO (the reference
+ * prints and continues). FP32 storage only. */
+int tdlb_checkpoint_read(tdlb_handle h, const char* dir, const char* unit_name);
+
 /* Step-kernel variant: cells per thread (1, 2 or 4; default 4 = float4
  * traffic). All variants compute identical results. */
 int tdlb_set_cells_per_thread(tdlb_handle h, int v);

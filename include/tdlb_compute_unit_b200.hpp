@@ -85,6 +85,15 @@ public:
     void synchronize() { check(tdlb_synchronize(h_)); }
     tdlb_handle handle() const { return h_; }
 
+    // checkpoint_write / checkpoint_read (ComputeUnit.hpp:318-439); the
+    // directory is passed in, params_json carries the run's params sections.
+    void checkpoint_write(const std::string& dir, const std::string& unit_name, const std::string& params_json = "") {
+        check(tdlb_checkpoint_write(h_, dir.c_str(), unit_name.c_str(), params_json.empty() ? nullptr : params_json.c_str()));
+    }
+    void checkpoint_read(const std::string& dir, const std::string& unit_name) {
+        check(tdlb_checkpoint_read(h_, dir.c_str(), unit_name.c_str()));
+    }
+
     int64_t x = 0, y = 0, z = 0;
 
 private:

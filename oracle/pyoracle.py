@@ -94,6 +94,8 @@ def load(kind: str) -> ctypes.CDLL:
         sig["set_threads"] = (None, [ci])
     else:
         sig["kat_simple_golden"] = (ci, [ci, vp])
+        sig["checkpoint_write"] = (cl, [vp, ctypes.c_char_p, cl, ctypes.c_char_p, cl])
+        sig["checkpoint_read"] = (ci, [vp, ctypes.c_char_p, ctypes.c_char_p])
     for name, (res, args) in sig.items():
         fn = getattr(lib, p + name)
         fn.restype = res
@@ -219,6 +221,19 @@ class CpuLattice:
         out = np.empty((n, 3), np.float64)
         self._fn("get_forcing_sums")(self.h, _ptr(out), n)
         return out
+
+    def checkpoint_write(self, unit: str, step: int) -> str:
+        """The reference's own checkpoint_write (ref only); returns its directory."""
+        buf = ctypes.create_string_buffer(4096)
+        n = self._fn("checkpoint_write")(self.h, unit.encode(), step, buf, len(buf))
+        if n <= 0:
+            raise RuntimeError("reference checkpoint_write failed")
+        return buf.value.decode()
+
+    def checkpoint_read(self, directory: str, unit: str):
+        """The reference's own checkpoint_read (ref only)."""
+        if self._fn("checkpoint_read")(self.h, directory.encode(), unit.encode()) != 0:
+            raise RuntimeError("reference checkpoint_read failed")
 
     def get_o(self) -> np.ndarray:
         """Cells the last forcing() touched (port only; the reference resets O)."""

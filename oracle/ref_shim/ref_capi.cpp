@@ -76,6 +76,7 @@ struct Handle {
     int precision;          // 4 or 8
     int streaming;          // 0 Simple, 1 Esotwist
     void* cu;               // ComputeUnitBase<T,18,IJKL>*
+    std::string tmpdir;     // root of the DiskOutputTree (checkpoints go below it)
 };
 
 template <typename T>
@@ -158,6 +159,28 @@ void readMoments(Base<T>* b, double* out) {
 
 }  // namespace
 
+// checkpoint_write through the reference's own DiskOutputTree
+// (ComputeUnit.hpp:389-439): its params are set as main.cpp:237 sets them,
+// with the checkpoint root and prefix of makeTree(); returns the directory
+// the reference chose (DiskOutputTree.h:560-570).
+template <typename T>
+std::string checkpointWrite(Base<T>* cu, const std::string& tmpdir, const char* unit, long step) {
+    MuteCout mute;
+    GridParams grid;
+    grid.x = cu->xg - 2; grid.y = cu->yg - 2; grid.z = cu->zg - 2;
+    grid.multiStep = 1;
+    RunningParams run;
+    run.step = step;
+    OutputParams out(tmpdir + "/ref_output");
+    CheckpointParams chk;
+    chk.checkpointWriteRootDir = tmpdir;
+    chk.checkpointWriteDirPrefix = "ref";
+    cu->outputTree.setParams(makeCuParams(grid.x, grid.y, grid.z), grid.getJson(), cu->flow.getJson(), run.getJson(),
+                             out.getJson(), chk.getJson());
+    cu->checkpoint_write(unit, run);
+    return cu->outputTree.getCheckpointDirName(run, false);
+}
+
 extern "C" {
 
 typedef FlowC tdlbref_flow;
@@ -167,7 +190,7 @@ void* tdlbref_create(int precision, int streaming, long x, long y, long z,
                      const tdlbref_flow* flow, const char* tmpdir) {
     if ((precision != 4 && precision != 8) || (streaming != 0 && streaming != 1)) return nullptr;
     if (x < 1 || y < 1 || z < 1) return nullptr;
-    Handle* h = new Handle{precision, streaming, nullptr};
+    Handle* h = new Handle{precision, streaming, nullptr, tmpdir ? tmpdir : "/tmp"};
     if (precision == 4) h->cu = create<float>(streaming, x, y, z, flow, tmpdir);
     else h->cu = create<double>(streaming, x, y, z, flow, tmpdir);
     return h;
@@ -328,6 +351,33 @@ int tdlbref_kat_esotwist_read(long x, long y, long z, int even, uint64_t* out) {
                 QVec<unsigned long, QLen::D3Q19> q = AF::read(cu, i, j, k);
                 for (int l = 0; l < 18; l++) out[c * 18 + l] = q.q[l];
             }
+    return 0;
+}
+
+// Checkpoint through the reference's own writer / reader. write returns the
+// directory length (0 on failure) and copies the path into dir_out.
+long tdlbref_checkpoint_write(void* hv, const char* unit, long step, char* dir_out, long cap) {
+    Handle* h = (Handle*)hv;
+    std::string dir;
+    try {
+        if (h->precision == 4) dir = checkpointWrite<float>(as<float>(h), h->tmpdir, unit, step);
+        else dir = checkpointWrite<double>(as<double>(h), h->tmpdir, unit, step);
+    } catch (const std::exception&) {
+        return 0;
+    }
+    if ((long)dir.size() + 1 > cap) return 0;
+    std::memcpy(dir_out, dir.c_str(), dir.size() + 1);
+    return (long)dir.size();
+}
+
+int tdlbref_checkpoint_read(void* hv, const char* dir, const char* unit) {
+    Handle* h = (Handle*)hv;
+    try {
+        MuteCout mute;
+        TDLBREF_DISPATCH(h, cu->checkpoint_read(dir, unit));
+    } catch (const std::exception&) {
+        return -1;
+    }
     return 0;
 }
 

@@ -164,6 +164,8 @@ def load_library() -> ctypes.CDLL:
         "tdlb_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "tdlb_set_cells_per_thread": (i32, [H, i32]),
         "tdlb_reduce_fp64": (i32, [H, vp]),
+        "tdlb_checkpoint_write": (i32, [H, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]),
+        "tdlb_checkpoint_read": (i32, [H, ctypes.c_char_p, ctypes.c_char_p]),
         "tdlb_batch_create": (i32, [ctypes.POINTER(Config), i32, i32, ctypes.POINTER(H)]),
         "tdlb_batch_destroy": (i32, [H]),
         "tdlb_batch_last_error": (ctypes.c_char_p, [H]),
@@ -332,6 +334,17 @@ class ComputeUnit:
         out = np.zeros(4, np.float64)
         self._check(self.lib.tdlb_reduce_fp64(self.h, _p(out)))
         return out
+
+    # ---- checkpoint (ComputeUnit.hpp:318-439) ----
+    def checkpoint_write(self, directory: str, unit_name: str, params=None):
+        """Q/F/Nu + AllParams JSON in the reference's layout under `directory`.
+        `params`: the run's params (dict or JSON text), e.g. its RunningParams."""
+        text = None if params is None else (params if isinstance(params, str) else json.dumps(params))
+        self._check(self.lib.tdlb_checkpoint_write(self.h, directory.encode(), unit_name.encode(),
+                                                   None if text is None else text.encode()))
+
+    def checkpoint_read(self, directory: str, unit_name: str):
+        self._check(self.lib.tdlb_checkpoint_read(self.h, directory.encode(), unit_name.encode()))
 
     def set_cells_per_thread(self, v: int):
         """Step-kernel variant (1, 2 or 4 cells per thread); results are identical."""

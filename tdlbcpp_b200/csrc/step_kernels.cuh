@@ -446,16 +446,10 @@ __global__ void __launch_bounds__(128, 4) k_step_esotwist(Planes Q, float* __res
 // layout. mode: 0 = Simple populations (pull), 1 = moments (own cell),
 // 2 = Esotwist populations (read map, parity `even`), 3 = Esotwist moments.
 template <typename S>
-__global__ void __launch_bounds__(256) k_state_moments(Planes A, Planes M, Dims g, int mode, int even, CollideParams p) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long total = g.rows() * g.nz;
-    if (t >= total) return;
-    const int k = (int)(t % g.nz);
-    const long long row = t / g.nz;
-    const int j = (int)(row % g.ny);
-    const int i = (int)(row / g.ny);
-    const int e = (int)(row * g.kp + k);
-    float q[NQ], m[NQ];
+__device__ __forceinline__ void state_moments18(const Planes& A, const Dims& g, int mode, int even, const CollideParams& p,
+                                                int i, int j, int k, float (&m)[NQ]) {
+    const int e = (int)(((long long)i * g.ny + j) * g.kp + k);
+    float q[NQ];
     if (mode <= 1) {
 #pragma unroll
         for (int d = 0; d < NQ; d++) {
@@ -483,6 +477,20 @@ __global__ void __launch_bounds__(256) k_state_moments(Planes A, Planes M, Dims 
 #pragma unroll
         for (int d = 0; d < NQ; d++) m[d] = q[d];
     }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_state_moments(Planes A, Planes M, Dims g, int mode, int even, CollideParams p) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = g.rows() * g.nz;
+    if (t >= total) return;
+    const int k = (int)(t % g.nz);
+    const long long row = t / g.nz;
+    const int j = (int)(row % g.ny);
+    const int i = (int)(row / g.ny);
+    float m[NQ];
+    state_moments18<S>(A, g, mode, even, p, i, j, k, m);
+    const long long e = row * g.kp + k;
 #pragma unroll
     for (int d = 0; d < NQ; d++) M.p[d][e] = m[d];
 }
