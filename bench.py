@@ -386,6 +386,145 @@ def run_batched(args, rank, world, device):
     }
 
 
+# ---------------------------------------------------------------- serving form
+
+SERVE_EDGES = (48, 64, 96, 128, 192, 256)
+SERVE_SEED = 20261204
+SERVE_RATE = 20.0          # requests per second
+SERVE_TOTAL = 2000
+SERVE_TIP = 0.1
+
+
+def draw_serving_requests(n=SERVE_TOTAL, seed=SERVE_SEED):
+    """The request stream of the serving workload: Poisson arrivals at
+    SERVE_RATE per second; per request, in this order, the exponential gap to
+    its arrival, the edge uniform over SERVE_EDGES, the step count uniform on
+    [500, 5000], Re log-uniform on [1e3, 2e4] and the storage, FP32 or FP16
+    with probability 1/2 each, all from numpy's default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for q in range(n):
+        t += float(rng.exponential(1.0 / SERVE_RATE))
+        edge = int(rng.choice(SERVE_EDGES))
+        steps = int(rng.integers(500, 5001))
+        re = float(np.exp(rng.uniform(np.log(1e3), np.log(2e4))))
+        storage = "fp16" if rng.uniform() < 0.5 else "fp32"
+        out.append({"id": q, "arrival": t, "edge": edge, "steps": steps, "re": re, "storage": storage})
+    return out
+
+
+def plain_fields(tb, edge, re, steps, device):
+    """One request solved alone in the plain FP32 form (the per-request
+    error reference): host-driven rotate / collision / forcing steps."""
+    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=SERVE_TIP, startup_steps=0)
+    nu = tb.nu_from_reynolds(re, SERVE_TIP, rt.blade_outer_radius())
+    cu = tb.ComputeUnit(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0, device=device)
+    d1 = rt.increment(1)
+    cu.attach_rushton(rt, d1, d1, d1)
+    cu.initialise(1.0)
+    cu.forcing_resident(ALPHA, BETA)
+    angle = d1
+    for s in range(2, steps + 2):
+        d = rt.increment(s)
+        angle += d
+        cu.rotate_impeller(angle, d)
+        cu.collision()
+        cu.forcing_resident(ALPHA, BETA)
+    rho, u = cu.read_velocity_density()
+    cu.close()
+    return rho, u
+
+
+def run_serving(args, rank, world, device):
+    """The serving form on a prefix of the seeded request stream: requests
+    are submitted at their arrival times from a host thread; the native
+    server admits, batches and retires them."""
+    import torch
+    import tdlbcpp_b200 as tb
+
+    torch.cuda.set_device(device)
+    reqs = draw_serving_requests()[:args.requests]
+    # per-request error: the two smallest FP16 requests and the smallest FP32 one
+    fp16 = sorted((r for r in reqs if r["storage"] == "fp16"), key=lambda r: r["edge"] ** 3 * r["steps"])[:2]
+    fp32 = sorted((r for r in reqs if r["storage"] == "fp32"), key=lambda r: r["edge"] ** 3 * r["steps"])[:1]
+    checked = {r["id"] for r in fp16 + fp32}
+    server = tb.Server(device=device, max_active=64, chunk_steps=args.chunk)
+    t_start = time.perf_counter()
+
+    def feeder():
+        for r in reqs:
+            delay = r["arrival"] - (time.perf_counter() - t_start)
+            if delay > 0:
+                time.sleep(delay)
+            server.submit(r["id"], r["edge"], SERVE_TIP, r["re"], r["steps"], storage=r["storage"],
+                          fields=r["id"] in checked)
+
+    barrier(world)
+    with ClockSampler(device) as clk:
+        th = threading.Thread(target=feeder)
+        th.start()
+        th.join()
+        server.wait_idle(3600.0)
+    results = server.poll(len(reqs) + 8)
+    st = server.stats()
+    server.close()
+    bad = [r for r in results if r["status"] != 0]
+    if bad:
+        raise RuntimeError(f"{len(bad)} serving requests failed, first status {bad[0]['status']}")
+    lat = np.array([r["t_done"] - r["t_submit"] for r in results])
+    t0 = min(r["t_submit"] for r in results)
+    t1 = max(r["t_done"] for r in results)
+    lu = float(sum(r["cells"] * r["steps"] for r in results))
+    errors = []
+    for r in results:
+        if r["id"] not in checked:
+            continue
+        q = next(x for x in reqs if x["id"] == r["id"])
+        rho0, u0 = plain_fields(tb, q["edge"], q["re"], q["steps"], device)
+        f = r["fields"]
+        u = np.stack([f["ux"], f["uy"], f["uz"]], axis=-1)
+        eu = float(np.linalg.norm((u - u0).ravel()) / max(np.linalg.norm(u0.ravel()), 1e-300))
+        er = float(np.linalg.norm((f["rho"] - rho0).ravel()) / np.linalg.norm(rho0.ravel()))
+        errors.append({"id": q["id"], "edge": q["edge"], "steps": q["steps"], "storage": q["storage"],
+                       "u_rel_l2_vs_plain_fp32": eu, "rho_rel_l2_vs_plain_fp32": er})
+    bytes_done = sum(r["cells"] * r["steps"] * (152 if next(x for x in reqs if x["id"] == r["id"])["storage"] == "fp32"
+                                                 else 80) for r in results)
+    return {
+        "value_mlups": world * lu / (t1 - t0) / 1e6,
+        "busy_mlups": st["lattice_updates"] / st["busy_s"] / 1e6 if st["busy_s"] > 0 else None,
+        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+        "mean_s": float(lat.mean()), "span_s": t1 - t0, "lattice_updates": lu,
+        "achieved_gbs": bytes_done / st["busy_s"] / 1e9 if st["busy_s"] > 0 else None,
+        "chunks": st["chunks"], "requests": len(results), "errors": errors, "clocks": clk.summary(),
+        "ms_per_step": None,
+    }
+
+
+def report_serving(args, rank, world, local, config):
+    res = run_serving(args, rank, world, local)
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peak()
+    config = dict(config, p50_latency_s=res["p50_s"], p99_latency_s=res["p99_s"], mean_latency_s=res["mean_s"],
+                  span_s=res["span_s"], device_busy_mlups=res["busy_mlups"], chunks=res["chunks"],
+                  per_request_error=res["errors"])
+    line = {
+        "metric": "MLUPS", "value": res["value_mlups"], "unit": "MLUPS", "n_gpus": world,
+        "steps": int(res["lattice_updates"]), "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32/fp16", "data": "synthetic", "config": config,
+        "roofline": {"bound": "hbm", "achieved": res["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": None if res["achieved_gbs"] is None else res["achieved_gbs"] / peak,
+                     "peak_kind": peak_kind, "kernel": "whole serving step (stepping wall time)",
+                     "bytes_per_cell": "152 (fp32) / 80 (fp16)", "traffic": None},
+        "e2e": {"value": res["value_mlups"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "submit to result through the public server API, wall clock"},
+        "latency_p50_s": res["p50_s"], "latency_p99_s": res["p99_s"],
+        "clocks": res["clocks"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- reference arm
 
 def slab_markers(tb, rt, j0, height, angle, dth):
@@ -520,13 +659,22 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["simple", "esotwist", "batched"], default="simple")
+    ap.add_argument("--workload", choices=["simple", "esotwist", "batched", "serving"], default="simple")
+    ap.add_argument("--requests", type=int, default=64, help="serving: prefix of the request stream to serve")
+    ap.add_argument("--chunk", type=int, default=100, help="serving: steps per batched chunk")
     ap.add_argument("--edge", type=int, default=EDGE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3   # timing rule: at least 3 warm-up steps
-    if args.workload == "batched":
+    if args.workload == "serving":
+        workload = f"serving-{args.requests}-of-{SERVE_TOTAL}-requests"
+        config = {"workload": workload, "requests": args.requests, "stream_total": SERVE_TOTAL, "seed": SERVE_SEED,
+                  "rate_per_s": SERVE_RATE, "edges": list(SERVE_EDGES), "steps": [500, 5000], "re": [1e3, 2e4],
+                  "storage": "fp32/fp16 50/50", "tip_speed": SERVE_TIP, "chunk_steps": args.chunk,
+                  "sample": f"the first {args.requests} requests of the seeded {SERVE_TOTAL}-request stream",
+                  "l2": "lattices > L2 (no flush needed)"}
+    elif args.workload == "batched":
         tanks = draw_batched_tanks()
         workload = f"batched-{len(tanks)}-tanks-simple-fp32-les"
         config = {"workload": workload, "tanks": len(tanks), "edges": [t[0] for t in tanks],
@@ -560,6 +708,8 @@ def main():
 
     if args.workload == "batched":
         return report_batched(args, rank, world, local, config)
+    if args.workload == "serving":
+        return report_serving(args, rank, world, local, config)
 
     res = run_ours(args, rank, world, local)
     if rank != 0:

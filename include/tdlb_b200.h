@@ -90,6 +90,11 @@ int tdlb_create(const char* params_json, int device, tdlb_handle* out);
 /* Same, from a filled tdlb_config (nu used as given). */
 int tdlb_create_config(const tdlb_config* cfg, int device, tdlb_handle* out);
 
+/* Device bytes a lattice of this config takes (fields, flags, and the marker
+ * buffers of a tank-wall geometry; an upper estimate). No counterpart in the
+ * reference (its checkEnoughMemory only compares, ComputeUnitGpu.hpp:15-30). */
+int tdlb_lattice_bytes(const tdlb_config* cfg, int64_t* bytes);
+
 /* Replaces: ~ComputeUnitBase / freeMemory (ComputeUnit.hpp:150-154). */
 int tdlb_destroy(tdlb_handle h);
 
@@ -285,10 +290,16 @@ int tdlb_schedule_levels(const tdlb_marker* markers, size_t n, int64_t x, int64_
 typedef struct tdlb_batch_s* tdlb_batch;
 
 int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* out);
+/* A batch with no tanks yet, for tanks added later (tdlb_batch_add). */
+int tdlb_batch_create_empty(int device, int streaming, int storage, tdlb_batch* out);
 int tdlb_batch_destroy(tdlb_batch b);
 /* Last error of b; of the calling thread's last failed create if b is NULL. */
 const char* tdlb_batch_last_error(tdlb_batch b);
 int tdlb_batch_size(tdlb_batch b, int* n);
+/* A tank joins (index: its position) or leaves the batch between runs; a
+ * removed tank's handle is destroyed and later tanks move down by one. */
+int tdlb_batch_add(tdlb_batch b, const tdlb_config* cfg, int* index);
+int tdlb_batch_remove(tdlb_batch b, int index);
 int tdlb_batch_tank(tdlb_batch b, int t, tdlb_handle* out);
 /* Shape of the fused batched launch: cells per thread (1, 2, 4; 16-bit
  * storage 1 or 4), threads per block (128 or 256), resident blocks per SM
@@ -312,6 +323,65 @@ int tdlb_batch_run_eager(tdlb_batch b, int steps, float alpha, float beta);
 int tdlb_batch_kernel_launches(tdlb_batch b, long long* n);
 int tdlb_batch_synchronize(tdlb_batch b);
 int tdlb_batch_get_stream(tdlb_batch b, void** stream);
+
+/* ---- serving form: a request loop over resident, batched tanks ----
+ * No counterpart in the reference. A server runs one worker thread that
+ * admits submitted requests in arrival order while a slot is free and the
+ * tank's device bytes (tdlb_lattice_bytes) fit the free HBM (less 1 GiB)
+ * and the budget; builds each admitted tank (a Rushton turbine filling the
+ * lattice, tip speed and Re as requested, LES with Cs = 0.1, rho = 1),
+ * forces it once (main.cpp:305) and adds it to the resident batch of its
+ * precision and scheme; advances every resident tank in chunks of
+ * min(chunk_steps, smallest remaining step count) with alpha = 0.97,
+ * beta = 1.9; and retires finished tanks, freeing their memory. A tank's
+ * result does not depend on what else is resident. */
+typedef struct tdlb_server_s* tdlb_server;
+
+typedef struct tdlb_request {
+    int64_t id;               /* caller's tag, returned in the result */
+    int64_t x, y, z;          /* lattice; the tank diameter is x */
+    double tip_speed;         /* impeller tip speed (lattice units) */
+    double reynolds;          /* nu from calcNuAndRe_m (FlowParams.hpp:65-70) */
+    int64_t steps;
+    int32_t storage;          /* TDLB_STORAGE_* */
+    int32_t streaming;        /* TDLB_STREAMING_* */
+    int32_t les;              /* Smagorinsky LES on/off */
+    int32_t pad;
+    float* out_rho;           /* optional host buffers (x*y*z each), filled */
+    float* out_ux;            /* at completion; must stay valid until then */
+    float* out_uy;
+    float* out_uz;
+} tdlb_request;
+
+typedef struct tdlb_result {
+    int64_t id;
+    int32_t status;           /* TDLB_OK, or why the request failed */
+    int32_t pad;
+    double t_submit, t_admit, t_done;   /* seconds since the server started */
+    int64_t cells, steps;
+    double mass, momentum[3];           /* FP64 sums at the end (tdlb_reduce_fp64) */
+    double force[3], torque;            /* FP64 impeller load of the last pass */
+    double power_number;                /* |torque * omega| / (N^3 D^5), N = omega / 2 pi, rho = 1 */
+} tdlb_result;
+
+typedef struct tdlb_server_stats {
+    int64_t submitted, completed, queued, active, admitted, chunks, bytes_in_use;
+    double lattice_updates;   /* cell updates done so far */
+    double busy_s;            /* wall time spent stepping */
+    double elapsed_s;         /* since the server started */
+} tdlb_server_stats;
+
+/* hbm_budget_bytes: 0 = free HBM only; max_active: resident tank slots. */
+int tdlb_server_create(int device, int64_t hbm_budget_bytes, int max_active, int chunk_steps, tdlb_server* out);
+int tdlb_server_destroy(tdlb_server s);   /* unfinished requests end with TDLB_ESTATE */
+const char* tdlb_server_last_error(tdlb_server s);
+/* Thread-safe; the request is copied (its output buffers are not). */
+int tdlb_server_submit(tdlb_server s, const tdlb_request* r);
+/* Up to cap finished results, in completion order; n: how many. */
+int tdlb_server_poll(tdlb_server s, tdlb_result* out, int cap, int* n);
+/* Wait until every submitted request has finished (TDLB_ESTATE on timeout). */
+int tdlb_server_wait_idle(tdlb_server s, double timeout_s);
+int tdlb_server_get_stats(tdlb_server s, tdlb_server_stats* st);
 
 /* ---- known-answer-test support (integer-coded transport) ----
  * Raw population state: for Simple the current buffer, for Esotwist the

@@ -19,7 +19,7 @@ from typing import Optional
 import numpy as np
 
 __all__ = [
-    "ComputeUnit", "Batch", "TdlbError", "MARKER_DTYPE", "library_path", "load_library", "make_config",
+    "ComputeUnit", "Batch", "Server", "TdlbError", "MARKER_DTYPE", "library_path", "load_library", "make_config",
     "STREAMING_SIMPLE", "STREAMING_ESOTWIST",
 ]
 
@@ -86,6 +86,39 @@ class Rushton(ctypes.Structure):
         ("n_blades", ctypes.c_int32), ("n_baffles", ctypes.c_int32),
         ("baffle_width", ctypes.c_double), ("wall_inset", ctypes.c_double), ("tip_speed", ctypes.c_double),
         ("startup_steps", ctypes.c_int64),
+    ]
+
+
+class Request(ctypes.Structure):
+    """tdlb_request: one tank solve submitted to a Server."""
+
+    _fields_ = [
+        ("id", ctypes.c_int64), ("x", ctypes.c_int64), ("y", ctypes.c_int64), ("z", ctypes.c_int64),
+        ("tip_speed", ctypes.c_double), ("reynolds", ctypes.c_double), ("steps", ctypes.c_int64),
+        ("storage", ctypes.c_int32), ("streaming", ctypes.c_int32), ("les", ctypes.c_int32), ("pad", ctypes.c_int32),
+        ("out_rho", ctypes.c_void_p), ("out_ux", ctypes.c_void_p), ("out_uy", ctypes.c_void_p),
+        ("out_uz", ctypes.c_void_p),
+    ]
+
+
+class Result(ctypes.Structure):
+    """tdlb_result: a finished request's timing and FP64 diagnostics."""
+
+    _fields_ = [
+        ("id", ctypes.c_int64), ("status", ctypes.c_int32), ("pad", ctypes.c_int32),
+        ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+        ("cells", ctypes.c_int64), ("steps", ctypes.c_int64), ("mass", ctypes.c_double),
+        ("momentum", ctypes.c_double * 3), ("force", ctypes.c_double * 3), ("torque", ctypes.c_double),
+        ("power_number", ctypes.c_double),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("queued", ctypes.c_int64),
+        ("active", ctypes.c_int64), ("admitted", ctypes.c_int64), ("chunks", ctypes.c_int64),
+        ("bytes_in_use", ctypes.c_int64), ("lattice_updates", ctypes.c_double), ("busy_s", ctypes.c_double),
+        ("elapsed_s", ctypes.c_double),
     ]
 
 
@@ -171,12 +204,23 @@ def load_library() -> ctypes.CDLL:
         "tdlb_batch_last_error": (ctypes.c_char_p, [H]),
         "tdlb_batch_size": (i32, [H, ctypes.POINTER(i32)]),
         "tdlb_batch_tank": (i32, [H, i32, ctypes.POINTER(H)]),
+        "tdlb_batch_add": (i32, [H, ctypes.POINTER(Config), ctypes.POINTER(i32)]),
+        "tdlb_batch_remove": (i32, [H, i32]),
         "tdlb_batch_set_shape": (i32, [H, i32, i32, i32]),
         "tdlb_batch_get_shape": (i32, [H, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
         "tdlb_batch_autotune": (i32, [H, i32, ctypes.POINTER(ctypes.c_double)]),
         "tdlb_batch_run": (i32, [H, i32, f32, f32]),
         "tdlb_batch_run_eager": (i32, [H, i32, f32, f32]),
         "tdlb_batch_synchronize": (i32, [H]),
+        "tdlb_batch_create_empty": (i32, [i32, i32, i32, ctypes.POINTER(H)]),
+        "tdlb_lattice_bytes": (i32, [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_int64)]),
+        "tdlb_server_create": (i32, [i32, ctypes.c_int64, i32, i32, ctypes.POINTER(H)]),
+        "tdlb_server_destroy": (i32, [H]),
+        "tdlb_server_last_error": (ctypes.c_char_p, [H]),
+        "tdlb_server_submit": (i32, [H, ctypes.POINTER(Request)]),
+        "tdlb_server_poll": (i32, [H, ctypes.POINTER(Result), i32, ctypes.POINTER(i32)]),
+        "tdlb_server_wait_idle": (i32, [H, ctypes.c_double]),
+        "tdlb_server_get_stats": (i32, [H, ctypes.POINTER(ServerStats)]),
         "tdlb_batch_kernel_launches": (i32, [H, ctypes.POINTER(ctypes.c_longlong)]),
         "tdlb_batch_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
     }
@@ -471,6 +515,22 @@ class Batch:
     def ncell(self) -> int:
         return sum(cu.ncell for cu in self.tanks)
 
+    def add(self, config) -> "ComputeUnit":
+        """A new tank joins the batch (keyword dict or Config); returns its view."""
+        cfg = config if isinstance(config, Config) else make_config(**config)
+        idx = ctypes.c_int()
+        self._check(self.lib.tdlb_batch_add(self.h, ctypes.byref(cfg), ctypes.byref(idx)))
+        th = ctypes.c_void_p()
+        self._check(self.lib.tdlb_batch_tank(self.h, idx.value, ctypes.byref(th)))
+        cu = ComputeUnit._borrowed(self.lib, th)
+        self.tanks.append(cu)
+        return cu
+
+    def remove(self, index: int):
+        """Tank `index` leaves the batch (its handle is destroyed)."""
+        self._check(self.lib.tdlb_batch_remove(self.h, index))
+        self.tanks.pop(index).h = None
+
     def set_shape(self, cells_per_thread: int, threads: int, blocks_per_sm: int):
         self._check(self.lib.tdlb_batch_set_shape(self.h, cells_per_thread, threads, blocks_per_sm))
 
@@ -500,6 +560,92 @@ class Batch:
         s = ctypes.c_void_p()
         self._check(self.lib.tdlb_batch_get_stream(self.h, ctypes.byref(s)))
         return s.value or 0
+
+
+class Server:
+    """The serving form (``tdlb_server_*``): submit tank solves from any
+    thread; a native worker admits them by free HBM, keeps their lattices
+    resident, batches them continuously and returns FP64 diagnostics (and,
+    on request, the final density and velocity fields)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, max_active: int = 64, chunk_steps: int = 100):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.tdlb_server_create(device, hbm_budget, max_active, chunk_steps, ctypes.byref(h))
+        if rc != 0:
+            raise TdlbError(rc, self.lib.tdlb_server_last_error(None).decode())
+        self.h = h
+        self._fields = {}
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise TdlbError(rc, self.lib.tdlb_server_last_error(self.h).decode())
+
+    def submit(self, rid: int, edge, tip_speed: float, reynolds: float, steps: int, storage: str = "fp32",
+               streaming: str = "Simple", les: bool = True, fields: bool = False):
+        x, y, z = (edge, edge, edge) if isinstance(edge, int) else edge
+        r = Request()
+        r.id, r.x, r.y, r.z = rid, x, y, z
+        r.tip_speed, r.reynolds, r.steps = tip_speed, reynolds, steps
+        r.storage = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16}[storage]
+        r.streaming = STREAMING_SIMPLE if streaming == "Simple" else STREAMING_ESOTWIST
+        r.les = int(les)
+        if fields:
+            out = {"rho": np.zeros((x, y, z), np.float32), "ux": np.zeros((x, y, z), np.float32),
+                   "uy": np.zeros((x, y, z), np.float32), "uz": np.zeros((x, y, z), np.float32)}
+            r.out_rho, r.out_ux, r.out_uy, r.out_uz = (out[k].ctypes.data for k in ("rho", "ux", "uy", "uz"))
+            self._fields[rid] = out
+        self._check(self.lib.tdlb_server_submit(self.h, ctypes.byref(r)))
+
+    def poll(self, cap: int = 256):
+        buf = (Result * cap)()
+        n = ctypes.c_int()
+        self._check(self.lib.tdlb_server_poll(self.h, buf, cap, ctypes.byref(n)))
+        out = []
+        for q in range(n.value):
+            r = buf[q]
+            d = {name: getattr(r, name) for name, _ in Result._fields_ if name != "pad"}
+            d["momentum"], d["force"] = list(r.momentum), list(r.force)
+            if r.id in self._fields:
+                d["fields"] = self._fields.pop(r.id)
+            out.append(d)
+        return out
+
+    def wait_idle(self, timeout_s: float = 3600.0):
+        self._check(self.lib.tdlb_server_wait_idle(self.h, timeout_s))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        self._check(self.lib.tdlb_server_get_stats(self.h, ctypes.byref(st)))
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tdlb_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def lattice_bytes(x: int, y: int, z: int, storage: str = "fp32", streaming: str = "Simple") -> int:
+    """Device bytes of a lattice (tdlb_lattice_bytes)."""
+    lib = load_library()
+    cfg = make_config(x=x, y=y, z=z, storage=storage, streaming=streaming)
+    b = ctypes.c_int64()
+    rc = lib.tdlb_lattice_bytes(ctypes.byref(cfg), ctypes.byref(b))
+    if rc != 0:
+        raise TdlbError(rc, "bad lattice size")
+    return b.value
 
 
 class RushtonTurbine:

@@ -147,7 +147,11 @@ struct WorkList {
 
 struct tdlb_batch_s {
     int device = 0;
+    int storage = TDLB_STORAGE_FP32;   // shared by every tank
+    int streaming = TDLB_STREAMING_SIMPLE;
     std::vector<tdlb_lattice*> tanks;
+    int view_cap = 0;                  // tanks the per-tank device arrays hold
+    bool members_changed = true;       // work lists and arrays must follow the tank list
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;       // large-plane spreads
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -199,8 +203,8 @@ int bguard(tdlb_batch_s* b, F&& fn) {
     }
 }
 
-int storage_of(const tdlb_batch_s* b) { return b->tanks[0]->cfg.storage; }
-bool eso_of(const tdlb_batch_s* b) { return b->tanks[0]->cfg.streaming == TDLB_STREAMING_ESOTWIST; }
+int storage_of(const tdlb_batch_s* b) { return b->storage; }
+bool eso_of(const tdlb_batch_s* b) { return b->streaming == TDLB_STREAMING_ESOTWIST; }
 
 // Upload `items` into `w` (the stream is idle: callers synchronise first).
 void put(WorkList& w, const std::vector<int2>& items) {
@@ -407,6 +411,63 @@ void finish_tables(tdlb_batch_s* b, int steps) {
     }
 }
 
+// Per-tank device arrays for at least the current number of tanks.
+void ensure_capacity(tdlb_batch_s* b) {
+    const int n = (int)b->tanks.size();
+    if (n <= b->view_cap) return;
+    const int cap = std::max(n, 2 * b->view_cap);
+    TDLB_BCK(cudaStreamSynchronize(b->stream));
+    cudaFree(b->d_steps);
+    cudaFree(b->d_ibm);
+    cudaFree(b->d_rotors);
+    b->d_steps = nullptr;
+    b->d_ibm = nullptr;
+    b->d_rotors = nullptr;
+    b->view_cap = 0;
+    TDLB_BCK(cudaMalloc(&b->d_steps, (size_t)2 * cap * sizeof(TankStep)));
+    TDLB_BCK(cudaMalloc(&b->d_ibm, (size_t)2 * cap * sizeof(tdlb::IbmArgs)));
+    TDLB_BCK(cudaMalloc(&b->d_rotors, (size_t)cap * sizeof(TankRotor)));
+    b->view_cap = cap;
+}
+
+// After tanks joined or left: arrays, fused work list and (through the
+// generation check) the immersed-boundary lists follow the new tank list.
+void sync_members(tdlb_batch_s* b) {
+    if (!b->members_changed) return;
+    ensure_capacity(b);
+    build_work(b);
+    for (auto& g : b->ibm_gen) g = ~0u;
+    b->members_changed = false;
+}
+
+tdlb_lattice* add_tank(tdlb_batch_s* b, const tdlb_config& cfg) {
+    if (cfg.streaming != b->streaming || cfg.storage != b->storage)
+        throw BFail{TDLB_EINVAL, "all tanks of a batch share one streaming scheme and one storage precision"};
+    tdlb_handle h = nullptr;
+    const int rc = tdlb_create_config(&cfg, b->device, &h);
+    if (rc != TDLB_OK) throw BFail{rc, std::string("tank: ") + tdlb_last_error(nullptr)};
+    tdlb_rt::borrow_stream(h, b->stream);
+    h->vec = b->vec;
+    b->tanks.push_back(h);
+    b->d_table.push_back(nullptr);
+    b->table_cap.push_back(0);
+    b->ibm_gen.push_back(~0u);
+    b->members_changed = true;
+    return h;
+}
+
+void remove_tank(tdlb_batch_s* b, int t) {
+    if (t < 0 || t >= (int)b->tanks.size()) throw BFail{TDLB_EINVAL, "tank index out of range"};
+    TDLB_BCK(cudaStreamSynchronize(b->stream));
+    tdlb_destroy(b->tanks[(size_t)t]);
+    cudaFree(b->d_table[(size_t)t]);
+    b->tanks.erase(b->tanks.begin() + t);
+    b->d_table.erase(b->d_table.begin() + t);
+    b->table_cap.erase(b->table_cap.begin() + t);
+    b->ibm_gen.erase(b->ibm_gen.begin() + t);
+    b->members_changed = true;
+}
+
 void check_ready(tdlb_batch_s* b) {
     for (tdlb_lattice* h : b->tanks)
         if (!h->initialised) throw BFail{TDLB_ESTATE, "every tank must be initialised first"};
@@ -416,8 +477,10 @@ void check_ready(tdlb_batch_s* b) {
 // moments (right after initialise) runs eagerly: its views differ from the
 // repeating pair's.
 void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
+    if (b->tanks.empty()) return;
     check_ready(b);
     TDLB_BCK(cudaStreamSynchronize(b->stream));   // the previous run may still read the tables and lists
+    sync_members(b);
     build_ibm_work(b);
     build_tables(b, steps);
     TDLB_BCK(cudaMemsetAsync(b->d_step, 0, sizeof(int), b->stream));
@@ -503,30 +566,18 @@ int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* ou
     *out = nullptr;
     auto* b = new tdlb_batch_s();
     b->device = device;
+    b->storage = cfgs[0].storage;
+    b->streaming = cfgs[0].streaming;
+    b->vec = cfgs[0].streaming == TDLB_STREAMING_SIMPLE ? 1 : 4;
     try {
-        for (int t = 0; t < n; t++) {
-            if (cfgs[t].streaming != cfgs[0].streaming || cfgs[t].storage != cfgs[0].storage)
-                throw BFail{TDLB_EINVAL, "all tanks of a batch share one streaming scheme and one storage precision"};
-            tdlb_handle h = nullptr;
-            const int rc = tdlb_create_config(&cfgs[t], device, &h);
-            if (rc != TDLB_OK) throw BFail{rc, std::string("tank ") + std::to_string(t) + ": " + tdlb_last_error(nullptr)};
-            b->tanks.push_back(h);
-        }
         TDLB_BCK(cudaSetDevice(device));
         TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
         TDLB_BCK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
         TDLB_BCK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
         TDLB_BCK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
-        for (tdlb_lattice* h : b->tanks) tdlb_rt::borrow_stream(h, b->stream);
-        TDLB_BCK(cudaMalloc(&b->d_steps, (size_t)2 * n * sizeof(TankStep)));
-        TDLB_BCK(cudaMalloc(&b->d_ibm, (size_t)2 * n * sizeof(tdlb::IbmArgs)));
-        TDLB_BCK(cudaMalloc(&b->d_rotors, (size_t)n * sizeof(TankRotor)));
         TDLB_BCK(cudaMalloc(&b->d_step, sizeof(int)));
-        b->d_table.assign((size_t)n, nullptr);
-        b->table_cap.assign((size_t)n, 0);
-        b->ibm_gen.assign((size_t)n, ~0u);
-        b->vec = cfgs[0].streaming == TDLB_STREAMING_SIMPLE ? 1 : 4;
-        build_work(b);
+        for (int t = 0; t < n; t++) add_tank(b, cfgs[t]);
+        sync_members(b);
     } catch (const BFail& f) {
         g_batch_create_error = f.msg;
         release(b);
@@ -535,6 +586,47 @@ int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* ou
     }
     *out = b;
     return TDLB_OK;
+}
+
+int tdlb_batch_create_empty(int device, int streaming, int storage, tdlb_batch* out) {
+    if (!out || (streaming != TDLB_STREAMING_SIMPLE && streaming != TDLB_STREAMING_ESOTWIST) ||
+        (storage != TDLB_STORAGE_FP32 && storage != TDLB_STORAGE_FP16 && storage != TDLB_STORAGE_BF16)) {
+        g_batch_create_error = "bad arguments";
+        return TDLB_EINVAL;
+    }
+    *out = nullptr;
+    auto* b = new tdlb_batch_s();
+    b->device = device;
+    b->storage = storage;
+    b->streaming = streaming;
+    b->vec = streaming == TDLB_STREAMING_SIMPLE ? 1 : 4;
+    try {
+        TDLB_BCK(cudaSetDevice(device));
+        TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        TDLB_BCK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+        TDLB_BCK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        TDLB_BCK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+        TDLB_BCK(cudaMalloc(&b->d_step, sizeof(int)));
+    } catch (const BFail& f) {
+        g_batch_create_error = f.msg;
+        release(b);
+        delete b;
+        return f.code;
+    }
+    *out = b;
+    return TDLB_OK;
+}
+
+int tdlb_batch_add(tdlb_batch b, const tdlb_config* cfg, int* index) {
+    return bguard(b, [&] {
+        if (!cfg) throw BFail{TDLB_EINVAL, "cfg is NULL"};
+        add_tank(b, *cfg);
+        if (index) *index = (int)b->tanks.size() - 1;
+    });
+}
+
+int tdlb_batch_remove(tdlb_batch b, int index) {
+    return bguard(b, [&] { remove_tank(b, index); });
 }
 
 int tdlb_batch_destroy(tdlb_batch b) {
@@ -589,7 +681,9 @@ int tdlb_batch_get_shape(tdlb_batch b, int* cells_per_thread, int* threads, int*
 // the next step's view, so they change the fields; callers initialise again.
 int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms) {
     return bguard(b, [&] {
+        if (b->tanks.empty()) throw BFail{TDLB_ESTATE, "the batch has no tanks"};
         check_ready(b);
+        sync_members(b);
         if (trials < 1) trials = 3;
         struct Cand { int v, nt, bps; };
         std::vector<Cand> cands;

@@ -534,6 +534,20 @@ int tdlb_create(const char* params_json, int device, tdlb_handle* out) {
     }
 }
 
+int tdlb_lattice_bytes(const tdlb_config* c, int64_t* bytes) {
+    if (!c || !bytes || c->x < 1 || c->y < 1 || c->z < 1) return TDLB_EINVAL;
+    const long long kp = round_up(c->z, 16), kw = (kp + 31) / 32;
+    const long long plane = round_up(c->x * c->y * kp, 64);
+    const long long mask_words = round_up(c->x * c->y * kw, 64);
+    const long long esz = c->storage == TDLB_STORAGE_FP32 ? 4 : 2;
+    const long long pops = (long long)tdlb::NQ * plane * esz * (c->streaming == TDLB_STREAMING_SIMPLE ? 2 : 1);
+    // fields, flags, and the marker buffers of a tank-wall geometry
+    // (about 8 markers per (i, j) column at most, 256 bytes each with
+    // their schedule, stencil-cell and per-pass data)
+    *bytes = pops + 4 * plane * 4 + 2 * mask_words * 4 + 8 * c->x * c->y * 256;
+    return TDLB_OK;
+}
+
 int tdlb_destroy(tdlb_handle h) {
     if (!h) return TDLB_EINVAL;
     release(h);
