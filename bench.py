@@ -219,6 +219,7 @@ def run_ours(args, rank, world, device):
     w1 = time.perf_counter()
     barrier(world)
     e2e_s = max_over_ranks(w1 - w0, world)
+    red = cu.reduce_fp64()
     cu.close()
 
     result = {
@@ -234,6 +235,8 @@ def run_ours(args, rank, world, device):
         "n_rot": n_rot,
         "nu": nu,
         "load": load_np.tolist(),
+        "fields_finite": bool(np.isfinite(red).all() and np.isfinite(load_np).all()),
+        "mass_drift": float(red[0] / cells - 1.0),
     }
     return result
 
@@ -259,14 +262,14 @@ def draw_batched_tanks(n=BATCH_TANKS, seed=BATCH_SEED):
     return out
 
 
-def batched_configs(tb, tanks, storage="fp32"):
+def batched_configs(tb, tanks, storage="fp32", streaming="Esotwist"):
     rts, cfgs = [], []
     for edge, tip, re in tanks:
         rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=tip, startup_steps=0)
         nu = tb.nu_from_reynolds(re, tip, rt.blade_outer_radius())
         rts.append(rt)
         cfgs.append(dict(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0,
-                         streaming="Simple", storage=storage))
+                         streaming=streaming, storage=storage))
     return rts, cfgs
 
 
@@ -336,6 +339,7 @@ def run_batched(args, rank, world, device):
             cu.impeller_load(load[t])
     b.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - w0, world)
+    finite = bool(np.isfinite(load).all())
     b.close()
 
     # the same tanks in the plain form, one after another
@@ -383,6 +387,7 @@ def run_batched(args, rank, world, device):
         "launches": launches,
         "clocks": clk.summary(),
         "tanks": len(tanks),
+        "fields_finite": finite,
     }
 
 
@@ -393,6 +398,9 @@ SERVE_SEED = 20261204
 SERVE_RATE = 20.0          # requests per second
 SERVE_TOTAL = 2000
 SERVE_TIP = 0.1
+# Esotwist (periodic in the reference): the reference's Simple wall rule lets
+# small tanks diverge after a few hundred steps, Esotwist tanks stay finite
+SERVE_STREAMING = "Esotwist"
 
 
 def draw_serving_requests(n=SERVE_TOTAL, seed=SERVE_SEED):
@@ -418,7 +426,8 @@ def plain_fields(tb, edge, re, steps, device):
     error reference): host-driven rotate / collision / forcing steps."""
     rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=SERVE_TIP, startup_steps=0)
     nu = tb.nu_from_reynolds(re, SERVE_TIP, rt.blade_outer_radius())
-    cu = tb.ComputeUnit(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0, device=device)
+    cu = tb.ComputeUnit(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0, device=device,
+                        streaming=SERVE_STREAMING)
     d1 = rt.increment(1)
     cu.attach_rushton(rt, d1, d1, d1)
     cu.initialise(1.0)
@@ -457,7 +466,7 @@ def run_serving(args, rank, world, device):
             if delay > 0:
                 time.sleep(delay)
             server.submit(r["id"], r["edge"], SERVE_TIP, r["re"], r["steps"], storage=r["storage"],
-                          fields=r["id"] in checked)
+                          streaming=SERVE_STREAMING, fields=r["id"] in checked)
 
     barrier(world)
     with ClockSampler(device) as clk:
@@ -467,10 +476,11 @@ def run_serving(args, rank, world, device):
         server.wait_idle(3600.0)
     results = server.poll(len(reqs) + 8)
     st = server.stats()
+    why = server.lib.tdlb_server_last_error(server.h).decode()
     server.close()
     bad = [r for r in results if r["status"] != 0]
     if bad:
-        raise RuntimeError(f"{len(bad)} serving requests failed, first status {bad[0]['status']}")
+        raise RuntimeError(f"{len(bad)} serving requests failed, first status {bad[0]['status']}: {why}")
     lat = np.array([r["t_done"] - r["t_submit"] for r in results])
     t0 = min(r["t_submit"] for r in results)
     t1 = max(r["t_done"] for r in results)
@@ -644,6 +654,7 @@ def report_batched(args, rank, world, local, config):
                 "d2h_bytes_per_step": res["d2h"], "steps": res["e2e_steps"]},
         "gpu_launches": res["launches"],
         "clocks": res["clocks"],
+        "fields_finite": res["fields_finite"],
     }
     if world == 1 and not args.no_cpu_baseline:
         r = reference_sample(1, 0, host_threads())
@@ -672,15 +683,16 @@ def main():
         config = {"workload": workload, "requests": args.requests, "stream_total": SERVE_TOTAL, "seed": SERVE_SEED,
                   "rate_per_s": SERVE_RATE, "edges": list(SERVE_EDGES), "steps": [500, 5000], "re": [1e3, 2e4],
                   "storage": "fp32/fp16 50/50", "tip_speed": SERVE_TIP, "chunk_steps": args.chunk,
+                  "streaming": SERVE_STREAMING,
                   "sample": f"the first {args.requests} requests of the seeded {SERVE_TOTAL}-request stream",
                   "l2": "lattices > L2 (no flush needed)"}
     elif args.workload == "batched":
         tanks = draw_batched_tanks()
-        workload = f"batched-{len(tanks)}-tanks-simple-fp32-les"
+        workload = f"batched-{len(tanks)}-tanks-esotwist-fp32-les"
         config = {"workload": workload, "tanks": len(tanks), "edges": [t[0] for t in tanks],
                   "cells": sum(t[0] ** 3 for t in tanks), "seed": BATCH_SEED,
                   "draw": "edge U{32,48,64,96,128}, tip U[0.05,0.12], Re log-U[1e3,2e4] per tank, in that order",
-                  "streaming": "Simple", "collision": "EgglesSomers+LES(cs0=0.1)", "ibm": "Rushton turbine, rotating",
+                  "streaming": "Esotwist", "collision": "EgglesSomers+LES(cs0=0.1)", "ibm": "Rushton turbine, rotating",
                   "l2": "lattices > L2 every step (no flush needed)"}
     else:
         workload = f"rushton-{args.edge}^3-{args.workload}-fp32-les"
@@ -732,6 +744,8 @@ def main():
         "gpu_launches": 4 * args.steps,
         "clocks": res["clocks"],
         "markers": res["n_markers"],
+        "fields_finite": res["fields_finite"],
+        "mass_drift": res["mass_drift"],
     }
     if world == 1 and not args.no_cpu_baseline:
         r = reference_sample(1, 0, host_threads())

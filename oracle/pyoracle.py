@@ -96,6 +96,7 @@ def load(kind: str) -> ctypes.CDLL:
         sig["kat_simple_golden"] = (ci, [ci, vp])
         sig["checkpoint_write"] = (cl, [vp, ctypes.c_char_p, cl, ctypes.c_char_p, cl])
         sig["checkpoint_read"] = (ci, [vp, ctypes.c_char_p, ctypes.c_char_p])
+        sig["calc_nu"] = (cd, [cd, cd, ci])
     for name, (res, args) in sig.items():
         fn = getattr(lib, p + name)
         fn.restype = res

@@ -354,6 +354,15 @@ int tdlbref_kat_esotwist_read(long x, long y, long z, int even, uint64_t* out) {
     return 0;
 }
 
+// FlowParams<float>::calcNuAndRe_m (FlowParams.hpp:65-70) itself.
+double tdlbref_calc_nu(double re, double uav, int radius) {
+    FlowParams<float> f;
+    f.reMNonDimensional = (float)re;
+    f.uav = (float)uav;
+    f.calcNuAndRe_m(radius);
+    return (double)f.nu;
+}
+
 // Checkpoint through the reference's own writer / reader. write returns the
 // directory length (0 on failure) and copies the path into dir_out.
 long tdlbref_checkpoint_write(void* hv, const char* unit, long step, char* dir_out, long cap) {

@@ -706,5 +706,5 @@ def schedule_levels(markers, x: int, y: int, z: int):
 
 def nu_from_reynolds(re: float, tip_speed: float, blade_outer_radius: int) -> float:
     """FlowParams::calcNuAndRe_m (FlowParams.hpp:65-70), in the reference's float arithmetic."""
-    re_m = np.float32(np.float32(re) * np.pi / 2.0)
+    re_m = np.float32(float(np.float32(re)) * np.pi / 2.0)   # float * M_PI promotes to double
     return float(np.float32(np.float32(tip_speed) * np.float32(blade_outer_radius) / re_m))

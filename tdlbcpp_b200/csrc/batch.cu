@@ -74,7 +74,7 @@ __device__ __forceinline__ void tank_quad(const TankStep& ts, unsigned t) {
 // bodies are not built. `counter` (may be NULL) is advanced once: this
 // launch runs after the step's rotation, which reads it.
 template <typename S, int V, int NT, bool ESO>
-__global__ void __launch_bounds__(NT) k_batch_step(const TankStep* __restrict__ tanks, const int2* __restrict__ work,
+__global__ void __launch_bounds__(NT, (ESO ? kEsotwistBlocksPerSM<V> : 4) * 128 / NT) k_batch_step(const TankStep* __restrict__ tanks, const int2* __restrict__ work,
                                                    int nwork, int* counter) {
     constexpr bool kFM = sizeof(S) == 4;
     __shared__ TankStep ts;
@@ -568,7 +568,7 @@ int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* ou
     b->device = device;
     b->storage = cfgs[0].storage;
     b->streaming = cfgs[0].streaming;
-    b->vec = cfgs[0].streaming == TDLB_STREAMING_SIMPLE ? 1 : 4;
+    b->vec = 1;
     try {
         TDLB_BCK(cudaSetDevice(device));
         TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
@@ -599,7 +599,7 @@ int tdlb_batch_create_empty(int device, int streaming, int storage, tdlb_batch* 
     b->device = device;
     b->storage = storage;
     b->streaming = streaming;
-    b->vec = streaming == TDLB_STREAMING_SIMPLE ? 1 : 4;
+    b->vec = 1;
     try {
         TDLB_BCK(cudaSetDevice(device));
         TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));

@@ -32,6 +32,9 @@
 #include "tdlb_rotate.hpp"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <utility>
 
 namespace tdlb {
 
@@ -581,10 +584,27 @@ size_t ibm_smem_bytes(const Dims& g, int cells) {
     return (size_t)3 * cells * sizeof(float);
 }
 
-cudaError_t ibm_prepare_smem(size_t bytes) {
-    cudaError_t e = cudaFuncSetAttribute(k_ibm_spread<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+// The dynamic shared-memory limit is a per-kernel, per-device attribute that
+// every lattice and batch shares: it only ever grows, so that a smaller
+// lattice set up later cannot lower it below what a larger one launches with.
+cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> set;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_ibm_spread<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = set[{fn, dev}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
+cudaError_t ibm_prepare_smem(size_t bytes) {
+    cudaError_t e = raise_smem_limit((const void*)k_ibm_spread<256>, bytes);
+    if (e != cudaSuccess) return e;
+    return raise_smem_limit((const void*)k_ibm_spread<512>, bytes);
 }
 
 cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, cudaStream_t st) {
@@ -695,11 +715,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread_
 }
 
 cudaError_t ibm_batch_prepare_smem(size_t small_bytes, size_t big_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(k_ibm_spread_batch<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)std::max<size_t>(small_bytes, 1));
+    cudaError_t e = raise_smem_limit((const void*)k_ibm_spread_batch<256>, small_bytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_ibm_spread_batch<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)std::max<size_t>(big_bytes, 1));
+    return raise_smem_limit((const void*)k_ibm_spread_batch<512>, big_bytes);
 }
 
 cudaError_t launch_ibm_batch(const IbmBatch& b, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {

@@ -130,6 +130,11 @@ long long need_of(const tdlb_request& r) {
     return (long long)b;
 }
 
+void note(tdlb_server_s* s, const std::string& msg) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->err = msg;
+}
+
 void push_result(tdlb_server_s* s, const tdlb_result& res) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->done.push_back(res);
@@ -183,6 +188,7 @@ bool admit_one(tdlb_server_s* s, const Pending& p, long long need) {
     int idx = -1;
     int rc = tdlb_batch_add(b, &c, &idx);
     if (rc != TDLB_OK) {
+        note(s, std::string("admission: ") + tdlb_batch_last_error(b));
         push_result(s, failed(r, rc, p.t_submit, s->now()));
         return false;
     }
@@ -193,6 +199,7 @@ bool admit_one(tdlb_server_s* s, const Pending& p, long long need) {
     if (rc == TDLB_OK) rc = tdlb_initialise(h, 1.0f);
     if (rc == TDLB_OK) rc = tdlb_forcing_resident(h, s->alpha, s->beta);
     if (rc != TDLB_OK) {
+        note(s, std::string("tank setup: ") + tdlb_last_error(h));
         tdlb_batch_remove(b, idx);
         push_result(s, failed(r, rc, p.t_submit, s->now()));
         return false;
@@ -258,6 +265,7 @@ void retire(tdlb_server_s* s, size_t k) {
     if (rc == TDLB_OK) rc = tdlb_reduce_fp64(a.h, red);
     if (rc == TDLB_OK && (a.req.out_rho || a.req.out_ux || a.req.out_uy || a.req.out_uz))
         rc = tdlb_read_velocity_density(a.h, a.req.out_rho, a.req.out_ux, a.req.out_uy, a.req.out_uz);
+    if (rc != TDLB_OK) note(s, std::string("retirement: ") + tdlb_last_error(a.h));
     res.status = rc;
     res.mass = red[0];
     for (int c = 0; c < 3; c++) {
@@ -284,13 +292,24 @@ void step_chunk(tdlb_server_s* s) {
     for (const Active& a : s->active) chunk = std::min(chunk, a.remaining);
     const double t = s->now();
     int rc = TDLB_OK;
+    std::string why;
     for (auto& kv : s->batches) {
         int n = 0;
         tdlb_batch_size(kv.second, &n);
-        if (n && rc == TDLB_OK) rc = tdlb_batch_run(kv.second, (int)chunk, s->alpha, s->beta);
+        if (n && rc == TDLB_OK) {
+            rc = tdlb_batch_run(kv.second, (int)chunk, s->alpha, s->beta);
+            if (rc != TDLB_OK) why = tdlb_batch_last_error(kv.second);
+        }
     }
     for (auto& kv : s->batches)
-        if (tdlb_batch_synchronize(kv.second) != TDLB_OK && rc == TDLB_OK) rc = TDLB_ECUDA;
+        if (tdlb_batch_synchronize(kv.second) != TDLB_OK && rc == TDLB_OK) {
+            rc = TDLB_ECUDA;
+            why = tdlb_batch_last_error(kv.second);
+        }
+    if (rc != TDLB_OK) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->err = "chunk failed: " + why;
+    }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->busy_s += s->now() - t;
@@ -394,7 +413,12 @@ int tdlb_server_create(int device, int64_t hbm_budget_bytes, int max_active, int
     return TDLB_OK;
 }
 
-const char* tdlb_server_last_error(tdlb_server s) { return s ? s->err.c_str() : g_server_error.c_str(); }
+const char* tdlb_server_last_error(tdlb_server s) {
+    if (!s) return g_server_error.c_str();
+    std::lock_guard<std::mutex> lk(s->mu);
+    g_server_error = s->err;   // a per-thread copy the caller may read
+    return g_server_error.c_str();
+}
 
 int tdlb_server_submit(tdlb_server s, const tdlb_request* r) {
     if (!s || !r) return TDLB_EINVAL;

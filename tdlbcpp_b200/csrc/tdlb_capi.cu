@@ -103,9 +103,9 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
     try {
         h->cfg = c;
         h->device = device;
-        // measured on B200 at 400^3: Simple is fastest with one cell per
-        // thread (direct loads), Esotwist with four (float4 + shuffles)
-        h->vec = c.streaming == TDLB_STREAMING_SIMPLE ? 1 : 4;
+        // measured on B200 at 400^3: both schemes are fastest with one cell
+        // per thread (direct loads; Esotwist with 64 registers, 8 blocks/SM)
+        h->vec = 1;
         h->err.reserve(512);
         TDLB_CK(cudaSetDevice(device));
         TDLB_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));

@@ -94,3 +94,12 @@ def test_restatement_bit_identical(ref_oracle, port_oracle, streaming, precision
     np.testing.assert_array_equal(a.interior(a.get_f()), b.interior(b.get_f()))
     np.testing.assert_array_equal(a.interior(a.get_nu()), b.interior(b.get_nu()))
     assert a.even_step == b.even_step
+
+
+@pytest.mark.parametrize("re,uav,radius", [(7300.0, 0.1, 10), (20000.0, 0.1, 66), (1276.9886727287553, 0.1, 8),
+                                           (13432.792223087894, 0.07532754608704051, 21)])
+def test_nu_from_reynolds_bit_exact_with_reference(ref_oracle, re, uav, radius):
+    """The host's calcNuAndRe_m restatements equal the reference's own."""
+    import tdlbcpp_b200 as tb
+    lib = ref_oracle.load("ref")
+    assert tb.nu_from_reynolds(re, uav, radius) == lib.tdlbref_calc_nu(re, uav, radius)
