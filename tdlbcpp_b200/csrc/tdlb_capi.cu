@@ -333,11 +333,18 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
     }
     if (n0) TDLB_CK(cudaMalloc(&h->d_prep, (size_t)tdlb::PF_COUNT * n0 * sizeof(float)));
     {
-        // F tiles: 4608 cells (3 CTAs of 256 threads per SM) for typical
-        // planes; planes with more cells (an impeller disk) go to a second
-        // launch with a tile for the largest of them (global memory beyond
-        // the 227 KB shared-memory limit)
-        const int small_cap = 4608;
+        // F tiles of the 256-thread launch: 3 CTAs per SM (80 registers a
+        // thread) fit 3 tiles of up to 6144 cells (72 KB) in shared memory;
+        // the tile is sized for the most crowded ordinary plane, at least
+        // 4608 cells. Planes with more cells (an impeller disk) go to a
+        // second, 512-thread launch with a tile for the largest of them
+        // (global memory beyond the 227 KB shared-memory limit).
+        int typical = 0;
+        for (int j = 0; j < g.ny; j++) {
+            const int nc = h->cells.plane_cell[(size_t)j + 1] - h->cells.plane_cell[(size_t)j];
+            if (nc <= 6144) typical = std::max(typical, nc);
+        }
+        const int small_cap = std::max(4608, round_up(typical, 64) > 6144 ? 6144 : (int)round_up(typical, 64));
         std::vector<int> small, big;
         int big_max = 0;
         for (int j = 0; j < g.ny; j++) {
