@@ -391,6 +391,154 @@ def run_batched(args, rank, world, device):
     }
 
 
+# ---------------------------------------------------------------- precision form
+
+PREC_STEPS = 2000
+PREC_ORACLE_EDGE = 120
+PREC_STREAMING = "Esotwist"   # the Simple wall rule diverges within these step counts
+
+
+def power_number(torque, omega, D):
+    """|torque * omega| / (N^3 D^5), N = omega / 2 pi, rho = 1 (lattice units)."""
+    n = omega / (2.0 * math.pi)
+    return abs(torque * omega) / (n ** 3 * D ** 5)
+
+
+def gpu_precision_run(tb, edge, storage, steps, device, timed=False):
+    import torch
+    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=TIP, startup_steps=0)
+    nu = tb.nu_from_reynolds(RE, TIP, rt.blade_outer_radius())
+    cu = tb.ComputeUnit(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0, storage=storage,
+                        streaming=PREC_STREAMING, device=device)
+    d1 = rt.increment(1)
+    cu.attach_rushton(rt, d1, d1, d1)
+    cu.initialise(1.0)
+    cu.forcing_resident(ALPHA, BETA)
+    mass0 = cu.reduce_fp64()[0]
+    st = torch.cuda.ExternalStream(cu.stream, device=device)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    angle = d1
+    cu.synchronize()
+    t0.record(st)
+    for s in range(2, steps + 2):
+        d = rt.increment(s)
+        angle += d
+        cu.rotate_impeller(angle, d)
+        cu.collision()
+        cu.forcing_resident(ALPHA, BETA)
+    t1.record(st)
+    cu.synchronize()
+    ms = t0.elapsed_time(t1)
+    rho, u = cu.read_velocity_density()
+    red = cu.reduce_fp64()
+    load = cu.impeller_load()
+    cu.close()
+    return {"u": u, "rho": rho, "mass0": mass0, "mass": red[0], "torque": load[3], "ms": ms,
+            "omega": d1, "D": rt.spec.impeller_diameter or edge / 3.0}
+
+
+def oracle_precision_run(tb, po, edge, steps, threads):
+    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=TIP, startup_steps=0)
+    nu = tb.nu_from_reynolds(RE, TIP, rt.blade_outer_radius())
+    flow = po.Flow(initialRho=1.0, nu=nu, cs0=0.1, g3=0.8, alpha=ALPHA, beta=BETA, useLES=True)
+    po.load("port").tdlbo_set_threads(threads)
+    lat = po.CpuLattice("port", edge, edge, edge, flow, PREC_STREAMING, 8)
+    d1 = rt.increment(1)
+    n_fixed = len(rt.fixed())
+    lat.initialise(1.0)
+    lat.forcing(rt.forcing_list(d1, d1, nonupdating_delta=d1), ALPHA, BETA)
+    angle = d1
+    t = time.perf_counter()
+    mk = None
+    for s in range(2, steps + 2):
+        d = rt.increment(s)
+        angle += d
+        mk = rt.forcing_list(angle, d, nonupdating_delta=d1)
+        lat.step(mk, ALPHA, BETA)
+    secs = time.perf_counter() - t
+    m = lat.get_moments()
+    f = lat.interior(lat.get_f())
+    rho = m[..., 0]
+    u = (m[..., 1:4] + 0.5 * f) / rho[..., None]
+    sums = lat.get_forcing_sums(len(mk))[n_fixed:]
+    imp = mk[n_fixed:]
+    ci = ck = (edge - 1) / 2.0
+    di = imp["i"] + imp["iCartFraction"].astype(np.float64) - ci
+    dk = imp["k"] + imp["kCartFraction"].astype(np.float64) - ck
+    fx, fz = -BETA * sums[:, 0], -BETA * sums[:, 2]
+    torque = float(np.sum(dk * fx - di * fz))
+    lat.close()
+    return {"u": u, "rho": rho, "mass0": float(edge ** 3), "mass": float(rho.sum()), "torque": torque,
+            "seconds": secs, "omega": d1, "D": edge / 3.0}
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def run_precision(args, rank, world, device):
+    """FP16 / BF16 deviation storage against the FP64 oracle (120^3) and
+    against the plain FP32 GPU form (400^3), both after PREC_STEPS steps."""
+    import torch
+    import tdlbcpp_b200 as tb
+    from oracle import pyoracle as po
+
+    torch.cuda.set_device(device)
+    steps = args.steps if args.steps != 500 else PREC_STEPS
+    out = {"steps": steps, "oracle_edge": PREC_ORACLE_EDGE}
+    # FP64 oracle at 120^3 (host threads), then the GPU forms at 120^3
+    threads = max(1, min(64, os.cpu_count() or 1))
+    ref = oracle_precision_run(tb, po, PREC_ORACLE_EDGE, steps, threads)
+    np_ref = power_number(ref["torque"], ref["omega"], ref["D"])
+    out["oracle"] = {"threads": threads, "seconds": ref["seconds"], "mass_drift": ref["mass"] / ref["mass0"] - 1.0,
+                     "power_number": np_ref, "finite": bool(np.isfinite(ref["u"]).all())}
+    small = {}
+    for storage in ("fp32", "fp16", "bf16"):
+        g = gpu_precision_run(tb, PREC_ORACLE_EDGE, storage, steps, device)
+        small[storage] = g
+        npn = power_number(g["torque"], g["omega"], g["D"])
+        out[f"{storage}_vs_fp64_120"] = {
+            "u_rel_l2": rel(g["u"], ref["u"]), "rho_rel_l2": rel(g["rho"], ref["rho"]),
+            "mass_drift": g["mass"] / g["mass0"] - 1.0, "power_number": npn,
+            "power_number_rel_err": abs(npn - np_ref) / abs(np_ref) if np_ref else None}
+    # the 400^3 forms: throughput, and the 16-bit forms against FP32
+    big = {}
+    for storage in ("fp32", "fp16", "bf16"):
+        g = gpu_precision_run(tb, args.edge, storage, steps, device, timed=True)
+        big[storage] = {"mlups": args.edge ** 3 * steps / (g["ms"] / 1e3) / 1e6, "ms_per_step": g["ms"] / steps,
+                        "mass_drift": g["mass"] / g["mass0"] - 1.0,
+                        "power_number": power_number(g["torque"], g["omega"], g["D"]), "u": g["u"]}
+    for storage in ("fp16", "bf16"):
+        big[storage]["u_rel_l2_vs_fp32"] = rel(big[storage]["u"], big["fp32"]["u"])
+    for storage in big:
+        big[storage].pop("u")
+    out["gpu_400"] = big
+    return out
+
+
+def report_precision(args, rank, world, local, config):
+    res = run_precision(args, rank, world, local)
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peak()
+    fp16 = res["gpu_400"]["fp16"]
+    achieved = 80 * args.edge ** 3 / (fp16["ms_per_step"] / 1e3) / 1e9
+    config = dict(config, results=res)
+    line = {
+        "metric": "MLUPS", "value": fp16["mlups"], "unit": "MLUPS", "n_gpus": world, "steps": res["steps"],
+        "warmup": 0, "ms_per_step": fp16["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp16 storage, fp32 arithmetic", "data": "synthetic", "config": config,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "kernel": "whole step (rotate + fused step + IBM), 80 B/cell",
+                     "bytes_per_cell": 80, "traffic": None},
+        "fp32_mlups": res["gpu_400"]["fp32"]["mlups"], "bf16_mlups": res["gpu_400"]["bf16"]["mlups"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- serving form
 
 SERVE_EDGES = (48, 64, 96, 128, 192, 256)
@@ -670,7 +818,7 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["simple", "esotwist", "batched", "serving"], default="simple")
+    ap.add_argument("--workload", choices=["simple", "esotwist", "batched", "serving", "precision"], default="simple")
     ap.add_argument("--requests", type=int, default=64, help="serving: prefix of the request stream to serve")
     ap.add_argument("--chunk", type=int, default=100, help="serving: steps per batched chunk")
     ap.add_argument("--edge", type=int, default=EDGE)
@@ -678,7 +826,13 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3   # timing rule: at least 3 warm-up steps
-    if args.workload == "serving":
+    if args.workload == "precision":
+        workload = f"precision-{args.edge}^3-esotwist-fp16-bf16-les"
+        config = {"workload": workload, "grid": [args.edge] * 3, "oracle_grid": [PREC_ORACLE_EDGE] * 3,
+                  "streaming": PREC_STREAMING, "storage": "fp16/bf16 deviations f_i - w_i*rho0, fp32 arithmetic",
+                  "fp64": "mass/momentum sums, impeller torque, power number", "re": RE, "tip_speed": TIP,
+                  "collision": "EgglesSomers+LES(cs0=0.1)", "ibm": "Rushton turbine, rotating"}
+    elif args.workload == "serving":
         workload = f"serving-{args.requests}-of-{SERVE_TOTAL}-requests"
         config = {"workload": workload, "requests": args.requests, "stream_total": SERVE_TOTAL, "seed": SERVE_SEED,
                   "rate_per_s": SERVE_RATE, "edges": list(SERVE_EDGES), "steps": [500, 5000], "re": [1e3, 2e4],
@@ -722,6 +876,8 @@ def main():
         return report_batched(args, rank, world, local, config)
     if args.workload == "serving":
         return report_serving(args, rank, world, local, config)
+    if args.workload == "precision":
+        return report_precision(args, rank, world, local, config)
 
     res = run_ours(args, rank, world, local)
     if rank != 0:
