@@ -48,6 +48,9 @@ extern "C" {
 #define TDLB_STORAGE_FP32 0
 #define TDLB_STORAGE_FP16 1
 #define TDLB_STORAGE_BF16 2
+/* 16-bit fixed point deviations in units of 2^-18 (range +-0.125, a uniform
+ * step of 3.8e-6; needs initialRho <= 1). No counterpart in the reference. */
+#define TDLB_STORAGE_I16 3
 
 typedef struct tdlb_lattice* tdlb_handle;
 
@@ -167,6 +170,51 @@ int tdlb_reduce_fp64(tdlb_handle h, double* out4);
 
 /* Make all queued device work complete. */
 int tdlb_synchronize(tdlb_handle h);
+
+/* Replaces: ComputeUnitBase::doubleResolutionFullCU() (ComputeUnit.hpp:
+ * 258-316): x, y, z double; every new cell takes the moments and Nu of old
+ * cell (i/2, j/2, k/2); F, the touched flags and the excluded points start
+ * at zero; the state then holds moments, as after tdlb_initialise. The
+ * markers are dropped: set the geometry of the new size (as main.cpp:
+ * 349-397 does). FP32 storage, handles outside a batch. */
+int tdlb_double_resolution(tdlb_handle h);
+
+/* ---- output: excluded points, vorticity slices, plane dump ---- */
+
+/* Replaces: setOutputExcludePoints / unsetOutputExcludePoints
+ * (ComputeUnitOutput.hpp:20-53): the cells of the markers (i, j, k) become
+ * (exclude = 1) or stop being (0) excluded output points. */
+int tdlb_set_output_exclude(tdlb_handle h, const tdlb_marker* markers, size_t n, int exclude);
+
+/* Replaces: calcVorticityXZ(j) / calcVorticityXY(k) (ComputeUnitOutput.hpp:
+ * 113-285; GPU ComputeUnitOutput.cuh:10-64) up to the picture: the float
+ * field log |curl u|^2, u = j / rho of the current moments, central
+ * differences; -1 at excluded points. XZ: out[i*z + k] (x*z floats); XY:
+ * out[j*x + i] (x*y floats). A neighbour beyond a lattice face is replaced
+ * by the cell itself (the reference reads its ghost layer there). */
+int tdlb_vorticity_xz(tdlb_handle h, int64_t j, float* out);
+int tdlb_vorticity_xy(tdlb_handle h, int64_t k, float* out);
+
+/* tDiskGrid<float, 4> and tDiskGrid<float, 3> (Output.hpp:22-26): cell
+ * coordinates and 4 moments / 3 force components, 24 and 20 bytes. */
+typedef struct tdlb_disk_grid4 {
+    uint16_t iGrid, jGrid, kGrid, pad;
+    float q[4];
+} tdlb_disk_grid4;
+typedef struct tdlb_disk_grid3 {
+    uint16_t iGrid, jGrid, kGrid, pad;
+    float q[3];
+} tdlb_disk_grid3;
+
+/* Replaces: savePlaneXZ<float, 4> (ComputeUnitOutput.hpp:354-447) up to the
+ * files: the records of the plane j, in (i, k) order -- every non-excluded
+ * cell's first four moments, and F where F is non-zero. Coordinates as the
+ * reference writes them: iGrid = i, kGrid = k, jGrid = j for the moments and
+ * j + 1 for F. q_n / f_n return the counts; with q_out / f_out NULL only the
+ * counts are computed. The caller writes the records as the reference's
+ * QVec.bin / F3.bin files. */
+int tdlb_plane_xz(tdlb_handle h, int64_t j, tdlb_disk_grid4* q_out, size_t q_cap, size_t* q_n, tdlb_disk_grid3* f_out,
+                  size_t f_cap, size_t* f_n);
 
 /* Replaces: ComputeUnitBase::checkpoint_write(unit_name, RunningParams)
  * (ComputeUnit.hpp:389-439) with the directory given instead of derived

@@ -97,6 +97,8 @@ def load(kind: str) -> ctypes.CDLL:
         sig["checkpoint_write"] = (cl, [vp, ctypes.c_char_p, cl, ctypes.c_char_p, cl])
         sig["checkpoint_read"] = (ci, [vp, ctypes.c_char_p, ctypes.c_char_p])
         sig["calc_nu"] = (cd, [cd, cd, ci])
+        sig["set_exclude"] = (None, [vp, vp, cl, ci])
+        sig["save_plane_xz"] = (cl, [vp, cl, cl, ctypes.c_char_p, cl])
     for name, (res, args) in sig.items():
         fn = getattr(lib, p + name)
         fn.restype = res
@@ -235,6 +237,18 @@ class CpuLattice:
         """The reference's own checkpoint_read (ref only)."""
         if self._fn("checkpoint_read")(self.h, directory.encode(), unit.encode()) != 0:
             raise RuntimeError("reference checkpoint_read failed")
+
+    def set_exclude(self, markers: np.ndarray, exclude: bool = True):
+        """The reference's setOutputExcludePoints / unset (ref only)."""
+        m = np.ascontiguousarray(markers)
+        self._fn("set_exclude")(self.h, _ptr(m), len(m), 1 if exclude else 0)
+
+    def save_plane_xz(self, j: int, step: int) -> str:
+        """The reference's savePlaneXZ<float, 4> (ref only); returns its directory."""
+        buf = ctypes.create_string_buffer(4096)
+        if self._fn("save_plane_xz")(self.h, j, step, buf, len(buf)) <= 0:
+            raise RuntimeError("reference savePlaneXZ failed")
+        return buf.value.decode()
 
     def get_o(self) -> np.ndarray:
         """Cells the last forcing() touched (port only; the reference resets O)."""

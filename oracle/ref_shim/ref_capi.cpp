@@ -17,6 +17,7 @@
 //     the Simple push golden vectors of tests/StreamingSimplePushTest.hpp,
 //     and the Esotwist read/write/writeMoments maps (StreamingEsoteric.hpp:28-180).
 #include <cstdint>
+#include <type_traits>
 #include <cstring>
 #include <cstdlib>
 #include <string>
@@ -179,6 +180,30 @@ std::string checkpointWrite(Base<T>* cu, const std::string& tmpdir, const char* 
                              out.getJson(), chk.getJson());
     cu->checkpoint_write(unit, run);
     return cu->outputTree.getCheckpointDirName(run, false);
+}
+
+template <typename T>
+void setExclude(Base<T>* cu, const MarkerC* m, long n, int exclude) {
+    std::vector<PosPolar<tNi, T>> pts((size_t)n);
+    for (long q = 0; q < n; q++) {
+        pts[(size_t)q].i = m[q].i;
+        pts[(size_t)q].j = m[q].j;
+        pts[(size_t)q].k = m[q].k;
+    }
+    if (exclude) cu->setOutputExcludePoints(pts);
+    else cu->unsetOutputExcludePoints(pts);
+}
+
+template <typename T>
+std::string savePlane(Base<T>* cu, long j, long step) {
+    MuteCout mute;
+    OrthoPlaneParams plane;
+    plane.cutAt = j;
+    BinFileParams bin;
+    RunningParams run;
+    run.step = step;
+    cu->template savePlaneXZ<float, 4>(plane, bin, run);
+    return cu->outputTree.formatXZPlaneDir(run.step, plane.cutAt);
 }
 
 extern "C" {
@@ -361,6 +386,28 @@ double tdlbref_calc_nu(double re, double uav, int radius) {
     f.uav = (float)uav;
     f.calcNuAndRe_m(radius);
     return (double)f.nu;
+}
+
+// setOutputExcludePoints / unsetOutputExcludePoints (ComputeUnitOutput.hpp:20-53).
+void tdlbref_set_exclude(void* hv, const tdlbref_marker* m, long n, int exclude) {
+    Handle* h = (Handle*)hv;
+    if (h->precision == 4) setExclude<float>(as<float>(h), m, n, exclude);
+    else setExclude<double>(as<double>(h), m, n, exclude);
+}
+
+// savePlaneXZ<float, 4> (ComputeUnitOutput.hpp:354-447) through the
+// reference's own DiskOutputTree; returns the plot directory it wrote.
+long tdlbref_save_plane_xz(void* hv, long j, long step, char* dir_out, long cap) {
+    Handle* h = (Handle*)hv;
+    std::string dir;
+    try {
+        dir = h->precision == 4 ? savePlane<float>(as<float>(h), j, step) : savePlane<double>(as<double>(h), j, step);
+    } catch (const std::exception&) {
+        return 0;
+    }
+    if ((long)dir.size() + 1 > cap) return 0;
+    std::memcpy(dir_out, dir.c_str(), dir.size() + 1);
+    return (long)dir.size();
 }
 
 // Checkpoint through the reference's own writer / reader. write returns the

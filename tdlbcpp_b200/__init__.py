@@ -32,6 +32,7 @@ STREAMING_ESOTWIST = 1
 STORAGE_FP32 = 0
 STORAGE_FP16 = 1
 STORAGE_BF16 = 2
+STORAGE_I16 = 3
 
 # Lattice vectors of population slots Q01..Q18 (tdlbcpp/src/Header.h:70-100);
 # opposite(d) = d ^ 1.
@@ -49,6 +50,14 @@ MARKER_DTYPE = np.dtype(
     ]
 )
 assert MARKER_DTYPE.itemsize == 48
+
+# tdlb_disk_grid4 / tdlb_disk_grid3: the reference's tDiskGrid<float, 4 / 3>
+# plane-dump records (Output.hpp:22-26).
+DISK_GRID4_DTYPE = np.dtype([("iGrid", np.uint16), ("jGrid", np.uint16), ("kGrid", np.uint16), ("pad", np.uint16),
+                             ("q", np.float32, 4)])
+DISK_GRID3_DTYPE = np.dtype([("iGrid", np.uint16), ("jGrid", np.uint16), ("kGrid", np.uint16), ("pad", np.uint16),
+                             ("q", np.float32, 3)])
+assert DISK_GRID4_DTYPE.itemsize == 24 and DISK_GRID3_DTYPE.itemsize == 20
 
 _ERRORS = {
     -1: "TDLB_EINVAL", -2: "TDLB_ECUDA", -3: "TDLB_ENOMEM", -4: "TDLB_EIO", -5: "TDLB_ESTATE", -6: "TDLB_EJSON",
@@ -134,7 +143,7 @@ def make_config(**fields) -> Config:
         if key == "streaming" and isinstance(val, str):
             val = STREAMING_SIMPLE if val == "Simple" else STREAMING_ESOTWIST
         if key == "storage" and isinstance(val, str):
-            val = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16}[val.lower()]
+            val = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16, "i16": STORAGE_I16}[val.lower()]
         setattr(cfg, key, val)
     return cfg
 
@@ -199,6 +208,11 @@ def load_library() -> ctypes.CDLL:
         "tdlb_reduce_fp64": (i32, [H, vp]),
         "tdlb_checkpoint_write": (i32, [H, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]),
         "tdlb_checkpoint_read": (i32, [H, ctypes.c_char_p, ctypes.c_char_p]),
+        "tdlb_set_output_exclude": (i32, [H, vp, sz, i32]),
+        "tdlb_double_resolution": (i32, [H]),
+        "tdlb_vorticity_xz": (i32, [H, ctypes.c_int64, vp]),
+        "tdlb_vorticity_xy": (i32, [H, ctypes.c_int64, vp]),
+        "tdlb_plane_xz": (i32, [H, ctypes.c_int64, vp, sz, ctypes.POINTER(sz), vp, sz, ctypes.POINTER(sz)]),
         "tdlb_batch_create": (i32, [ctypes.POINTER(Config), i32, i32, ctypes.POINTER(H)]),
         "tdlb_batch_destroy": (i32, [H]),
         "tdlb_batch_last_error": (ctypes.c_char_p, [H]),
@@ -389,6 +403,40 @@ class ComputeUnit:
 
     def checkpoint_read(self, directory: str, unit_name: str):
         self._check(self.lib.tdlb_checkpoint_read(self.h, directory.encode(), unit_name.encode()))
+
+    def doubleResolutionFullCU(self):
+        """Double x, y, z on the device (ComputeUnit.hpp:258-316); set the
+        geometry of the new size afterwards."""
+        self._check(self.lib.tdlb_double_resolution(self.h))
+        x, y, z = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.tdlb_get_dims(self.h, ctypes.byref(x), ctypes.byref(y), ctypes.byref(z)))
+        self.x, self.y, self.z = x.value, y.value, z.value
+
+    # ---- output (ComputeUnitOutput.hpp) ----
+    def set_output_exclude(self, markers, exclude: bool = True):
+        m = as_markers(markers)
+        self._check(self.lib.tdlb_set_output_exclude(self.h, _p(m), len(m), 1 if exclude else 0))
+
+    def vorticity_xz(self, j: int) -> np.ndarray:
+        """log |curl u|^2 on the plane j, [x, z]; -1 at excluded points."""
+        out = np.empty((self.x, self.z), np.float32)
+        self._check(self.lib.tdlb_vorticity_xz(self.h, j, _p(out)))
+        return out
+
+    def vorticity_xy(self, k: int) -> np.ndarray:
+        """log |curl u|^2 on the plane k, [y, x] (the reference's picture order)."""
+        out = np.empty((self.y, self.x), np.float32)
+        self._check(self.lib.tdlb_vorticity_xy(self.h, k, _p(out)))
+        return out
+
+    def plane_xz(self, j: int):
+        """savePlaneXZ<float, 4> records: (moments of non-excluded cells, F where non-zero)."""
+        nq, nf = ctypes.c_size_t(), ctypes.c_size_t()
+        self._check(self.lib.tdlb_plane_xz(self.h, j, None, 0, ctypes.byref(nq), None, 0, ctypes.byref(nf)))
+        q = np.zeros(nq.value, DISK_GRID4_DTYPE)
+        f = np.zeros(nf.value, DISK_GRID3_DTYPE)
+        self._check(self.lib.tdlb_plane_xz(self.h, j, _p(q), len(q), ctypes.byref(nq), _p(f), len(f), ctypes.byref(nf)))
+        return q, f
 
     def set_cells_per_thread(self, v: int):
         """Step-kernel variant (1, 2 or 4 cells per thread); results are identical."""
@@ -587,7 +635,7 @@ class Server:
         r = Request()
         r.id, r.x, r.y, r.z = rid, x, y, z
         r.tip_speed, r.reynolds, r.steps = tip_speed, reynolds, steps
-        r.storage = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16}[storage]
+        r.storage = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16, "i16": STORAGE_I16}[storage]
         r.streaming = STREAMING_SIMPLE if streaming == "Simple" else STREAMING_ESOTWIST
         r.les = int(les)
         if fields:

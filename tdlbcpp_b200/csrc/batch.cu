@@ -125,9 +125,10 @@ BatchFn pick(int v, int nt) {
 }
 
 BatchFn batch_kernel(int storage, bool eso, int v, int nt) {
-    if (storage == STORE_F16) return eso ? pick<__half, true>(v, nt) : pick<__half, false>(v, nt);
-    if (storage == STORE_BF16) return eso ? pick<__nv_bfloat16, true>(v, nt) : pick<__nv_bfloat16, false>(v, nt);
-    return eso ? pick<float, true>(v, nt) : pick<float, false>(v, nt);
+    return with_storage(storage, [&](auto s) {
+        using S = decltype(s);
+        return eso ? pick<S, true>(v, nt) : pick<S, false>(v, nt);
+    });
 }
 
 }  // namespace tdlb
@@ -590,7 +591,7 @@ int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* ou
 
 int tdlb_batch_create_empty(int device, int streaming, int storage, tdlb_batch* out) {
     if (!out || (streaming != TDLB_STREAMING_SIMPLE && streaming != TDLB_STREAMING_ESOTWIST) ||
-        (storage != TDLB_STORAGE_FP32 && storage != TDLB_STORAGE_FP16 && storage != TDLB_STORAGE_BF16)) {
+        storage < TDLB_STORAGE_FP32 || storage > TDLB_STORAGE_I16) {
         g_batch_create_error = "bad arguments";
         return TDLB_EINVAL;
     }

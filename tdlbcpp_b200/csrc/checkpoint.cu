@@ -370,12 +370,9 @@ int tdlb_checkpoint_write(tdlb_handle h, const char* dir, const char* unit_name,
         TDLB_CCK(cudaMemsetAsync(sc.dev, 0, (size_t)ng * tdlb::NQ * sizeof(float), h->stream));
         const Planes A = h->planes(h->state_buf());
         const int mode = h->state_mode(), even = h->even ? 1 : 0;
-        if (h->cfg.storage == TDLB_STORAGE_FP16)
-            tdlb::k_ckpt_q_out<__half><<<blocks(cells), 256, 0, h->stream>>>(A, g, mode, even, h->cp, eso, sc.dev);
-        else if (h->cfg.storage == TDLB_STORAGE_BF16)
-            tdlb::k_ckpt_q_out<__nv_bfloat16><<<blocks(cells), 256, 0, h->stream>>>(A, g, mode, even, h->cp, eso, sc.dev);
-        else
-            tdlb::k_ckpt_q_out<float><<<blocks(cells), 256, 0, h->stream>>>(A, g, mode, even, h->cp, eso, sc.dev);
+        tdlb::with_storage(h->cfg.storage, [&](auto s) {
+            tdlb::k_ckpt_q_out<decltype(s)><<<blocks(cells), 256, 0, h->stream>>>(A, g, mode, even, h->cp, eso, sc.dev);
+        });
         TDLB_CCK(cudaGetLastError());
         write_device(grid_file(sdir, id, unit, "Q"), sc.dev, (size_t)ng * tdlb::NQ * sizeof(float), h->stream, sc.pin);
         // F and Nu share the scratch: F at [0, 3 ng), Nu at [3 ng, 4 ng)

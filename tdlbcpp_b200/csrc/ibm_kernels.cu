@@ -552,9 +552,9 @@ __global__ void k_reduce_fp64_final(const double* partial, int nblocks, double* 
 }
 
 cudaError_t launch_reduce_fp64(const IbmArgs& a, const uint32_t* mask, double* partial, double* out, cudaStream_t st) {
-    if (a.storage == STORE_F16) k_reduce_fp64<__half><<<kReduceBlocks, 256, 0, st>>>(a, mask, partial);
-    else if (a.storage == STORE_BF16) k_reduce_fp64<__nv_bfloat16><<<kReduceBlocks, 256, 0, st>>>(a, mask, partial);
-    else k_reduce_fp64<float><<<kReduceBlocks, 256, 0, st>>>(a, mask, partial);
+    with_storage(a.storage, [&](auto s) {
+        k_reduce_fp64<decltype(s)><<<kReduceBlocks, 256, 0, st>>>(a, mask, partial);
+    });
     k_reduce_fp64_final<<<1, 32, 0, st>>>(partial, kReduceBlocks, out);
     return cudaGetLastError();
 }
@@ -574,8 +574,7 @@ cudaError_t launch_fill_rest(Planes Q, long long plane, float rho, float rho0, i
                              cudaStream_t st) {
     const unsigned b = (unsigned)((plane + 255) / 256);
     const float r = rho / rho0 - 1.f;
-    if (storage == STORE_F16) k_fill_rest<__half><<<b, 256, 0, st>>>(Q, plane, r, p);
-    else k_fill_rest<__nv_bfloat16><<<b, 256, 0, st>>>(Q, plane, r, p);
+    with_storage(storage, [&](auto s) { k_fill_rest<decltype(s)><<<b, 256, 0, st>>>(Q, plane, r, p); });
     return cudaGetLastError();
 }
 
@@ -617,17 +616,13 @@ cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
     if (a.ncell > 0) {
         const unsigned b = (a.ncell + 255) / 256;
-        if (a.storage == STORE_F16) k_ibm_cells<__half><<<b, 256, 0, st>>>(a);
-        else if (a.storage == STORE_BF16) k_ibm_cells<__nv_bfloat16><<<b, 256, 0, st>>>(a);
-        else k_ibm_cells<float><<<b, 256, 0, st>>>(a);
+        with_storage(a.storage, [&](auto s) { k_ibm_cells<decltype(s)><<<b, 256, 0, st>>>(a); });
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }
     if (a.n > a.n0) {
         const unsigned b = (a.n - a.n0 + 127) / 128;
-        if (a.storage == STORE_F16) k_ibm_gather_tail<__half><<<b, 128, 0, st>>>(a);
-        else if (a.storage == STORE_BF16) k_ibm_gather_tail<__nv_bfloat16><<<b, 128, 0, st>>>(a);
-        else k_ibm_gather_tail<float><<<b, 128, 0, st>>>(a);
+        with_storage(a.storage, [&](auto s) { k_ibm_gather_tail<decltype(s)><<<b, 128, 0, st>>>(a); });
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }
@@ -722,14 +717,14 @@ cudaError_t ibm_batch_prepare_smem(size_t small_bytes, size_t big_bytes) {
 
 cudaError_t launch_ibm_batch(const IbmBatch& b, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
     if (b.n_cells > 0) {
-        if (b.storage == STORE_F16) k_ibm_cells_batch<__half><<<b.n_cells, 256, 0, st>>>(b.args, b.cells);
-        else if (b.storage == STORE_BF16) k_ibm_cells_batch<__nv_bfloat16><<<b.n_cells, 256, 0, st>>>(b.args, b.cells);
-        else k_ibm_cells_batch<float><<<b.n_cells, 256, 0, st>>>(b.args, b.cells);
+        with_storage(b.storage, [&](auto s) {
+            k_ibm_cells_batch<decltype(s)><<<b.n_cells, 256, 0, st>>>(b.args, b.cells);
+        });
     }
     if (b.n_tails > 0) {
-        if (b.storage == STORE_F16) k_ibm_tail_batch<__half><<<b.n_tails, 128, 0, st>>>(b.args, b.tails);
-        else if (b.storage == STORE_BF16) k_ibm_tail_batch<__nv_bfloat16><<<b.n_tails, 128, 0, st>>>(b.args, b.tails);
-        else k_ibm_tail_batch<float><<<b.n_tails, 128, 0, st>>>(b.args, b.tails);
+        with_storage(b.storage, [&](auto s) {
+            k_ibm_tail_batch<decltype(s)><<<b.n_tails, 128, 0, st>>>(b.args, b.tails);
+        });
     }
     if (b.n_copies > 0) k_mask_copy_batch<<<b.n_copies, 256, 0, st>>>(b.args, b.copies);
     cudaError_t err = cudaGetLastError();

@@ -102,9 +102,9 @@ cudaError_t launch_fill_uniform_moments(Planes Q, const Dims& g, float rho, cuda
 cudaError_t launch_state_moments(Planes A, Planes M, const Dims& g, int mode, int even, cudaStream_t st, int storage,
                                  const CollideParams& p) {
     const unsigned blocks = blocks_for(g.rows() * g.nz, 256);
-    if (storage == STORE_F16) k_state_moments<__half><<<blocks, 256, 0, st>>>(A, M, g, mode, even, p);
-    else if (storage == STORE_BF16) k_state_moments<__nv_bfloat16><<<blocks, 256, 0, st>>>(A, M, g, mode, even, p);
-    else k_state_moments<float><<<blocks, 256, 0, st>>>(A, M, g, mode, even, p);
+    with_storage(storage, [&](auto s) {
+        k_state_moments<decltype(s)><<<blocks, 256, 0, st>>>(A, M, g, mode, even, p);
+    });
     return cudaGetLastError();
 }
 

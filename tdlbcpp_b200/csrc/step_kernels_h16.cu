@@ -1,6 +1,6 @@
-// 16-bit deviation storage (FP16 and BF16) instances of the step kernels
-// (step_kernels.cuh). Populations are stored as f - w_d * rho0; collision and
-// LES run in FP32. One and four cells per thread.
+// 16-bit deviation storage (FP16, BF16 and 16-bit fixed point) instances of
+// the step kernels (step_kernels.cuh). Populations are stored as
+// f - w_d * rho0; collision and LES run in FP32. One and four cells per thread.
 #include "step_kernels.cuh"
 
 namespace tdlb {
@@ -30,14 +30,20 @@ static cudaError_t eso16(const StepArgs& a, cudaStream_t st) {
 
 cudaError_t launch_step_simple_h16(const StepArgs& a, cudaStream_t st) {
     if (!a.collide || a.from_moments) return cudaErrorInvalidValue;   // 16-bit state is always populations
-    if (a.storage == STORE_F16) return a.vec == 1 ? simple16<__half, 1>(a, st) : simple16<__half, 4>(a, st);
-    return a.vec == 1 ? simple16<__nv_bfloat16, 1>(a, st) : simple16<__nv_bfloat16, 4>(a, st);
+    return with_storage(a.storage, [&](auto s) {
+        using S = decltype(s);
+        if constexpr (sizeof(S) == 4) return cudaErrorInvalidValue;
+        else return a.vec == 1 ? simple16<S, 1>(a, st) : simple16<S, 4>(a, st);
+    });
 }
 
 cudaError_t launch_step_esotwist_h16(const StepArgs& a, cudaStream_t st) {
     if (!a.collide || a.from_moments) return cudaErrorInvalidValue;
-    if (a.storage == STORE_F16) return a.vec == 1 ? eso16<__half, 1>(a, st) : eso16<__half, 4>(a, st);
-    return a.vec == 1 ? eso16<__nv_bfloat16, 1>(a, st) : eso16<__nv_bfloat16, 4>(a, st);
+    return with_storage(a.storage, [&](auto s) {
+        using S = decltype(s);
+        if constexpr (sizeof(S) == 4) return cudaErrorInvalidValue;
+        else return a.vec == 1 ? eso16<S, 1>(a, st) : eso16<S, 4>(a, st);
+    });
 }
 
 }  // namespace tdlb

@@ -60,6 +60,8 @@ struct tdlb_lattice {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     uint32_t* d_mask_static = nullptr;   // first segment's touched cells
+    uint32_t* d_exclude = nullptr;       // excluded output points (1 bit per cell), when set
+    std::vector<uint32_t> h_exclude;
     double* d_red = nullptr;             // FP64 reduction partials + result
     long long marker_cap = 0;
     long long level_cap = 0;

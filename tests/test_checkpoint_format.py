@@ -50,3 +50,24 @@ def test_reference_checkpoint_layout(ref_oracle, tmp_path, streaming):
     if streaming == "Esotwist":
         # three steps leave the parity odd; the reference's reader starts even
         assert lat.even_step is False and back.even_step is True
+
+
+def test_reference_plane_dump_layout(ref_oracle, tmp_path):
+    """savePlaneXZ<float, 4> (ComputeUnitOutput.hpp:354-447): 24-byte
+    tDiskGrid<float, 4> records in (i, k) order with jGrid = j - 1 (ghosted j);
+    no F records before any forcing."""
+    import tdlbcpp_b200 as tb
+    po = ref_oracle
+    x, y, z = 5, 6, 7
+    lat = po.CpuLattice("ref", x, y, z, po.Flow(initialRho=1.0, nu=0.01), "Simple", 4, tmpdir=str(tmp_path))
+    lat.initialise(1.0)
+    d = lat.save_plane_xz(3, 1)
+    q = np.fromfile(os.path.join(d, "CUid.0.0.0.V5.QVec.bin"), tb.DISK_GRID4_DTYPE)
+    f = np.fromfile(os.path.join(d, "CUid.0.0.0.V5.F3.bin"), tb.DISK_GRID3_DTYPE)
+    assert len(q) == x * z and len(f) == 0
+    ii, kk = np.meshgrid(np.arange(x), np.arange(z), indexing="ij")
+    np.testing.assert_array_equal(q["iGrid"], ii.ravel())
+    np.testing.assert_array_equal(q["kGrid"], kk.ravel())
+    assert np.all(q["jGrid"] == 2)
+    np.testing.assert_array_equal(q["q"][:, 0], 1.0)
+    np.testing.assert_array_equal(q["q"][:, 1:], 0.0)
