@@ -495,7 +495,7 @@ def run_precision(args, rank, world, device):
     out["oracle"] = {"threads": threads, "seconds": ref["seconds"], "mass_drift": ref["mass"] / ref["mass0"] - 1.0,
                      "power_number": np_ref, "finite": bool(np.isfinite(ref["u"]).all())}
     small = {}
-    for storage in ("fp32", "fp16", "bf16", "i16"):
+    for storage in ("fp32", "fp16", "bf16"):
         g = gpu_precision_run(tb, PREC_ORACLE_EDGE, storage, steps, device)
         small[storage] = g
         npn = power_number(g["torque"], g["omega"], g["D"])
@@ -505,12 +505,12 @@ def run_precision(args, rank, world, device):
             "power_number_rel_err": abs(npn - np_ref) / abs(np_ref) if np_ref else None}
     # the 400^3 forms: throughput, and the 16-bit forms against FP32
     big = {}
-    for storage in ("fp32", "fp16", "bf16", "i16"):
+    for storage in ("fp32", "fp16", "bf16"):
         g = gpu_precision_run(tb, args.edge, storage, steps, device, timed=True)
         big[storage] = {"mlups": args.edge ** 3 * steps / (g["ms"] / 1e3) / 1e6, "ms_per_step": g["ms"] / steps,
                         "mass_drift": g["mass"] / g["mass0"] - 1.0,
                         "power_number": power_number(g["torque"], g["omega"], g["D"]), "u": g["u"]}
-    for storage in ("fp16", "bf16", "i16"):
+    for storage in ("fp16", "bf16"):
         big[storage]["u_rel_l2_vs_fp32"] = rel(big[storage]["u"], big["fp32"]["u"])
     for storage in big:
         big[storage].pop("u")
@@ -534,7 +534,6 @@ def report_precision(args, rank, world, local, config):
                      "peak_kind": peak_kind, "kernel": "whole step (rotate + fused step + IBM), 80 B/cell",
                      "bytes_per_cell": 80, "traffic": None},
         "fp32_mlups": res["gpu_400"]["fp32"]["mlups"], "bf16_mlups": res["gpu_400"]["bf16"]["mlups"],
-        "i16_mlups": res["gpu_400"]["i16"]["mlups"],
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -48,9 +48,6 @@ extern "C" {
 #define TDLB_STORAGE_FP32 0
 #define TDLB_STORAGE_FP16 1
 #define TDLB_STORAGE_BF16 2
-/* 16-bit fixed point deviations in units of 2^-18 (range +-0.125, a uniform
- * step of 3.8e-6; needs initialRho <= 1). No counterpart in the reference. */
-#define TDLB_STORAGE_I16 3
 
 typedef struct tdlb_lattice* tdlb_handle;
 
@@ -208,7 +205,9 @@ typedef struct tdlb_disk_grid3 {
 
 /* Replaces: savePlaneXZ<float, 4> (ComputeUnitOutput.hpp:354-447) up to the
  * files: the records of the plane j, in (i, k) order -- every non-excluded
- * cell's first four moments, and F where F is non-zero. Coordinates as the
+ * cell's Q slots 0..3 as the reference holds them (Simple: the first four
+ * moments; Esotwist: the raw slots of the writeMoments placement, i.e.
+ * moments of neighbouring cells), and F where F is non-zero. Coordinates as the
  * reference writes them: iGrid = i, kGrid = k, jGrid = j for the moments and
  * j + 1 for F. q_n / f_n return the counts; with q_out / f_out NULL only the
  * counts are computed. The caller writes the records as the reference's

@@ -32,7 +32,6 @@ STREAMING_ESOTWIST = 1
 STORAGE_FP32 = 0
 STORAGE_FP16 = 1
 STORAGE_BF16 = 2
-STORAGE_I16 = 3
 
 # Lattice vectors of population slots Q01..Q18 (tdlbcpp/src/Header.h:70-100);
 # opposite(d) = d ^ 1.
@@ -143,7 +142,7 @@ def make_config(**fields) -> Config:
         if key == "streaming" and isinstance(val, str):
             val = STREAMING_SIMPLE if val == "Simple" else STREAMING_ESOTWIST
         if key == "storage" and isinstance(val, str):
-            val = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16, "i16": STORAGE_I16}[val.lower()]
+            val = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16}[val.lower()]
         setattr(cfg, key, val)
     return cfg
 
@@ -635,7 +634,7 @@ class Server:
         r = Request()
         r.id, r.x, r.y, r.z = rid, x, y, z
         r.tip_speed, r.reynolds, r.steps = tip_speed, reynolds, steps
-        r.storage = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16, "i16": STORAGE_I16}[storage]
+        r.storage = {"fp32": STORAGE_FP32, "fp16": STORAGE_FP16, "bf16": STORAGE_BF16}[storage]
         r.streaming = STREAMING_SIMPLE if streaming == "Simple" else STREAMING_ESOTWIST
         r.les = int(les)
         if fields:

@@ -591,7 +591,7 @@ int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* ou
 
 int tdlb_batch_create_empty(int device, int streaming, int storage, tdlb_batch* out) {
     if (!out || (streaming != TDLB_STREAMING_SIMPLE && streaming != TDLB_STREAMING_ESOTWIST) ||
-        storage < TDLB_STORAGE_FP32 || storage > TDLB_STORAGE_I16) {
+        storage < TDLB_STORAGE_FP32 || storage > TDLB_STORAGE_BF16) {
         g_batch_create_error = "bad arguments";
         return TDLB_EINVAL;
     }

@@ -8,9 +8,10 @@
 //              excluded cells give -1 (the GPU kernel's value).
 //   plane      savePlaneXZ<float, 4> (ComputeUnitOutput.hpp:354-447): for
 //              every non-excluded cell of the plane, in (i, k) order, a
-//              tDiskGrid<float, 4> record (Output.hpp:22-26) of the first
-//              four moments, and a tDiskGrid<float, 3> record of F where F
-//              is non-zero.
+//              tDiskGrid<float, 4> record (Output.hpp:22-26) of Q slots 0..3
+//              (Simple: the first four moments; Esotwist: the raw slots,
+//              see k_plane_xz), and a tDiskGrid<float, 3> record of F where
+//              F is non-zero.
 //   exclude    setOutputExcludePoints / unsetOutputExcludePoints
 //              (ComputeUnitOutput.hpp:20-53): one bit per cell.
 //
@@ -85,26 +86,43 @@ __global__ void __launch_bounds__(256) k_vorticity(Planes A, Dims g, int mode, i
     out[o] = logf(b * b + c * c + a * a);
 }
 
-// The XZ plane at j: moments 0..3, F (zero where the last pass did not touch
-// the cell) and the excluded bit of every cell, out[(i * z + k) * 8 + l].
+// The XZ plane at j: Q slots 0..3 as the reference holds them, F (zero where
+// the last pass did not touch the cell) and the excluded bit of every cell,
+// out[(i * z + k) * 8 + l]. Simple: the cell's own first four moments.
+// Esotwist: the reference's savePlaneXZ copies the raw slots of its Q, which
+// after moments() hold the writeMoments placement -- slot s at location x is
+// moment d = (even ? s : s^1) of cell x - max(-c_d, 0) (wrapping) -- so each
+// slot is that moment of that cell.
 template <typename S>
 __global__ void __launch_bounds__(256) k_plane_xz(Planes A, Dims g, int mode, int even, CollideParams p, int j,
-                                                  const float* __restrict__ Fx, const float* __restrict__ Fy,
-                                                  const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
-                                                  const uint32_t* __restrict__ excl, float* __restrict__ out) {
+                                                  int esotwist, const float* __restrict__ Fx,
+                                                  const float* __restrict__ Fy, const float* __restrict__ Fz,
+                                                  const uint32_t* __restrict__ mask, const uint32_t* __restrict__ excl,
+                                                  float* __restrict__ out) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)g.nx * g.nz) return;
     const int i = (int)(t / g.nz), k = (int)(t - (long long)(t / g.nz) * g.nz);
     const long long row = (long long)i * g.ny + j;
     const long long e = row * g.kp + k;
-    float m[NQ];
-    state_moments18<S>(A, g, mode, even, p, i, j, k, m);
-    const bool on = (mask[row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
     float* o = out + t * 8;
-    o[0] = m[0];
-    o[1] = m[1];
-    o[2] = m[2];
-    o[3] = m[3];
+    float m[NQ];
+    if (!esotwist) {
+        state_moments18<S>(A, g, mode, even, p, i, j, k, m);
+        o[0] = m[0];
+        o[1] = m[1];
+        o[2] = m[2];
+        o[3] = m[3];
+    } else {
+        for (int s = 0; s < 4; s++) {
+            const int d = even ? s : (s ^ 1);
+            const int si = cx_of(d) < 0 ? (i == 0 ? g.nx - 1 : i - 1) : i;
+            const int sj = cy_of(d) < 0 ? (j == 0 ? g.ny - 1 : j - 1) : j;
+            const int sk = cz_of(d) < 0 ? (k == 0 ? g.nz - 1 : k - 1) : k;
+            state_moments18<S>(A, g, mode, even, p, si, sj, sk, m);
+            o[s] = m[d];
+        }
+    }
+    const bool on = (mask[row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
     o[4] = on ? Fx[e] : 0.f;
     o[5] = on ? Fy[e] : 0.f;
     o[6] = on ? Fz[e] : 0.f;
@@ -221,7 +239,9 @@ int tdlb_plane_xz(tdlb_handle h, int64_t j, tdlb_disk_grid4* q_out, size_t q_cap
         const Planes A = h->planes(h->state_buf());
         const int mode = h->state_mode(), even = h->even ? 1 : 0;
         tdlb::with_storage(h->cfg.storage, [&](auto s) {
-            tdlb::k_plane_xz<decltype(s)><<<blocks(n), 256, 0, h->stream>>>(A, g, mode, even, h->cp, (int)j, h->F,
+            tdlb::k_plane_xz<decltype(s)><<<blocks(n), 256, 0, h->stream>>>(A, g, mode, even, h->cp, (int)j,
+                                                                           h->cfg.streaming == TDLB_STREAMING_ESOTWIST,
+                                                                           h->F,
                                                                            h->F + g.plane, h->F + 2 * g.plane,
                                                                            h->mask_cur(), h->d_exclude, d.p);
         });

@@ -424,7 +424,7 @@ int tdlb_server_submit(tdlb_server s, const tdlb_request* r) {
     if (!s || !r) return TDLB_EINVAL;
     std::lock_guard<std::mutex> lk(s->mu);
     if (r->x < 8 || r->y < 8 || r->z < 8 || r->steps < 1 || r->tip_speed <= 0 || r->reynolds <= 0 ||
-        r->storage < TDLB_STORAGE_FP32 || r->storage > TDLB_STORAGE_I16 ||
+        r->storage < TDLB_STORAGE_FP32 || r->storage > TDLB_STORAGE_BF16 ||
         (r->streaming != TDLB_STREAMING_SIMPLE && r->streaming != TDLB_STREAMING_ESOTWIST)) {
         s->err = "bad request (sizes >= 8, steps >= 1, tip speed and Re > 0, known storage and streaming)";
         return TDLB_EINVAL;

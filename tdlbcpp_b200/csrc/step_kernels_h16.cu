@@ -1,6 +1,6 @@
-// 16-bit deviation storage (FP16, BF16 and 16-bit fixed point) instances of
-// the step kernels (step_kernels.cuh). Populations are stored as
-// f - w_d * rho0; collision and LES run in FP32. One and four cells per thread.
+// 16-bit deviation storage (FP16 and BF16) instances of the step kernels
+// (step_kernels.cuh). Populations are stored as f - w_d * rho0; collision and
+// LES run in FP32. One and four cells per thread.
 #include "step_kernels.cuh"
 
 namespace tdlb {

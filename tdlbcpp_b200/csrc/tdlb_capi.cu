@@ -83,12 +83,10 @@ void validate_config(const tdlb_config& c) {
     if (c.x > 32767 || c.y > 32767 || c.z > 32767) throw Fail{TDLB_EINVAL, "grid extent above 32767"};
     if (c.streaming != TDLB_STREAMING_SIMPLE && c.streaming != TDLB_STREAMING_ESOTWIST)
         throw Fail{TDLB_EINVAL, "streaming must be Simple (0) or Esotwist (1)"};
-    if (c.storage < TDLB_STORAGE_FP32 || c.storage > TDLB_STORAGE_I16)
-        throw Fail{TDLB_EINVAL, "storage must be FP32 (0), FP16 (1), BF16 (2) or I16 (3)"};
+    if (c.storage < TDLB_STORAGE_FP32 || c.storage > TDLB_STORAGE_BF16)
+        throw Fail{TDLB_EINVAL, "storage must be FP32 (0), FP16 (1) or BF16 (2)"};
     if (c.storage != TDLB_STORAGE_FP32 && !(c.initialRho > 0.0))
         throw Fail{TDLB_EINVAL, "16-bit storage needs initialRho > 0 (deviations are taken from it)"};
-    if (c.storage == TDLB_STORAGE_I16 && c.initialRho > 1.0)
-        throw Fail{TDLB_EINVAL, "I16 fixed-point storage needs initialRho <= 1 (its range is +-0.125)"};
     if (!(c.nu >= 0.0) || !std::isfinite(c.nu)) throw Fail{TDLB_EINVAL, "nu must be finite and >= 0"};
 }
 

@@ -55,7 +55,7 @@ struct Planes {
 // deviation f - w_d * rho0 from the rest weight of the direction's class
 // (w = 1/12 for faces, 1/24 for edges: the populations the Eggels-Somers
 // inverse filter gives at rest), and all arithmetic stays FP32.
-enum StorageKind { STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2, STORE_I16 = 3 };
+enum StorageKind { STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2 };
 
 template <typename S>
 struct Storage;
@@ -77,30 +77,14 @@ struct Storage<__nv_bfloat16> {
     __device__ __forceinline__ static float dec(__nv_bfloat16 x) { return __bfloat162float(x); }
     __device__ __forceinline__ static __nv_bfloat16 enc(float x) { return __float2bfloat16_rn(x); }
 };
-// 16-bit fixed point: the deviation in units of 2^-18 (range +-0.125, step
-// 3.8e-6, the same everywhere). Against FP16, whose step grows with the
-// value (1.5e-5 at 0.02-0.03, where the velocity term puts most
-// deviations), this rounds the large deviations 4-8x more finely; values
-// beyond the range saturate. Valid for initialRho <= 1.
-template <>
-struct Storage<short> {
-    static constexpr bool deviation = true;
-    static constexpr float kUnit = 1.0f / 262144.0f;
-    __device__ __forceinline__ static float dec(short x) { return (float)x * kUnit; }
-    __device__ __forceinline__ static short enc(float x) {
-        return (short)__float2int_rn(fminf(fmaxf(x * 262144.0f, -32767.0f), 32767.0f));
-    }
-};
-
 // Calls f with a value of the storage type of `kind` (float, __half,
-// __nv_bfloat16, short), so that one generic lambda launches the matching
-// kernel instance.
+// __nv_bfloat16), so that one generic lambda launches the matching kernel
+// instance.
 template <typename F>
 inline auto with_storage(int kind, F&& f) {
     switch (kind) {
         case STORE_F16: return f(__half());
         case STORE_BF16: return f(__nv_bfloat16());
-        case STORE_I16: return f(short());
         default: return f(float());
     }
 }
