@@ -207,6 +207,8 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
 #pragma unroll
         for (int d = 0; d < NQ; d++) pload<S, V, true>(A.p[d], q.e0, f[d]);
     } else if (V == 1) {
+        // direct (unaligned) read-only loads: the texture path serves the
+        // k-shifted rows better here than aligned loads plus lane shuffles
 #pragma unroll
         for (int d = 0; d < NQ; d++) {
             const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
@@ -321,13 +323,31 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
     const int last_e = g.nz - 1 - q.k0;   // element holding the row's last cell (if < V)
     float f[NQ][V];
     if (V == 1) {
-        const int k1 = q.k0 + 1 == g.nz ? 0 : q.k0 + 1;
+        // Slots with a k offset read element k + 1: every lane loads its own
+        // (aligned) element k and takes k + 1 from the next lane; the lane at
+        // a warp's end or a row's end loads its element itself.
+        const bool row_end = q.k0 == g.nz - 1;
+        const int k1 = row_end ? 0 : q.k0 + 1;
+        float v[NQ], x[NQ];
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
             const int sg = EVEN ? -1 : 1;
             const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
+            const int base = ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp;
+            v[s] = pload1<S, false>(Q.p[s], base + q.k0);
+            if (ok) x[s] = (lane == 31 || row_end) ? pload1<S, false>(Q.p[s], base + k1) : 0.f;
+        }
+#pragma unroll
+        for (int s = 0; s < NQ; s++) {
+            const int sg = EVEN ? -1 : 1;
+            const bool ok = sg * cz_of(s) > 0;
             const int d = EVEN ? s : (s ^ 1);
-            f[d][0] = pload1<S, false>(Q.p[s], ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp + (ok ? k1 : q.k0));
+            if (ok) {
+                const float right = __shfl_down_sync(FULL, v[s], 1);
+                f[d][0] = (lane == 31 || row_end) ? x[s] : right;
+            } else {
+                f[d][0] = v[s];
+            }
         }
     } else {
         float hal[NQ], wrap[NQ];
@@ -377,16 +397,27 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
             for (int e = 0; e < V; e++) f[d][e] -= rest_of<S>(d, p);
     }
     if (V == 1) {
-        if (!q.active) return;
-        const int k1 = q.k0 + 1 == g.nz ? 0 : q.k0 + 1;
+        // Slots with a k offset write element k + 1: lane l writes element k
+        // with the value of the previous lane (cell k - 1, same row), so the
+        // warp's store is aligned; the lane at a warp's end or a row's end
+        // writes its own element k + 1 (k = nz - 1: element 0) itself.
+        const bool row_end = q.k0 == g.nz - 1;
+        const int k1 = row_end ? 0 : q.k0 + 1;
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
             const int sg = EVEN ? -1 : 1;
             const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
             const int d = EVEN ? (s ^ 1) : s;
-            pstore1<S>(Q.p[s], ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp + (ok ? k1 : q.k0), f[d][0]);
+            const int base = ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp;
+            if (!ok) {
+                if (q.active) pstore1<S>(Q.p[s], base + q.k0, f[d][0]);
+                continue;
+            }
+            const float left = __shfl_up_sync(FULL, f[d][0], 1);
+            if (lane > 0 && q.k0 > 0 && q.k0 <= g.nz - 1 && q.active) pstore1<S>(Q.p[s], base + q.k0, left);
+            if (q.active && (lane == 31 || row_end)) pstore1<S>(Q.p[s], base + k1, f[d][0]);
         }
-        if (COLLIDE && LES) Nu[q.e0] = nu[0];
+        if (COLLIDE && LES && q.active) Nu[q.e0] = nu[0];
         return;
     }
     const bool k_first = q.k0 == 0;
