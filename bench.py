@@ -130,12 +130,12 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- our arm
 
-def make_unit(tb, workload: str, edge: int, device: int):
+def make_unit(tb, workload: str, edge: int, device: int, storage: str = "fp32"):
     rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=TIP, startup_steps=0)
     nu = tb.nu_from_reynolds(RE, TIP, rt.blade_outer_radius())
     streaming = tb.STREAMING_ESOTWIST if workload == "esotwist" else tb.STREAMING_SIMPLE
     cu = tb.ComputeUnit(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0,
-                        streaming=streaming, device=device)
+                        streaming=streaming, device=device, storage=storage)
     return cu, rt, nu
 
 
@@ -145,7 +145,7 @@ def run_ours(args, rank, world, device):
 
     torch.cuda.set_device(device)
     edge = args.edge
-    cu, rt, nu = make_unit(tb, args.workload, edge, device)
+    cu, rt, nu = make_unit(tb, args.workload, edge, device, args.storage)
     stream = torch.cuda.ExternalStream(cu.stream, device=device)
     dth = rt.increment(1)
     cu.attach_rushton(rt, dth, 0.0, dth)
@@ -156,37 +156,46 @@ def run_ours(args, rank, world, device):
     cells = edge ** 3
     angle = 0.0
 
-    def device_step(ev0=None, ev1=None):
+    def device_step():
         nonlocal angle
         angle += dth
         cu.rotate_impeller(angle, dth)
-        if ev0 is not None:
-            ev0.record(stream)
         cu.collision()
-        if ev1 is not None:
-            ev1.record(stream)
         cu.forcing_resident(ALPHA, BETA)
 
+    cu.set_overlap(args.overlap)
     for _ in range(args.warmup):
         device_step()
     cu.synchronize()
+    try:
+        zone = cu.read_zone() if args.overlap else None
+    except tb.TdlbError:
+        zone = None   # the zone covers most of this lattice: steps are not split
 
-    # ---- value: device-resident steps
-    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # ---- value: device-resident steps. The library brackets every step-kernel
+    # launch with CUDA events on the stream it runs on (a split step is two
+    # launches on two streams); t1 follows a join of both streams.
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(world)
     cu.synchronize()
     torch.cuda.synchronize()
+    cu.kernel_time()
+    cu.set_kernel_timing(True)
+    launches0 = cu.kernel_launches()
     with ClockSampler(device) as clk:
         t0.record(stream)
         for s in range(args.steps):
-            device_step(*kev[s])
+            device_step()
+        cu.join()
         t1.record(stream)
         cu.synchronize()
         torch.cuda.synchronize()
     barrier(world)
+    launches = cu.kernel_launches() - launches0
+    kernel_total_ms, kernel_n = cu.kernel_time()
+    cu.set_kernel_timing(False)
     ms = t0.elapsed_time(t1)
-    kernel_ms = sum(a.elapsed_time(b) for a, b in kev) / args.steps
+    kernel_ms = kernel_total_ms / args.steps
     ms = max_over_ranks(ms, world)
     kernel_ms_max = max_over_ranks(kernel_ms, world)
 
@@ -237,6 +246,9 @@ def run_ours(args, rank, world, device):
         "load": load_np.tolist(),
         "fields_finite": bool(np.isfinite(red).all() and np.isfinite(load_np).all()),
         "mass_drift": float(red[0] / cells - 1.0),
+        "launches": launches,
+        "step_launches": kernel_n,
+        "inner_fraction": None if zone is None else float(zone.mean()),
     }
     return result
 
@@ -426,6 +438,7 @@ def gpu_precision_run(tb, edge, storage, steps, device, timed=False):
         cu.rotate_impeller(angle, d)
         cu.collision()
         cu.forcing_resident(ALPHA, BETA)
+    cu.join()
     t1.record(st)
     cu.synchronize()
     ms = t0.elapsed_time(t1)
@@ -794,7 +807,8 @@ def report_batched(args, rank, world, local, config):
     line = {
         "metric": "MLUPS", "value": res["value_mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": config,
+        "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic", "config": config,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "kernel": "k_batch_step", "bytes_per_cell": bpc,
                      "kernel_ms": res["kernel_ms"], "traffic": None},
@@ -823,6 +837,10 @@ def main():
     ap.add_argument("--chunk", type=int, default=100, help="serving: steps per batched chunk")
     ap.add_argument("--edge", type=int, default=EDGE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--overlap", action="store_true",
+                    help="simple/esotwist: split steps (outer cells overlap the previous forcing pass)")
+    ap.add_argument("--storage", choices=["fp32", "fp16", "bf16"], default="fp32",
+                    help="simple/esotwist: population storage (16-bit forms store deviations from the rest weights)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3   # timing rule: at least 3 warm-up steps
@@ -849,7 +867,7 @@ def main():
                   "streaming": "Esotwist", "collision": "EgglesSomers+LES(cs0=0.1)", "ibm": "Rushton turbine, rotating",
                   "l2": "lattices > L2 every step (no flush needed)"}
     else:
-        workload = f"rushton-{args.edge}^3-{args.workload}-fp32-les"
+        workload = f"rushton-{args.edge}^3-{args.workload}-{args.storage}-les"
         config = {"workload": workload, "grid": [args.edge] * 3, "streaming": args.workload.capitalize(),
                   "collision": "EgglesSomers+LES(cs0=0.1)", "re": RE, "tip_speed": TIP,
                   "ibm": "Rushton turbine, rotating", "l2": "lattice > L2 every step (no flush needed)"}
@@ -884,22 +902,25 @@ def main():
         return 0
     peak, peak_kind = measured_peak()
     cells = args.edge ** 3
-    bpc = 152
+    bpc = 152 if args.storage == "fp32" else 80
     achieved = bpc * cells / (res["kernel_ms"] / 1e3) / 1e9
     traffic_pc = profile_traffic(workload)
     line = {
         "metric": "MLUPS", "value": res["value_mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": config,
+        "vs_baseline": None, "dtype": "fp32" if args.storage == "fp32" else f"fp32 arithmetic, {args.storage} storage",
+        "data": "synthetic", "config": config,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "kernel": "k_step_simple" if args.workload == "simple" else "k_step_esotwist",
                      "bytes_per_cell": bpc, "kernel_ms": res["kernel_ms"],
                      "traffic": None if traffic_pc is None else traffic_pc * cells},
         "e2e": {"value": res["e2e_mlups"], "unit": "MLUPS", "h2d_bytes_per_step": res["h2d"],
                 "d2h_bytes_per_step": res["d2h"], "steps": res["e2e_steps"]},
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": res["launches"],
         "clocks": res["clocks"],
         "markers": res["n_markers"],
+        "split_step": {"on": res["inner_fraction"] is not None, "inner_cell_fraction": res["inner_fraction"],
+                       "step_launches_per_step": res["step_launches"] / args.steps},
         "fields_finite": res["fields_finite"],
         "mass_drift": res["mass_drift"],
     }

@@ -245,6 +245,42 @@ int tdlb_checkpoint_read(tdlb_handle h, const char* dir, const char* unit_name);
  * compute identical results. */
 int tdlb_set_cells_per_thread(tdlb_handle h, int v);
 
+/* Split steps. mode 0 (default): off; 1: on when the inner chunks hold at
+ * most 60 % of the lattice (large tanks; a small one is mostly stencil
+ * cells); 2: on whenever possible. With resident markers (tdlb_set_markers
+ * or tdlb_attach_rushton) and one cell per thread, a step runs as two launches:
+ * the cells outside every marker stencil (the "outer" chunks, which read no
+ * force) on the handle's stream, and the stencil cells and their neighbours
+ * (the "inner" chunks) on a second stream, after the forcing pass. The
+ * previous step's forcing pass then runs while the outer cells of the next
+ * step are computed. Every cell computes what the single launch computes,
+ * so results are bit-identical with overlap on and off. Measured on B200
+ * at 400^3 (Rushton tank): whole steps 0-4 % faster, because the two
+ * launches over scattered chunks lose most of what the overlap hides, hence
+ * off by default. Entry points other
+ * than tdlb_collision, tdlb_forcing_resident, tdlb_rotate_impeller and
+ * tdlb_step first order the handle's stream after that second stream. */
+int tdlb_set_overlap(tdlb_handle h, int mode);
+
+/* Order the handle's stream (tdlb_get_stream) after every queued step and
+ * forcing pass, without waiting on the host. */
+int tdlb_join(tdlb_handle h);
+
+/* Per-cell flags (interior cells in (i, j, k) order) of the split-step zone:
+ * 1 where the cell belongs to an inner chunk. TDLB_ESTATE when the handle
+ * does not split its steps (see tdlb_set_overlap). */
+int tdlb_read_zone(tdlb_handle h, uint8_t* flags);
+
+/* Step-kernel timing: when on, every step-kernel launch (both launches of a
+ * split step) is bracketed by CUDA events on its own stream.
+ * tdlb_kernel_time waits for the device, returns the summed launch time in
+ * ms and the number of launches since the last call, and resets both. */
+int tdlb_set_kernel_timing(tdlb_handle h, int on);
+/* Kernels the handle's step loop has queued so far (step launches, forcing
+ * passes, blade rotations). */
+int tdlb_kernel_launches(tdlb_handle h, int64_t* n);
+int tdlb_kernel_time(tdlb_handle h, double* total_ms, int64_t* launches);
+
 /* The cudaStream_t (as void*) all of h's device work is queued on, for
  * callers that time it with CUDA events or order their own work after it. */
 int tdlb_get_stream(tdlb_handle h, void** stream);

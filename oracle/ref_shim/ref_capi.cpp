@@ -59,7 +59,11 @@ DiskOutputTree makeTree(const std::string& tmpdir) {
     CheckpointParams chk;
     chk.checkpointWriteRootDir = tmpdir;
     chk.checkpointWriteDirPrefix = "ref";
-    return DiskOutputTree(out, chk);
+    DiskOutputTree tree(out, chk);
+    // the reference's progress log goes below tmpdir, not into the caller's
+    // working directory (DiskOutputTree.h:80, :273-280)
+    tree.setRunningDataFile(tmpdir, "ref_running_data.txt");
+    return tree;
 }
 
 ComputeUnitParams makeCuParams(long x, long y, long z) {

@@ -204,6 +204,12 @@ def load_library() -> ctypes.CDLL:
         "tdlb_impeller_load_noalloc": (i32, [H, vp]),
         "tdlb_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "tdlb_set_cells_per_thread": (i32, [H, i32]),
+        "tdlb_set_overlap": (i32, [H, i32]),
+        "tdlb_join": (i32, [H]),
+        "tdlb_read_zone": (i32, [H, vp]),
+        "tdlb_set_kernel_timing": (i32, [H, i32]),
+        "tdlb_kernel_launches": (i32, [H, ctypes.POINTER(ctypes.c_int64)]),
+        "tdlb_kernel_time": (i32, [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),
         "tdlb_reduce_fp64": (i32, [H, vp]),
         "tdlb_checkpoint_write": (i32, [H, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]),
         "tdlb_checkpoint_read": (i32, [H, ctypes.c_char_p, ctypes.c_char_p]),
@@ -440,6 +446,41 @@ class ComputeUnit:
     def set_cells_per_thread(self, v: int):
         """Step-kernel variant (1, 2 or 4 cells per thread); results are identical."""
         self._check(self.lib.tdlb_set_cells_per_thread(self.h, v))
+
+    def set_overlap(self, mode):
+        """Split steps: the outer cells of a step run while the previous
+        forcing pass is in flight; results are identical. False/0 (default):
+        off; True/1: when the inner chunks hold at most 60 % of the lattice;
+        "always"/2: whenever the markers are resident."""
+        m = 2 if mode == "always" else int(bool(mode)) if isinstance(mode, bool) else int(mode)
+        self._check(self.lib.tdlb_set_overlap(self.h, m))
+
+    def join(self):
+        """Order this unit's stream after every queued step and forcing pass
+        (no host wait): call before recording an event on `stream`."""
+        self._check(self.lib.tdlb_join(self.h))
+
+    def read_zone(self) -> np.ndarray:
+        """Per-cell flags of the split-step inner chunks."""
+        out = np.empty((self.x, self.y, self.z), np.uint8)
+        self._check(self.lib.tdlb_read_zone(self.h, _p(out)))
+        return out
+
+    def set_kernel_timing(self, on: bool):
+        """Bracket every step-kernel launch with CUDA events on its stream."""
+        self._check(self.lib.tdlb_set_kernel_timing(self.h, 1 if on else 0))
+
+    def kernel_time(self):
+        """(summed step-kernel ms, launches) since the last call; waits for the device."""
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        self._check(self.lib.tdlb_kernel_time(self.h, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def kernel_launches(self) -> int:
+        """Kernels the step loop has queued so far."""
+        n = ctypes.c_int64()
+        self._check(self.lib.tdlb_kernel_launches(self.h, ctypes.byref(n)))
+        return n.value
 
     def impeller_load_noalloc(self, device_ptr: int):
         """Allocation-free impeller load into a caller-owned device buffer of

@@ -157,6 +157,8 @@ int cguard(tdlb_lattice* h, F&& fn) {
     if (!h) return TDLB_EINVAL;
     try {
         cudaSetDevice(h->device);
+        const cudaError_t je = tdlb_rt::join_side(h);   // after every queued step and forcing pass
+        if (je != cudaSuccess) throw CFail{TDLB_ECUDA, std::string("join: ") + cudaGetErrorString(je)};
         fn();
         return TDLB_OK;
     } catch (const CFail& f) {
@@ -451,8 +453,7 @@ int tdlb_checkpoint_read(tdlb_handle h, const char* dir, const char* unit_name) 
         TDLB_CCK(cudaStreamSynchronize(h->stream));
         h->cfg = c;
         h->cp = tdlb::make_collide_params(c.nu, c.cs0, c.g3);
-        h->cp.wface = (float)(c.initialRho / 12.0);
-        h->cp.wedge = (float)(c.initialRho / 24.0);
+        tdlb::set_rest(h->cp, c.initialRho);
         h->cur = 0;
         h->pass = 0;
         h->even = even;

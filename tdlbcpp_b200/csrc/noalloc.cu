@@ -116,6 +116,7 @@ extern "C" int tdlb_impeller_load_noalloc(tdlb_handle h, double* d_out5) {
     if ((long long)h->n_markers > (long long)kNoAllocChunk * kNoAllocMaxBlocks)
         return fail(h, TDLB_EINVAL, "marker list longer than the 1048576 markers tdlb_impeller_load_noalloc supports");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, TDLB_ECUDA, "cudaSetDevice failed");
+    if (tdlb_rt::join_side(h) != cudaSuccess) return fail(h, TDLB_ECUDA, "join of the split-step stream failed");
     double* partial = nullptr;
     if (partials_address(h->device, &partial) != cudaSuccess)
         return fail(h, TDLB_ECUDA, "cudaGetSymbolAddress of the no-allocation scratch failed");

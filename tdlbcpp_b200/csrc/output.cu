@@ -149,6 +149,8 @@ int oguard(tdlb_lattice* h, F&& fn) {
     if (!h) return TDLB_EINVAL;
     try {
         cudaSetDevice(h->device);
+        const cudaError_t je = tdlb_rt::join_side(h);   // after every queued step and forcing pass
+        if (je != cudaSuccess) throw OFail{TDLB_ECUDA, std::string("join: ") + cudaGetErrorString(je)};
         fn();
         return TDLB_OK;
     } catch (const OFail& f) {

@@ -86,19 +86,15 @@ int tdlb_double_resolution(tdlb_handle h) {
     uint32_t* mask = nullptr;
     try {
         cudaSetDevice(h->device);
+        TDLB_RCK(tdlb_rt::join_side(h));
+        TDLB_RCK(cudaStreamSynchronize(h->stream));   // the old buffers are freed below
         if (!h->initialised) throw RFail{TDLB_ESTATE, "not initialised (tdlb_initialise)"};
         if (h->own_stream) throw RFail{TDLB_ESTATE, "a tank of a batch cannot change size"};
         if (h->cfg.storage != TDLB_STORAGE_FP32) throw RFail{TDLB_EINVAL, "resolution doubling needs FP32 storage"};
         const Dims g = h->g;
         if ((long long)g.nx * 2 > 32767 || (long long)g.ny * 2 > 32767 || (long long)g.nz * 2 > 32767)
             throw RFail{TDLB_EINVAL, "doubled grid extent above 32767"};
-        Dims n{};
-        n.nx = g.nx * 2;
-        n.ny = g.ny * 2;
-        n.nz = g.nz * 2;
-        n.kp = (int)round_up_ll(n.nz, 16);
-        n.kw = (n.kp + 31) / 32;
-        n.plane = round_up_ll((long long)n.nx * n.ny * n.kp, 64);
+        const Dims n = tdlb::make_dims(g.nx * 2, g.ny * 2, g.nz * 2);
         if ((long long)n.nx * n.ny * n.kp >= (1LL << 31) - 64)
             throw RFail{TDLB_EINVAL, "doubled lattice too large: one plane must stay below 2^31 elements"};
         const long long words = round_up_ll((long long)n.nx * n.ny * n.kw, 64);
@@ -140,12 +136,7 @@ int tdlb_double_resolution(tdlb_handle h) {
     h->F = F;
     h->mask = mask;
     Dims& g = h->g;
-    g.nx *= 2;
-    g.ny *= 2;
-    g.nz *= 2;
-    g.kp = (int)round_up_ll(g.nz, 16);
-    g.kw = (g.kp + 31) / 32;
-    g.plane = round_up_ll((long long)g.nx * g.ny * g.kp, 64);
+    g = tdlb::make_dims(g.nx * 2, g.ny * 2, g.nz * 2);
     h->mask_words = round_up_ll((long long)g.nx * g.ny * g.kw, 64);
     h->cfg.x *= 2;
     h->cfg.y *= 2;
@@ -171,6 +162,9 @@ int tdlb_double_resolution(tdlb_handle h) {
     h->h_plane_list.clear();
     drop(h->d_rot_xz);
     h->marker_gen++;
+    h->resident = false;
+    h->inner_queued = false;
+    h->h_rot_xz.clear();
     return TDLB_OK;
 }
 

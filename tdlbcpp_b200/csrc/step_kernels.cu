@@ -48,35 +48,67 @@ __global__ void k_fill_uniform_moments(Planes Q, Dims g, float rho) {
 // ---------------------------------------------------------------------------
 static inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+// Grid of a launch: every quad (part 0) or one warp per listed chunk (1, 2).
+static inline unsigned step_blocks(const StepArgs& a, int V) {
+    if (a.part != 0) return blocks_for((long long)a.zone.count * 32, 128);
+    return blocks_for(a.g.rows() * (a.g.kp / V), 128);
+}
+
 template <int V>
 static cudaError_t launch_simple_v(const StepArgs& a, cudaStream_t st) {
-    const long long nquads = a.g.rows() * (a.g.kp / V);
-    const dim3 grid(blocks_for(nquads, 128)), block(128);
-#define TDLB_SIMPLE(LES, FM, COL) k_step_simple<float, V, LES, FM, COL><<<grid, block, 0, st>>>(a.A, a.B, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p)
-    if (!a.collide) TDLB_SIMPLE(false, false, false);
-    else if (a.les) { if (a.from_moments) TDLB_SIMPLE(true, true, true); else TDLB_SIMPLE(true, false, true); }
-    else { if (a.from_moments) TDLB_SIMPLE(false, true, true); else TDLB_SIMPLE(false, false, true); }
+    const dim3 grid(step_blocks(a, V)), block(128);
+#define TDLB_SIMPLE(LES, FM, COL, PART)                                                                       \
+    k_step_simple<float, V, LES, FM, COL, PART><<<grid, block, 0, st>>>(a.A, a.B, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, \
+                                                                      a.g, a.p, a.zone)
+    if (!a.collide) TDLB_SIMPLE(false, false, false, 0);
+    else if (a.from_moments) { if (a.les) TDLB_SIMPLE(true, true, true, 0); else TDLB_SIMPLE(false, true, true, 0); }
+    else if constexpr (V == 1) {
+        if (a.les) {
+            if (a.part == 1) TDLB_SIMPLE(true, false, true, 1);
+            else if (a.part == 2) TDLB_SIMPLE(true, false, true, 2);
+            else TDLB_SIMPLE(true, false, true, 0);
+        } else {
+            if (a.part == 1) TDLB_SIMPLE(false, false, true, 1);
+            else if (a.part == 2) TDLB_SIMPLE(false, false, true, 2);
+            else TDLB_SIMPLE(false, false, true, 0);
+        }
+    } else {
+        if (a.les) TDLB_SIMPLE(true, false, true, 0); else TDLB_SIMPLE(false, false, true, 0);
+    }
 #undef TDLB_SIMPLE
     return cudaGetLastError();
 }
 
+template <int V, bool LES, bool FM, bool COL, int PART>
+static void eso_launch(const StepArgs& a, dim3 grid, cudaStream_t st) {
+    if (a.even) k_step_esotwist<float, V, LES, FM, COL, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone);
+    else k_step_esotwist<float, V, LES, FM, COL, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone);
+}
+
 template <int V>
 static cudaError_t launch_esotwist_v(const StepArgs& a, cudaStream_t st) {
-    const long long nquads = a.g.rows() * (a.g.kp / V);
-    const dim3 grid(blocks_for(nquads, 128)), block(128);
-#define TDLB_ESO(LES, FM, COL)                                                                                        \
-    do {                                                                                                              \
-        if (a.even) k_step_esotwist<float, V, LES, FM, COL, true><<<grid, block, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p); \
-        else k_step_esotwist<float, V, LES, FM, COL, false><<<grid, block, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p); \
-    } while (0)
-    if (!a.collide) TDLB_ESO(false, false, false);
-    else if (a.les) { if (a.from_moments) TDLB_ESO(true, true, true); else TDLB_ESO(true, false, true); }
-    else { if (a.from_moments) TDLB_ESO(false, true, true); else TDLB_ESO(false, false, true); }
-#undef TDLB_ESO
+    const dim3 grid(step_blocks(a, V));
+    if (!a.collide) eso_launch<V, false, false, false, 0>(a, grid, st);
+    else if (a.from_moments) {
+        if (a.les) eso_launch<V, true, true, true, 0>(a, grid, st); else eso_launch<V, false, true, true, 0>(a, grid, st);
+    } else if constexpr (V == 1) {
+        if (a.les) {
+            if (a.part == 1) eso_launch<1, true, false, true, 1>(a, grid, st);
+            else if (a.part == 2) eso_launch<1, true, false, true, 2>(a, grid, st);
+            else eso_launch<1, true, false, true, 0>(a, grid, st);
+        } else {
+            if (a.part == 1) eso_launch<1, false, false, true, 1>(a, grid, st);
+            else if (a.part == 2) eso_launch<1, false, false, true, 2>(a, grid, st);
+            else eso_launch<1, false, false, true, 0>(a, grid, st);
+        }
+    } else {
+        if (a.les) eso_launch<V, true, false, true, 0>(a, grid, st); else eso_launch<V, false, false, true, 0>(a, grid, st);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st) {
+    if (a.part != 0 && (a.vec != 1 || a.from_moments || !a.collide)) return cudaErrorInvalidValue;
     if (a.storage != STORE_F32) return launch_step_simple_h16(a, st);
     switch (a.vec) {
         case 1: return launch_simple_v<1>(a, st);
@@ -86,6 +118,7 @@ cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_step_esotwist(const StepArgs& a, cudaStream_t st) {
+    if (a.part != 0 && (a.vec != 1 || a.from_moments || !a.collide)) return cudaErrorInvalidValue;
     if (a.storage != STORE_F32) return launch_step_esotwist_h16(a, st);
     switch (a.vec) {
         case 1: return launch_esotwist_v<1>(a, st);

@@ -124,15 +124,28 @@ struct Quad {
     bool active;      // k0 < nz (the quad holds at least one cell)
 };
 
-template <int V>
+// MUL_DIV: divide by multiply-high (Dims::by_kp16, by_ny). Measured on B200
+// at 400^3: 5 % faster for the 16-bit kernels (issue-bound), but 4-11 %
+// slower for the FP32 ones, whose loads the compiler then schedules worse;
+// the FP32 kernels keep the hardware division sequence.
+template <int V, bool MUL_DIV>
 __device__ __forceinline__ Quad quad_of(const Dims& g, int nq, unsigned t) {
     Quad q;
     const unsigned total = (unsigned)g.nx * (unsigned)g.ny * (unsigned)nq;
     const unsigned tc = t < total ? t : total - 1;   // keep spare lanes on a valid quad
-    const unsigned row = tc / (unsigned)nq;
+    // tc / nq = (tc / (16 / V)) / (kp / 16), nq = kp / V
+    constexpr unsigned kShift = V == 1 ? 4 : V == 2 ? 3 : V == 4 ? 2 : 1;
+    static_assert(V == 1 || V == 2 || V == 4 || V == 8, "cells per thread");
+    unsigned row;
+    if (MUL_DIV) {
+        row = g.by_kp16.div(tc >> kShift);
+        q.i = (int)g.by_ny.div(row);
+    } else {
+        row = tc / (unsigned)nq;
+        q.i = (int)(row / (unsigned)g.ny);
+    }
     const int kq = (int)(tc - row * (unsigned)nq);
     q.row = (int)row;
-    q.i = (int)(row / (unsigned)g.ny);
     q.j = (int)row - q.i * g.ny;
     q.k0 = kq * V;
     q.e0 = (int)row * g.kp + q.k0;
@@ -140,14 +153,18 @@ __device__ __forceinline__ Quad quad_of(const Dims& g, int nq, unsigned t) {
     return q;
 }
 
-template <int V, bool LES, bool COLLIDE>
+// FORCE = false: the cells are known to lie outside every immersed-boundary
+// stencil (the outer part of a split step), so F is zero without reading the
+// touched flags.
+template <int V, bool LES, bool COLLIDE, bool DEV, bool FORCE = true>
 __device__ __forceinline__ void collide_quad(float (&f)[NQ][V], const Quad& q, float* __restrict__ Nu,
                                              const float* __restrict__ Fx, const float* __restrict__ Fy,
                                              const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
                                              const Dims& g, const CollideParams& p, bool from_moments, float (&nu)[V]) {
     if (!COLLIDE) return;
     float fx[V], fy[V], fz[V];
-    const uint32_t bits = (__ldg(mask + (size_t)q.row * g.kw + (q.k0 >> 5)) >> (q.k0 & 31)) & ((1u << V) - 1u);
+    const uint32_t bits =
+        FORCE ? (__ldg(mask + (size_t)q.row * g.kw + (q.k0 >> 5)) >> (q.k0 & 31)) & ((1u << V) - 1u) : 0u;
     if (bits) {
         vload<V>(Fx + q.e0, fx);
         vload<V>(Fy + q.e0, fy);
@@ -172,7 +189,7 @@ __device__ __forceinline__ void collide_quad(float (&f)[NQ][V], const Quad& q, f
             moments_of(qv, m);
         }
         float n = LES ? nu[e] : 0.f;
-        collide<LES>(m, fx[e], fy[e], fz[e], n, p, qv);
+        collide<LES, DEV>(m, fx[e], fy[e], fz[e], n, p, qv);
         if (LES) nu[e] = n;
 #pragma unroll
         for (int d = 0; d < NQ; d++) f[d][e] = qv[d];
@@ -191,13 +208,14 @@ __device__ __forceinline__ void collide_quad(float (&f)[NQ][V], const Quad& q, f
 // scalar loads issued in the same batch (in bounds for every lane; the ones
 // a lane does not need hit L1).
 // ---------------------------------------------------------------------------
-template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE>
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool FORCE = true>
 __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, float* __restrict__ Nu,
                                             const float* __restrict__ Fx, const float* __restrict__ Fy,
                                             const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
                                             const Dims& g, const CollideParams& p, unsigned t) {
+    static_assert(!(Storage<S>::deviation && FROM_MOMENTS), "16-bit state always holds populations");
     const int nq = g.kp / V;
-    const Quad q = quad_of<V>(g, nq, t);
+    const Quad q = quad_of<V, sizeof(S) == 2>(g, nq, t);
     const int lane = threadIdx.x & 31;
     const int rs = g.ny * g.kp;   // elements per i step
     const bool i_lo = q.i == 0, i_hi = q.i == g.nx - 1, j_lo = q.j == 0, j_hi = q.j == g.ny - 1;
@@ -275,23 +293,11 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
             }
         }
     }
-    if (Storage<S>::deviation) {
-#pragma unroll
-        for (int d = 0; d < NQ; d++)
-#pragma unroll
-            for (int e = 0; e < V; e++) f[d][e] += rest_of<S>(d, p);
-    }
     float nu[V];
-    collide_quad<V, LES, COLLIDE>(f, q, Nu, Fx, Fy, Fz, mask, g, p, FROM_MOMENTS, nu);
+    collide_quad<V, LES, COLLIDE, Storage<S>::deviation, FORCE>(f, q, Nu, Fx, Fy, Fz, mask, g, p, FROM_MOMENTS, nu);
     if (!q.active) return;
 #pragma unroll
-    for (int d = 0; d < NQ; d++) {
-        if (Storage<S>::deviation) {
-#pragma unroll
-            for (int e = 0; e < V; e++) f[d][e] -= rest_of<S>(d, p);
-        }
-        pstore<S, V>(B.p[d], q.e0, f[d]);
-    }
+    for (int d = 0; d < NQ; d++) pstore<S, V>(B.p[d], q.e0, f[d]);
     if (COLLIDE && LES) vstore<V>(Nu + q.e0, nu);
 }
 
@@ -309,13 +315,14 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
 // loads from any lane's stores, so a location is always read by its owner
 // before a neighbour overwrites it.
 // ---------------------------------------------------------------------------
-template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN>
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN, bool FORCE = true>
 __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict__ Nu, const float* __restrict__ Fx,
                                               const float* __restrict__ Fy, const float* __restrict__ Fz,
                                               const uint32_t* __restrict__ mask, const Dims& g, const CollideParams& p,
                                               unsigned t) {
+    static_assert(!(Storage<S>::deviation && FROM_MOMENTS), "16-bit state always holds populations");
     const int nq = g.kp / V;
-    const Quad q = quad_of<V>(g, nq, t);
+    const Quad q = quad_of<V, sizeof(S) == 2>(g, nq, t);
     const int lane = threadIdx.x & 31;
     const int i1 = q.i + 1 == g.nx ? 0 : q.i + 1;
     const int j1 = q.j + 1 == g.ny ? 0 : q.j + 1;
@@ -325,9 +332,11 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
     if (V == 1) {
         // Slots with a k offset read element k + 1: every lane loads its own
         // (aligned) element k and takes k + 1 from the next lane; the lane at
-        // a warp's end or a row's end loads its element itself.
+        // a warp's end or a row's end loads its element itself. (Padding
+        // lanes, k >= nz, load element 0 of their row: in bounds, unused.)
         const bool row_end = q.k0 == g.nz - 1;
-        const int k1 = row_end ? 0 : q.k0 + 1;
+        const bool warp_end = lane == 31;
+        const int k1 = (row_end || q.k0 >= g.nz) ? 0 : q.k0 + 1;
         float v[NQ], x[NQ];
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
@@ -335,7 +344,7 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
             const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
             const int base = ((oi ? i1 : q.i) * g.ny + (oj ? j1 : q.j)) * g.kp;
             v[s] = pload1<S, false>(Q.p[s], base + q.k0);
-            if (ok) x[s] = (lane == 31 || row_end) ? pload1<S, false>(Q.p[s], base + k1) : 0.f;
+            if (ok) x[s] = (warp_end || row_end) ? pload1<S, false>(Q.p[s], base + k1) : 0.f;
         }
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
@@ -344,7 +353,7 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
             const int d = EVEN ? s : (s ^ 1);
             if (ok) {
                 const float right = __shfl_down_sync(FULL, v[s], 1);
-                f[d][0] = (lane == 31 || row_end) ? x[s] : right;
+                f[d][0] = (warp_end || row_end) ? x[s] : right;
             } else {
                 f[d][0] = v[s];
             }
@@ -382,27 +391,16 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
         }
     }
     __syncwarp();
-    if (Storage<S>::deviation) {
-#pragma unroll
-        for (int d = 0; d < NQ; d++)
-#pragma unroll
-            for (int e = 0; e < V; e++) f[d][e] += rest_of<S>(d, p);
-    }
     float nu[V];
-    collide_quad<V, LES, COLLIDE>(f, q, Nu, Fx, Fy, Fz, mask, g, p, FROM_MOMENTS, nu);
-    if (Storage<S>::deviation) {
-#pragma unroll
-        for (int d = 0; d < NQ; d++)
-#pragma unroll
-            for (int e = 0; e < V; e++) f[d][e] -= rest_of<S>(d, p);
-    }
+    collide_quad<V, LES, COLLIDE, Storage<S>::deviation, FORCE>(f, q, Nu, Fx, Fy, Fz, mask, g, p, FROM_MOMENTS, nu);
     if (V == 1) {
         // Slots with a k offset write element k + 1: lane l writes element k
         // with the value of the previous lane (cell k - 1, same row), so the
         // warp's store is aligned; the lane at a warp's end or a row's end
         // writes its own element k + 1 (k = nz - 1: element 0) itself.
         const bool row_end = q.k0 == g.nz - 1;
-        const int k1 = row_end ? 0 : q.k0 + 1;
+        const bool warp_end = lane == 31;
+        const int k1 = (row_end || q.k0 >= g.nz) ? 0 : q.k0 + 1;
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
             const int sg = EVEN ? -1 : 1;
@@ -414,8 +412,9 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
                 continue;
             }
             const float left = __shfl_up_sync(FULL, f[d][0], 1);
-            if (lane > 0 && q.k0 > 0 && q.k0 <= g.nz - 1 && q.active) pstore1<S>(Q.p[s], base + q.k0, left);
-            if (q.active && (lane == 31 || row_end)) pstore1<S>(Q.p[s], base + k1, f[d][0]);
+            if (lane > 0 && q.k0 > 0 && q.k0 <= g.nz - 1 && q.active)
+                pstore1<S>(Q.p[s], base + q.k0, left);
+            if (q.active && (warp_end || row_end)) pstore1<S>(Q.p[s], base + k1, f[d][0]);
         }
         if (COLLIDE && LES && q.active) Nu[q.e0] = nu[0];
         return;
@@ -455,12 +454,35 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
 }
 
 
-template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE>
+// Split step (one cell per thread). The immersed-boundary pass of a step
+// touches a thin set of cells, so a step can run as two launches over
+// 32-cell chunks of the flat (row, k) index, one warp per listed chunk:
+//   PART 1 (outer): the chunks outside the zone; F is zero there, so these
+//     warps read neither F nor the touched flags;
+//   PART 2 (inner): the chunks of the zone.
+// PART 0 runs every cell. The outer launch of a step depends on the previous
+// step's populations only, so it can run while the previous forcing pass is
+// still in flight.
+template <int PART>
+__device__ __forceinline__ bool part_thread(const StepPart& part, unsigned& t) {
+    t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (PART != 0) {
+        const unsigned w = t >> 5;
+        if (w >= (unsigned)part.count) return false;   // whole warps
+        t = (unsigned)__ldg(part.chunks + w) * kSplitChunk + (threadIdx.x & 31u);
+    }
+    return true;
+}
+
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, int PART = 0>
 __global__ void __launch_bounds__(128, 4) k_step_simple(Planes A, Planes B, float* __restrict__ Nu,
                                                        const float* __restrict__ Fx, const float* __restrict__ Fy,
                                                        const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
-                                                       Dims g, CollideParams p) {
-    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE>(A, B, Nu, Fx, Fy, Fz, mask, g, p, blockIdx.x * blockDim.x + threadIdx.x);
+                                                       Dims g, CollideParams p, StepPart part) {
+    static_assert(PART == 0 || V == 1, "split steps run one cell per thread");
+    unsigned t;
+    if (!part_thread<PART>(part, t)) return;   // whole warps
+    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE, PART != 1>(A, B, Nu, Fx, Fy, Fz, mask, g, p, t);
 }
 
 // Resident 128-thread blocks per SM the Esotwist kernel is built for: the
@@ -469,13 +491,15 @@ __global__ void __launch_bounds__(128, 4) k_step_simple(Planes A, Planes B, floa
 template <int V>
 constexpr int kEsotwistBlocksPerSM = V == 1 ? 8 : (V == 2 ? 6 : 4);
 
-template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN>
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN, int PART = 0>
 __global__ void __launch_bounds__(128, kEsotwistBlocksPerSM<V>) k_step_esotwist(Planes Q, float* __restrict__ Nu,
                                                          const float* __restrict__ Fx, const float* __restrict__ Fy,
                                                          const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
-                                                         Dims g, CollideParams p) {
-    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN>(Q, Nu, Fx, Fy, Fz, mask, g, p,
-                                                           blockIdx.x * blockDim.x + threadIdx.x);
+                                                         Dims g, CollideParams p, StepPart part) {
+    static_assert(PART == 0 || V == 1, "split steps run one cell per thread");
+    unsigned t;
+    if (!part_thread<PART>(part, t)) return;   // whole warps
+    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN, PART != 1>(Q, Nu, Fx, Fy, Fz, mask, g, p, t);
 }
 
 // Moments of the current state at every interior cell (what the reference's

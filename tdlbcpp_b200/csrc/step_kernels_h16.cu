@@ -1,30 +1,59 @@
 // 16-bit deviation storage (FP16 and BF16) instances of the step kernels
 // (step_kernels.cuh). Populations are stored as f - w_d * rho0; collision and
-// LES run in FP32. One and four cells per thread.
+// LES run in FP32. One, two and four cells per thread.
 #include "step_kernels.cuh"
 
 namespace tdlb {
 
 static inline unsigned blocks16(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+static inline unsigned grid16(const StepArgs& a, int V) {
+    if (a.part != 0) return blocks16((long long)a.zone.count * 32, 128);
+    return blocks16(a.g.rows() * (a.g.kp / V), 128);
+}
+
+template <typename S, int V, bool LES, int PART>
+static void simple16_part(const StepArgs& a, cudaStream_t st) {
+    k_step_simple<S, V, LES, false, true, PART><<<grid16(a, V), 128, 0, st>>>(a.A, a.B, a.Nu, a.Fx, a.Fy, a.Fz, a.mask,
+                                                                            a.g, a.p, a.zone);
+}
+
+template <typename S, int V, bool LES>
+static void simple16_les(const StepArgs& a, cudaStream_t st) {
+    if constexpr (V == 1) {
+        if (a.part == 1) return simple16_part<S, 1, LES, 1>(a, st);
+        if (a.part == 2) return simple16_part<S, 1, LES, 2>(a, st);
+    }
+    simple16_part<S, V, LES, 0>(a, st);
+}
+
 template <typename S, int V>
 static cudaError_t simple16(const StepArgs& a, cudaStream_t st) {
-    const dim3 grid(blocks16(a.g.rows() * (a.g.kp / V), 128)), block(128);
-    if (a.les) k_step_simple<S, V, true, false, true><<<grid, block, 0, st>>>(a.A, a.B, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p);
-    else k_step_simple<S, V, false, false, true><<<grid, block, 0, st>>>(a.A, a.B, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p);
+    if (a.les) simple16_les<S, V, true>(a, st);
+    else simple16_les<S, V, false>(a, st);
     return cudaGetLastError();
+}
+
+template <typename S, int V, bool LES, int PART>
+static void eso16_part(const StepArgs& a, cudaStream_t st) {
+    const unsigned grid = grid16(a, V);
+    if (a.even) k_step_esotwist<S, V, LES, false, true, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone);
+    else k_step_esotwist<S, V, LES, false, true, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone);
+}
+
+template <typename S, int V, bool LES>
+static void eso16_les(const StepArgs& a, cudaStream_t st) {
+    if constexpr (V == 1) {
+        if (a.part == 1) return eso16_part<S, 1, LES, 1>(a, st);
+        if (a.part == 2) return eso16_part<S, 1, LES, 2>(a, st);
+    }
+    eso16_part<S, V, LES, 0>(a, st);
 }
 
 template <typename S, int V>
 static cudaError_t eso16(const StepArgs& a, cudaStream_t st) {
-    const dim3 grid(blocks16(a.g.rows() * (a.g.kp / V), 128)), block(128);
-    if (a.les) {
-        if (a.even) k_step_esotwist<S, V, true, false, true, true><<<grid, block, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p);
-        else k_step_esotwist<S, V, true, false, true, false><<<grid, block, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p);
-    } else {
-        if (a.even) k_step_esotwist<S, V, false, false, true, true><<<grid, block, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p);
-        else k_step_esotwist<S, V, false, false, true, false><<<grid, block, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p);
-    }
+    if (a.les) eso16_les<S, V, true>(a, st);
+    else eso16_les<S, V, false>(a, st);
     return cudaGetLastError();
 }
 
@@ -33,7 +62,7 @@ cudaError_t launch_step_simple_h16(const StepArgs& a, cudaStream_t st) {
     return with_storage(a.storage, [&](auto s) {
         using S = decltype(s);
         if constexpr (sizeof(S) == 4) return cudaErrorInvalidValue;
-        else return a.vec == 1 ? simple16<S, 1>(a, st) : simple16<S, 4>(a, st);
+        else return a.vec == 1 ? simple16<S, 1>(a, st) : a.vec == 2 ? simple16<S, 2>(a, st) : simple16<S, 4>(a, st);
     });
 }
 
@@ -42,7 +71,7 @@ cudaError_t launch_step_esotwist_h16(const StepArgs& a, cudaStream_t st) {
     return with_storage(a.storage, [&](auto s) {
         using S = decltype(s);
         if constexpr (sizeof(S) == 4) return cudaErrorInvalidValue;
-        else return a.vec == 1 ? eso16<S, 1>(a, st) : eso16<S, 4>(a, st);
+        else return a.vec == 1 ? eso16<S, 1>(a, st) : a.vec == 2 ? eso16<S, 2>(a, st) : eso16<S, 4>(a, st);
     });
 }
 

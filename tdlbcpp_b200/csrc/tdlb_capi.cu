@@ -67,9 +67,15 @@ void release(tdlb_lattice* h) {
     cudaFree(h->d_mask_static);
     cudaFree(h->d_plane_list);
     cudaFree(h->d_exclude);
+    cudaFree(h->d_zone_list);
+    for (cudaEvent_t e : h->tev) cudaEventDestroy(e);
     if (h->side) cudaStreamDestroy(h->side);
+    if (h->ibm) cudaStreamDestroy(h->ibm);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->ev_outer) cudaEventDestroy(h->ev_outer);
+    if (h->ev_inner) cudaEventDestroy(h->ev_inner);
+    if (h->ev_sync) cudaEventDestroy(h->ev_sync);
     cudaFree(h->d_red);
     cudaFree(h->d_rot_xz);
     cudaFree(h->d_load);
@@ -110,22 +116,30 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
         h->err.reserve(512);
         TDLB_CK(cudaSetDevice(device));
         TDLB_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-        TDLB_CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        // the forcing pass is the latency-bound critical path of a split
+        // step: its streams get the highest priority, so its blocks are
+        // scheduled ahead of the outer launch's as SMs free up
+        int prio_lo = 0, prio_hi = 0;
+        TDLB_CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+#ifdef TDLB_EXP_PRIO_LO
+        prio_hi = prio_lo;
+#endif
+        TDLB_CK(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, prio_hi));
+        TDLB_CK(cudaStreamCreateWithPriority(&h->ibm, cudaStreamNonBlocking, prio_hi));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+        TDLB_CK(cudaEventCreateWithFlags(&h->ev_outer, cudaEventDisableTiming));
+        TDLB_CK(cudaEventCreateWithFlags(&h->ev_inner, cudaEventDisableTiming));
+        TDLB_CK(cudaEventCreateWithFlags(&h->ev_sync, cudaEventDisableTiming));
         Dims& g = h->g;
-        g.nx = (int)c.x; g.ny = (int)c.y; g.nz = (int)c.z;
-        g.kp = (int)round_up(c.z, 16);
-        g.kw = (g.kp + 31) / 32;
-        g.plane = round_up((long long)g.nx * g.ny * g.kp, 64);
+        g = tdlb::make_dims((int)c.x, (int)c.y, (int)c.z);
         h->mask_words = round_up((long long)g.nx * g.ny * g.kw, 64);
         if ((long long)g.nx * g.ny * g.kp >= (1LL << 31) - 64)
             throw Fail{TDLB_EINVAL, "lattice too large: one population plane must stay below 2^31 elements"};
         if (tdlb::ibm_smem_bytes(g, 0) > 200 * 1024)
             throw Fail{TDLB_EINVAL, "x * ceil(z/32) too large for the per-plane IBM flag tile"};
         h->cp = tdlb::make_collide_params(c.nu, c.cs0, c.g3);
-        h->cp.wface = (float)(c.initialRho / 12.0);
-        h->cp.wedge = (float)(c.initialRho / 24.0);
+        tdlb::set_rest(h->cp, c.initialRho);
 
         const size_t pop_bytes = (size_t)tdlb::NQ * g.plane * h->esz();
         size_t free_b = 0, total_b = 0;
@@ -197,11 +211,15 @@ tdlb_config config_from_json(const char* text) {
     return c;
 }
 
-template <typename F>
+// Entry points run `fn` after joining the split-step stream (JOIN), so they
+// see every queued step and forcing pass; the step loop's own calls
+// (collision, forcing_resident, rotate_impeller, step) do not join.
+template <bool JOIN = true, typename F>
 int guarded(tdlb_lattice* h, F&& fn) {
     if (!h) return TDLB_EINVAL;
     try {
         cudaSetDevice(h->device);
+        if (JOIN) TDLB_CK(tdlb_rt::join_side(h));
         fn();
         return TDLB_OK;
     } catch (const Fail& f) {
@@ -240,15 +258,205 @@ tdlb::StepArgs step_args(tdlb_lattice* h, bool collide) {
     return a;
 }
 
+// ---------------------------------------------------------------------------
+// Split steps.
+//
+// The forcing pass reads and writes only cells inside the stencils of the
+// markers, and the step reads F only there. The "zone" is a set of 32-element
+// chunks of the flat row*kp + k index that holds every stencil cell of the
+// resident markers at any impeller angle (and, for Esotwist, their 26
+// neighbours: an Esotwist location of a stencil cell is also a location of
+// its neighbours in the other parity). A step then runs as
+//   stream: wait(inner of step s-1), outer chunks of step s
+//   ibm:    forcing pass s-1 ... wait(outer of step s), inner chunks of step s,
+//           forcing pass s
+// so forcing pass s-1 runs concurrently with the outer chunks of step s:
+// those cells neither read F nor share a population location with a stencil
+// cell, and every cell computes exactly what the unsplit step computes.
+// ---------------------------------------------------------------------------
+
+// The split-step stream, ordered after everything queued on `stream` so far.
+cudaStream_t loop_stream(tdlb_lattice* h) {
+    if (!h->pending) {
+        TDLB_CK(cudaEventRecord(h->ev_sync, h->stream));
+        TDLB_CK(cudaStreamWaitEvent(h->ibm, h->ev_sync, 0));
+        h->pending = true;
+    }
+    return h->ibm;
+}
+
+inline void mark_bit(std::vector<uint64_t>& b, long long e) { b[(size_t)(e >> 6)] |= 1ull << (e & 63); }
+inline bool test_bit(const std::vector<uint64_t>& b, long long e) { return (b[(size_t)(e >> 6)] >> (e & 63)) & 1ull; }
+
+// Every stencil cell of markers [b, e) lies in `core`.
+bool stencils_inside(const tdlb_lattice* h, const tdlb_marker* m, size_t n, const std::vector<uint64_t>& core) {
+    const Dims& g = h->g;
+    for (size_t q = 0; q < n; q++) {
+        int st[9];
+        tdlb::MarkerSchedule::stencil(reinterpret_cast<const tdlb::Marker*>(m)[q], g.nx, g.nz, st);
+        for (int c = 0; c < 9; c++) {
+            const long long i = st[c] / g.nz, k = st[c] % g.nz;
+            if (!test_bit(core, (i * g.ny + m[q].j) * g.kp + k)) return false;
+        }
+    }
+    return true;
+}
+
+void build_zone(tdlb_lattice* h) {
+    TDLB_CK(tdlb_rt::join_side(h));
+    TDLB_CK(cudaStreamSynchronize(h->stream));   // no launch still reads the old zone
+    const Dims& g = h->g;
+    const long long nel = g.rows() * g.kp;
+    std::vector<uint64_t> core((size_t)((nel + 63) / 64), 0ull);
+    for (int e : h->cells.cell_e) mark_bit(core, e);   // first segment: its stencil cells, exactly
+    const int n1 = h->n_markers - h->n0;
+    const tdlb_marker* rot = h->h_markers.data() + h->n0;
+    if (n1 > 0 && h->impeller_begin >= 0 && h->h_rot_xz.size() == 2 * (size_t)n1) {
+        // Blades turn about (ci, ck). A blade marker at radius r rounds to the
+        // nearest cell, and its stencil cells lie within 1.5 cells of that
+        // position per axis, so within r +- 2.13 of the axis: mark, plane by
+        // plane, the annulus between the smallest and the largest blade radius
+        // widened by 3 cells.
+        std::vector<double> rlo((size_t)g.ny, 1e300), rhi((size_t)g.ny, -1.0);
+        for (int q = 0; q < n1; q++) {
+            const double r = std::sqrt(h->h_rot_xz[2 * q] * h->h_rot_xz[2 * q] + h->h_rot_xz[2 * q + 1] * h->h_rot_xz[2 * q + 1]);
+            const int j = (int)rot[q].j;
+            rlo[(size_t)j] = std::min(rlo[(size_t)j], r);
+            rhi[(size_t)j] = std::max(rhi[(size_t)j], r);
+        }
+        for (int j = 0; j < g.ny; j++) {
+            if (rhi[(size_t)j] < 0) continue;
+            const double lo = rlo[(size_t)j] - 3.0, hi = rhi[(size_t)j] + 3.0;
+            const int i0 = std::max(0, (int)std::floor(h->rot_ci - hi)), i1 = std::min(g.nx - 1, (int)std::ceil(h->rot_ci + hi));
+            const int k0 = std::max(0, (int)std::floor(h->rot_ck - hi)), k1 = std::min(g.nz - 1, (int)std::ceil(h->rot_ck + hi));
+            for (int i = i0; i <= i1; i++)
+                for (int k = k0; k <= k1; k++) {
+                    const double d = std::sqrt((i - h->rot_ci) * (i - h->rot_ci) + (k - h->rot_ck) * (k - h->rot_ck));
+                    if (d >= lo && d <= hi) mark_bit(core, ((long long)i * g.ny + j) * g.kp + k);
+                }
+        }
+    } else {
+        // blades set by the host without an attached impeller: their current cells
+        for (int q = 0; q < n1; q++) {
+            int st[9];
+            tdlb::MarkerSchedule::stencil(reinterpret_cast<const tdlb::Marker*>(rot)[q], g.nx, g.nz, st);
+            for (int c = 0; c < 9; c++) mark_bit(core, ((long long)(st[c] / g.nz) * g.ny + rot[q].j) * g.kp + st[c] % g.nz);
+        }
+    }
+    std::vector<uint64_t> zone;
+    if (h->cfg.streaming == TDLB_STREAMING_ESOTWIST) {
+        zone.assign(core.size(), 0ull);
+        for (size_t w = 0; w < core.size(); w++)
+            for (uint64_t b = core[w]; b; b &= b - 1) {
+                const long long e = (long long)w * 64 + __builtin_ctzll(b);
+                const long long row = e / g.kp;
+                const int k = (int)(e - row * g.kp), i = (int)(row / g.ny), j = (int)(row % g.ny);
+                for (int di = -1; di <= 1; di++)
+                    for (int dj = -1; dj <= 1; dj++)
+                        for (int dk = -1; dk <= 1; dk++) {
+                            const int a = (i + di + g.nx) % g.nx, b2 = (j + dj + g.ny) % g.ny, c = (k + dk + g.nz) % g.nz;
+                            mark_bit(zone, ((long long)a * g.ny + b2) * g.kp + c);
+                        }
+            }
+    } else {
+        zone = core;
+    }
+    // 32-element chunks (half a word of `zone`): the inner ones (any element
+    // in the zone), then the outer ones
+    static_assert(tdlb::kSplitChunk == 32, "chunk = half a word of the zone bitset");
+    const long long nchunks = (nel + 31) / 32;
+    std::vector<uint32_t> bits((size_t)((nchunks + 31) / 32), 0u);
+    std::vector<int> list, outer;
+    long long inner_cells = 0;   // interior cells of the inner chunks
+    for (long long c = 0; c < nchunks; c++) {
+        const uint32_t half = (uint32_t)(zone[(size_t)(c >> 1)] >> ((c & 1) * 32));
+        if (half) {
+            bits[(size_t)(c >> 5)] |= 1u << (c & 31);
+            list.push_back((int)c);
+            for (long long e = c * 32; e < std::min(c * 32 + 32, nel); e++) inner_cells += (e % g.kp) < g.nz;
+        } else {
+            outer.push_back((int)c);
+        }
+    }
+    const long long n_in = (long long)list.size();
+    list.insert(list.end(), outer.begin(), outer.end());
+    if ((long long)list.size() > h->zone_list_cap || !h->d_zone_list) {
+        cudaFree(h->d_zone_list);
+        h->d_zone_list = nullptr;
+        TDLB_CK(cudaMalloc(&h->d_zone_list, list.size() * sizeof(int)));
+        h->zone_list_cap = (long long)list.size();
+    }
+    TDLB_CK(cudaMemcpyAsync(h->d_zone_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    TDLB_CK(cudaStreamSynchronize(h->stream));
+    h->n_zone = (int)n_in;
+    h->n_outer = (int)(nchunks - n_in);
+    h->zone_small = (double)inner_cells <= 0.6 * (double)g.rows() * (double)g.nz;
+    h->h_zone_bits = std::move(bits);
+    h->zone_ok = stencils_inside(h, rot, (size_t)std::max(n1, 0), core);
+    h->h_zone_core = std::move(core);
+    h->zone_gen = h->marker_gen;
+}
+
+// Forcing passes may go to the split-step stream (the next step can split).
+bool split_capable(tdlb_lattice* h) {
+    if (!h->overlap || h->own_stream || h->vec != 1 || !h->markers_set || !h->resident) return false;
+    if (h->zone_gen != h->marker_gen) build_zone(h);
+    // a zone covering most of the lattice leaves little to overlap with
+    return h->zone_ok && (h->zone_small || h->overlap == 2);
+}
+
+bool can_split(tdlb_lattice* h) { return !h->holds_moments && split_capable(h); }
+
+// Queue one step-kernel launch, bracketed by timing events when enabled.
+template <typename L>
+void timed_launch(tdlb_lattice* h, cudaStream_t st, L&& launch) {
+    h->launches++;
+    if (!h->timing) {
+        TDLB_CK(launch());
+        return;
+    }
+    cudaEvent_t a = nullptr, b = nullptr;
+    TDLB_CK(cudaEventCreate(&a));
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        throw Fail{TDLB_ECUDA, "cudaEventCreate failed"};
+    }
+    h->tev.push_back(a);
+    h->tev.push_back(b);
+    TDLB_CK(cudaEventRecord(a, st));
+    TDLB_CK(launch());
+    TDLB_CK(cudaEventRecord(b, st));
+}
+
 void run_step(tdlb_lattice* h, bool collide) {
     tdlb::StepArgs a = step_args(h, collide);
-    if (h->cfg.streaming == TDLB_STREAMING_SIMPLE) {
-        TDLB_CK(tdlb::launch_step_simple(a, h->stream));
-        h->cur ^= 1;
+    const bool simple = h->cfg.streaming == TDLB_STREAMING_SIMPLE;
+    auto launch = [&](const tdlb::StepArgs& x, cudaStream_t st) {
+        return simple ? tdlb::launch_step_simple(x, st) : tdlb::launch_step_esotwist(x, st);
+    };
+    if (collide && can_split(h)) {
+        cudaStream_t side = loop_stream(h);
+        if (h->inner_queued) TDLB_CK(cudaStreamWaitEvent(h->stream, h->ev_inner, 0));
+        if (h->n_outer > 0) {
+            a.part = 1;
+            a.zone = tdlb::StepPart{h->d_zone_list + h->n_zone, h->n_outer};
+            timed_launch(h, h->stream, [&] { return launch(a, h->stream); });
+        }
+        TDLB_CK(cudaEventRecord(h->ev_outer, h->stream));
+        TDLB_CK(cudaStreamWaitEvent(side, h->ev_outer, 0));
+        if (h->n_zone > 0) {
+            a.part = 2;
+            a.zone = tdlb::StepPart{h->d_zone_list, h->n_zone};
+            timed_launch(h, side, [&] { return launch(a, side); });
+        }
+        TDLB_CK(cudaEventRecord(h->ev_inner, side));
+        h->inner_queued = true;
     } else {
-        TDLB_CK(tdlb::launch_step_esotwist(a, h->stream));
-        h->even = !h->even;   // StreamingEsoteric.hpp:15-18
+        TDLB_CK(tdlb_rt::join_side(h));
+        timed_launch(h, h->stream, [&] { return launch(a, h->stream); });
     }
+    if (simple) h->cur ^= 1;
+    else h->even = !h->even;   // StreamingEsoteric.hpp:15-18
     h->holds_moments = false;
 }
 
@@ -446,9 +654,19 @@ tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     return a;
 }
 
+// Stream of a forcing pass or blade rotation: the split-step stream when the
+// next step can split, else the handle's stream.
+cudaStream_t ibm_stream(tdlb_lattice* h) {
+    if (split_capable(h)) return loop_stream(h);
+    TDLB_CK(tdlb_rt::join_side(h));
+    return h->stream;
+}
+
 void run_forcing(tdlb_lattice* h, float alpha, float beta) {
     if (!h->markers_set) throw Fail{TDLB_ESTATE, "no markers set (tdlb_set_markers / tdlb_forcing)"};
-    TDLB_CK(tdlb::launch_ibm(ibm_args(h, alpha, beta), h->stream));
+    TDLB_CK(tdlb::launch_ibm(ibm_args(h, alpha, beta), ibm_stream(h)));
+    h->launches += (h->cells.cell_e.empty() ? 0 : 1) + (h->n_markers > h->n0 ? 1 : 0) + (h->n_small > 0 ? 1 : 0) +
+                   (h->n_big > 0 ? 1 : 0);
     h->pass++;
     h->last_beta = beta;
 }
@@ -589,11 +807,14 @@ int tdlb_initialise(tdlb_handle h, float rho) {
 }
 
 int tdlb_set_markers(tdlb_handle h, const tdlb_marker* markers, size_t n) {
-    return guarded(h, [&] { upload_markers(h, markers, n, n, nullptr); });
+    return guarded(h, [&] {
+        upload_markers(h, markers, n, n, nullptr);
+        h->resident = true;
+    });
 }
 
 int tdlb_forcing_resident(tdlb_handle h, float alpha, float beta) {
-    return guarded(h, [&] {
+    return guarded<false>(h, [&] {
         require_init(h);
         run_forcing(h, alpha, beta);
     });
@@ -603,12 +824,13 @@ int tdlb_forcing(tdlb_handle h, const tdlb_marker* markers, size_t n, float alph
     return guarded(h, [&] {
         require_init(h);
         upload_markers(h, markers, n, n, nullptr);
+        h->resident = false;   // a new list every pass: no split-step zone
         run_forcing(h, alpha, beta);
     });
 }
 
 int tdlb_collision(tdlb_handle h) {
-    return guarded(h, [&] {
+    return guarded<false>(h, [&] {
         require_init(h);
         run_step(h, true);
     });
@@ -619,7 +841,7 @@ int tdlb_streaming_push(tdlb_handle h) { return h ? TDLB_OK : TDLB_EINVAL; }
 int tdlb_moments(tdlb_handle h) { return h ? TDLB_OK : TDLB_EINVAL; }
 
 int tdlb_step(tdlb_handle h, float alpha, float beta) {
-    return guarded(h, [&] {
+    return guarded<false>(h, [&] {
         require_init(h);
         run_step(h, true);
         run_forcing(h, alpha, beta);
@@ -726,6 +948,63 @@ int tdlb_set_cells_per_thread(tdlb_handle h, int v) {
     });
 }
 
+int tdlb_set_overlap(tdlb_handle h, int mode) {
+    return guarded(h, [&] {
+        if (mode < 0 || mode > 2) throw Fail{TDLB_EINVAL, "overlap mode must be 0, 1 or 2"};
+        h->overlap = mode;
+    });
+}
+
+int tdlb_join(tdlb_handle h) {
+    return guarded(h, [&] {});
+}
+
+int tdlb_read_zone(tdlb_handle h, uint8_t* flags) {
+    return guarded(h, [&] {
+        if (!flags) throw Fail{TDLB_EINVAL, "out is NULL"};
+        if (!split_capable(h))
+            throw Fail{TDLB_ESTATE, "no split step (needs resident markers, one cell per thread, overlap on and, in "
+                                    "mode 1, inner chunks holding at most 60 % of the lattice)"};
+        const Dims& g = h->g;
+        const std::vector<uint32_t>& bits = h->h_zone_bits;
+        size_t c = 0;
+        for (long long i = 0; i < g.nx; i++)
+            for (long long j = 0; j < g.ny; j++)
+                for (long long k = 0; k < g.nz; k++, c++) {
+                    const long long chunk = ((i * g.ny + j) * g.kp + k) / tdlb::kSplitChunk;
+                    flags[c] = (uint8_t)((bits[(size_t)(chunk >> 5)] >> (chunk & 31)) & 1u);
+                }
+    });
+}
+
+int tdlb_kernel_launches(tdlb_handle h, int64_t* n) {
+    return guarded(h, [&] {
+        if (!n) throw Fail{TDLB_EINVAL, "out is NULL"};
+        *n = (int64_t)h->launches;
+    });
+}
+
+int tdlb_set_kernel_timing(tdlb_handle h, int on) {
+    return guarded(h, [&] { h->timing = on != 0; });
+}
+
+int tdlb_kernel_time(tdlb_handle h, double* total_ms, int64_t* launches) {
+    return guarded(h, [&] {
+        TDLB_CK(cudaStreamSynchronize(h->stream));
+        double ms = 0.0;
+        for (size_t q = 0; q + 1 < h->tev.size(); q += 2) {
+            float t = 0.f;
+            TDLB_CK(cudaEventElapsedTime(&t, h->tev[q], h->tev[q + 1]));
+            ms += t;
+        }
+        const int64_t n = (int64_t)(h->tev.size() / 2);
+        for (cudaEvent_t e : h->tev) cudaEventDestroy(e);
+        h->tev.clear();
+        if (total_ms) *total_ms = ms;
+        if (launches) *launches = n;
+    });
+}
+
 int tdlb_reduce_fp64(tdlb_handle h, double* out4) {
     return guarded(h, [&] {
         require_init(h);
@@ -775,6 +1054,8 @@ int tdlb_attach_rushton(tdlb_handle h, const tdlb_rushton* spec, double nonupdat
         if (G.ci - rmax < 2.0 || G.ci + rmax > h->g.nx - 3.0 || G.ck - rmax < 2.0 || G.ck + rmax > h->g.nz - 3.0)
             throw Fail{TDLB_EINVAL, "impeller does not stay 2 cells inside the lattice"};
         upload_markers(h, all.data(), all.size(), n0, xz.data());
+        h->resident = true;
+        h->h_rot_xz = xz;
         cudaFree(h->d_rot_xz);
         h->d_rot_xz = nullptr;
         if (!xz.empty()) {
@@ -792,11 +1073,13 @@ int tdlb_attach_rushton(tdlb_handle h, const tdlb_rushton* spec, double nonupdat
 }
 
 int tdlb_rotate_impeller(tdlb_handle h, double angle, double delta_angle) {
-    return guarded(h, [&] {
+    return guarded<false>(h, [&] {
         if (!h->rot_device) throw Fail{TDLB_ESTATE, "no impeller attached (tdlb_attach_rushton)"};
+        // after the previous forcing pass, which reads the blades
         TDLB_CK(tdlb::launch_rotate_markers(h->d_rot_xz, h->d_markers + h->n0, h->n_markers - h->n0, std::cos(angle),
                                             std::sin(angle), delta_angle, h->rot_ci, h->rot_ck, h->g.nx, h->g.nz,
-                                            h->stream));
+                                            ibm_stream(h)));
+        h->launches++;
         h->angle = angle;
     });
 }
@@ -822,6 +1105,9 @@ int tdlb_set_rotating_markers(tdlb_handle h, const tdlb_marker* markers, size_t 
                                        cudaMemcpyHostToDevice, h->stream));
         upload_seg1(h);
         h->rot_device = false;   // the blades now follow the host's list
+        // a split step needs every blade stencil cell inside the zone
+        if (h->zone_gen == h->marker_gen)
+            h->zone_ok = stencils_inside(h, h->h_markers.data() + h->n0, n, h->h_zone_core);
     });
 }
 
@@ -904,7 +1190,18 @@ namespace tdlb_rt {
 tdlb::StepArgs step_args(tdlb_lattice* h, bool collide) { return ::step_args(h, collide); }
 tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) { return ::ibm_args(h, alpha, beta); }
 void borrow_stream(tdlb_lattice* h, cudaStream_t s) {
+    if (join_side(h) == cudaSuccess) cudaStreamSynchronize(h->stream);
     if (!h->own_stream) h->own_stream = h->stream;
     h->stream = s;
+}
+
+cudaError_t join_side(tdlb_lattice* h) {
+    if (!h->pending) return cudaSuccess;
+    cudaError_t e = cudaEventRecord(h->ev_sync, h->ibm);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->stream, h->ev_sync, 0);
+    if (e != cudaSuccess) return e;
+    h->pending = false;
+    h->inner_queued = false;
+    return cudaSuccess;
 }
 }  // namespace tdlb_rt

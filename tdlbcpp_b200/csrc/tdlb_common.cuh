@@ -37,13 +37,46 @@ __host__ __device__ constexpr int cz_of(int d) {
          : d == 14 ? -1 : d == 15 ? 1 : d == 16 ? -1 : d == 17 ? 1 : 0;
 }
 
+// Division of n < 2^31 by a fixed divisor d >= 1 as one multiply-high, an
+// add and a shift (Granlund and Montgomery, "Division by invariant integers
+// using multiplication", PLDI 1994, the round-up method with l = ceil(log2 d)
+// and m = floor(2^32 (2^l - d) / d) + 1): q = (mulhi(n, m) + n) >> l.
+struct DivU31 {
+    unsigned mul, shift;
+    __device__ __forceinline__ unsigned div(unsigned n) const { return (__umulhi(n, mul) + n) >> shift; }
+};
+__host__ inline DivU31 make_div_u31(unsigned d) {
+    unsigned l = 0;
+    while ((1ull << l) < d) l++;
+    DivU31 r;
+    r.mul = (unsigned)((((1ull << l) - d) << 32) / d + 1);
+    r.shift = l;
+    return r;
+}
+
 struct Dims {
     int nx, ny, nz;     // interior extent
     int kp;             // row pitch in elements (multiple of 16)
     int kw;             // bitmask words per row
     long long plane;    // elements per population plane (multiple of 64)
+    DivU31 by_ny;       // n / ny
+    DivU31 by_kp16;     // n / (kp / 16)
     __host__ __device__ long long rows() const { return (long long)nx * ny; }
 };
+
+// Extent, row pitch, plane size and divisors of an nx x ny x nz lattice.
+__host__ inline Dims make_dims(int nx, int ny, int nz) {
+    Dims g{};
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.kp = (nz + 15) / 16 * 16;
+    g.kw = (g.kp + 31) / 32;
+    g.plane = ((long long)nx * ny * g.kp + 63) / 64 * 64;
+    g.by_ny = make_div_u31((unsigned)ny);
+    g.by_kp16 = make_div_u31((unsigned)(g.kp / 16));
+    return g;
+}
 
 // 18 plane base pointers of one population buffer. With 16-bit storage the
 // pointers address __half / __nv_bfloat16 elements (kernels cast them).
@@ -100,7 +133,15 @@ struct CollideParams {
     float g3;       // third-order relaxation
     float wface;    // rest populations rho0/12 and rho0/24 (16-bit storage offsets)
     float wedge;
+    float rho0;     // 6 wface + 12 wedge: the density of the rest populations
 };
+
+// Rest populations of the deviation storage for initial density rho0.
+__host__ inline void set_rest(CollideParams& p, double rho0) {
+    p.wface = (float)(rho0 / 12.0);
+    p.wedge = (float)(rho0 / 24.0);
+    p.rho0 = (float)(6.0 * (double)p.wface + 12.0 * (double)p.wedge);
+}
 
 __host__ inline CollideParams make_collide_params(double nu, double cs0, double g3) {
     CollideParams p;
@@ -109,8 +150,7 @@ __host__ inline CollideParams make_collide_params(double nu, double cs0, double 
     p.c0 = (float)(1.0 - 6.0 * (double)(float)nu);
     p.cs0sq = (float)cs0 * (float)cs0;
     p.g3 = (float)g3;
-    p.wface = 1.f / 12.f;
-    p.wedge = 1.f / 24.f;
+    set_rest(p, 1.0);
     return p;
 }
 
@@ -180,11 +220,17 @@ __device__ __forceinline__ void moments4_of(const float* q, float* m) {
 // The inverse filter (:137-171) is applied through the even/odd structure of
 // each group of opposite directions. alpha[M17] = alpha[M18] = 0, so the
 // fourth-order columns drop out.
+//
+// DEV (16-bit deviation storage): the populations in and out are deviations
+// f - w rho0. The moments of the rest populations are (rho0, 0, ..., 0) and
+// the inverse filter maps alpha0 = rho0 / 24 back to them, so m[0] holds
+// rho - rho0 and alpha0 is taken as (rho - rho0) / 24: every output is then
+// the deviation itself, without adding and removing the rest weights.
 // ---------------------------------------------------------------------------
-template <bool LES>
+template <bool LES, bool DEV = false>
 __device__ __forceinline__ void collide(const float* m, float fx, float fy, float fz, float& nu,
                                         const CollideParams& p, float* out) {
-    const float rho = m[0];
+    const float rho = DEV ? m[0] + p.rho0 : m[0];
     const float inv_rho = __frcp_rn(rho);
     const float jx = fmaf(0.5f, fx, m[1]);
     const float jy = fmaf(0.5f, fy, m[2]);
@@ -212,7 +258,7 @@ __device__ __forceinline__ void collide(const float* m, float fx, float fy, floa
     }
 
     constexpr float r24 = 1.f / 24.f;
-    const float a0 = rho * r24;
+    const float a0 = m[0] * r24;
     const float a1 = (m[1] + fx) * r24;
     const float a2 = (m[2] + fy) * r24;
     const float a3 = (m[3] + fz) * r24;

@@ -82,6 +82,28 @@ struct tdlb_lattice {
     double* d_load = nullptr;     // kLoadBlocks*5 partials + 5 results
     tdlb_marker* h_stage = nullptr;   // pinned staging of the blade upload
     size_t stage_cap = 0;
+    std::vector<double> h_rot_xz; // host copy of d_rot_xz
+
+    // Split steps: the outer chunks of a step run on `stream` while the
+    // previous forcing pass and the inner chunks run on `ibm`.
+    cudaStream_t ibm = nullptr;
+    cudaEvent_t ev_outer = nullptr, ev_inner = nullptr, ev_sync = nullptr;
+    int overlap = 0;              // split steps: 0 off, 1 when the zone is small, 2 always (tdlb_set_overlap)
+    bool zone_small = false;      // inner chunks hold at most 60 % of the elements
+    bool pending = false;         // `ibm` holds work that `stream` has not waited for
+    bool inner_queued = false;    // ev_inner marks the inner launch of the last step
+    bool resident = false;        // markers kept for many passes (set/attach), so a zone pays
+    unsigned zone_gen = ~0u;      // marker_gen the zone was built for
+    bool zone_ok = false;         // every stencil cell of the current markers lies in the zone
+    std::vector<uint64_t> h_zone_core;   // 1 bit per element: the stencil cells the zone covers
+    std::vector<uint32_t> h_zone_bits;   // 1 bit per 32-element chunk, set for the inner chunks
+    int* d_zone_list = nullptr;          // the inner chunks, then the outer chunks, each ascending
+    int n_zone = 0, n_outer = 0;
+    long long zone_list_cap = 0;
+    // step-kernel timing (tdlb_set_kernel_timing): start/stop event pairs
+    bool timing = false;
+    std::vector<cudaEvent_t> tev;
+    long long launches = 0;       // kernels queued by the step loop (tdlb_kernel_launches)
 
     std::string err = "no error";
 
@@ -115,4 +137,7 @@ tdlb::StepArgs step_args(tdlb_lattice* h, bool collide);
 tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta);
 // Queue h's work on `s` instead of its own stream (batches share one).
 void borrow_stream(tdlb_lattice* h, cudaStream_t s);
+// Make `stream` wait for the forcing pass and inner launches queued on the
+// split-step stream (every entry point other than the step loop calls it).
+cudaError_t join_side(tdlb_lattice* h);
 }  // namespace tdlb_rt

@@ -4,6 +4,14 @@
 
 namespace tdlb {
 
+// Chunks of a split step (32 consecutive elements of the flat row*kp + k
+// index, one warp each): the launch takes chunks[0, count).
+struct StepPart {
+    const int* chunks;
+    int count;
+};
+constexpr int kSplitChunk = 32;
+
 // Arguments of one fused step launch.
 struct StepArgs {
     Planes A;               // Simple: source buffer; Esotwist: the single buffer
@@ -21,6 +29,8 @@ struct StepArgs {
     int even;               // Esotwist parity (evenStep)
     int vec;                // cells per thread: 1, 2 or 4 (float, float2, float4 traffic)
     int storage;            // StorageKind of the population planes
+    int part;               // 0: every cell; 1: outer chunks; 2: inner chunks (vec == 1, populations)
+    StepPart zone;          // the chunks of part 1 or 2
 };
 
 cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st);
