@@ -370,7 +370,10 @@ int tdlb_schedule_levels(const tdlb_marker* markers, size_t n, int64_t x, int64_
  * handle (tdlb_batch_tank) for initialise, attach_rushton, set_markers and
  * the read functions, and all tanks share the batch's stream. All tanks of a
  * batch use one streaming scheme and one storage precision; sizes, nu, LES
- * and markers differ freely. */
+ * and markers differ freely. A run splits the tanks into two groups of about
+ * equal cell count on two streams whose fused steps take turns, so one
+ * group's forcing pass overlaps the other group's fused step; the batch's
+ * stream waits for both before tdlb_batch_run returns. */
 typedef struct tdlb_batch_s* tdlb_batch;
 
 int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* out);
@@ -386,8 +389,10 @@ int tdlb_batch_add(tdlb_batch b, const tdlb_config* cfg, int* index);
 int tdlb_batch_remove(tdlb_batch b, int index);
 int tdlb_batch_tank(tdlb_batch b, int t, tdlb_handle* out);
 /* Shape of the fused batched launch: cells per thread (1, 2, 4; 16-bit
- * storage 1 or 4), threads per block (128 or 256), resident blocks per SM
- * (1..16; the grid is min(work items, SMs x blocks_per_sm)). */
+ * storage 1 or 4) and threads per block (128 or 256). The launch runs one
+ * block per work item (threads x cells per thread cells of one tank), so
+ * the block scheduler balances it against the other group's forcing pass;
+ * blocks_per_sm (1..16) is kept for callers and no longer shapes the grid. */
 int tdlb_batch_set_shape(tdlb_batch b, int cells_per_thread, int threads, int blocks_per_sm);
 int tdlb_batch_get_shape(tdlb_batch b, int* cells_per_thread, int* threads, int* blocks_per_sm);
 /* Times every shape on the initialised batch and keeps the fastest

@@ -146,6 +146,24 @@ struct WorkList {
 
 }  // namespace
 
+// The tanks of a batch are split into two groups of about equal cell count,
+// each with its own stream. A step runs, per group, the blade rotation, the
+// fused step and the forcing pass; group 1's fused step waits for group 0's
+// and group 0's next fused step for group 1's, so each group's forcing pass
+// (latency-bound) runs while the other group's fused step (bandwidth-bound)
+// has the GPU. Tanks are independent, so every tank computes what it
+// computes alone.
+struct BatchGroup {
+    std::vector<int> tanks;            // indices into tdlb_batch_s::tanks
+    WorkList work;                     // fused-step items (tank, first quad)
+    WorkList rot_work;                 // (tank, first blade)
+    WorkList cells, tails, copies, small, big;   // immersed-boundary items
+    int small_tile = 0, big_tile = 0;
+    cudaStream_t stream = nullptr;     // group 0: the batch's stream
+    cudaStream_t side = nullptr;       // large-plane spreads
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fused = nullptr;
+};
+
 struct tdlb_batch_s {
     int device = 0;
     int storage = TDLB_STORAGE_FP32;   // shared by every tank
@@ -153,22 +171,18 @@ struct tdlb_batch_s {
     std::vector<tdlb_lattice*> tanks;
     int view_cap = 0;                  // tanks the per-tank device arrays hold
     bool members_changed = true;       // work lists and arrays must follow the tank list
-    cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;       // large-plane spreads
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t stream = nullptr;     // the batch's stream (group 0's)
+    cudaEvent_t ev_split = nullptr, ev_merge = nullptr;
     TankStep* d_steps = nullptr;       // [2][n]: views of an even and an odd step of a run
     tdlb::IbmArgs* d_ibm = nullptr;    // [2][n]: forcing passes of the same two steps
-    WorkList work;                     // fused-step items (tank, first quad)
-    int* d_step = nullptr;             // device step counter of a run
+    WorkList work;                     // fused-step items of every tank (autotuner)
+    BatchGroup grp[2];
+    int* d_step = nullptr;             // [2] device step counters of a run (one per group)
     std::vector<double*> d_table;      // per tank: [steps][3] cos, sin, delta
     std::vector<int> table_cap;
     TankRotor* d_rotors = nullptr;     // [n]
-    WorkList rot_work;                 // (tank, first blade)
-    WorkList cells, tails, copies, small, big;   // immersed-boundary items
-    int small_tile = 0, big_tile = 0;
     std::vector<unsigned> ibm_gen;     // marker generation the IBM lists were built for
     int vec = 1, threads = 128, bps = 4;   // fused-launch shape
-    int grid = 0;
     long long launches = 0;            // kernels run by tdlb_batch_run* so far
     std::string err = "no error";
 };
@@ -225,49 +239,76 @@ void drop(WorkList& w) {
     w = WorkList{};
 }
 
-// Fused-step work list for the current shape: (tank, first quad) per item.
-void build_work(tdlb_batch_s* b) {
-    std::vector<int2> w;
-    for (int t = 0; t < (int)b->tanks.size(); t++) {
-        const Dims& g = b->tanks[(size_t)t]->g;
-        const long long nq = g.rows() * (g.kp / b->vec);
-        for (long long q = 0; q < nq; q += b->threads) w.push_back(make_int2(t, (int)q));
+// The two groups: tanks by decreasing cell count, each to the group with
+// fewer cells so far.
+void assign_groups(tdlb_batch_s* b) {
+    std::vector<int> order(b->tanks.size());
+    for (size_t t = 0; t < order.size(); t++) order[t] = (int)t;
+    auto cells = [&](int t) { return b->tanks[(size_t)t]->g.rows() * (long long)b->tanks[(size_t)t]->g.nz; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cells(x) > cells(y); });
+    long long sum[2] = {0, 0};
+    b->grp[0].tanks.clear();
+    b->grp[1].tanks.clear();
+    for (int t : order) {
+        const int k = sum[1] < sum[0] ? 1 : 0;
+        b->grp[k].tanks.push_back(t);
+        sum[k] += cells(t);
     }
-    TDLB_BCK(cudaStreamSynchronize(b->stream));   // queued launches may still read the old list
-    put(b->work, w);
-    int sms = 0;
-    TDLB_BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-    b->grid = std::min(b->work.n, sms * b->bps);
+    for (BatchGroup& G : b->grp) std::sort(G.tanks.begin(), G.tanks.end());
 }
 
-// Immersed-boundary work lists; rebuilt when a tank's markers changed.
+// Fused-step work lists for the current shape: (tank, first quad) per item,
+// for every tank and per group.
+void build_work(tdlb_batch_s* b) {
+    auto items = [&](const std::vector<int>& ts) {
+        std::vector<int2> w;
+        for (int t : ts) {
+            const Dims& g = b->tanks[(size_t)t]->g;
+            const long long nq = g.rows() * (g.kp / b->vec);
+            for (long long q = 0; q < nq; q += b->threads) w.push_back(make_int2(t, (int)q));
+        }
+        return w;
+    };
+    std::vector<int> all(b->tanks.size());
+    for (size_t t = 0; t < all.size(); t++) all[t] = (int)t;
+    TDLB_BCK(cudaDeviceSynchronize());   // queued launches may still read the old lists
+    put(b->work, items(all));
+    for (BatchGroup& G : b->grp) put(G.work, items(G.tanks));
+}
+
+// Immersed-boundary work lists per group; rebuilt when a tank's markers changed.
 void build_ibm_work(tdlb_batch_s* b) {
     bool same = true;
     for (size_t t = 0; t < b->tanks.size(); t++) same = same && b->ibm_gen[t] == b->tanks[t]->marker_gen;
     if (same) return;
-    std::vector<int2> cells, tails, copies, small, big;
-    int small_tile = 0, big_tile = 0;
-    for (int t = 0; t < (int)b->tanks.size(); t++) {
-        const tdlb_lattice* h = b->tanks[(size_t)t];
-        if (!h->markers_set) continue;
-        const int ncell = (int)h->cells.cell_e.size();
-        for (int c = 0; c < ncell; c += 256) cells.push_back(make_int2(t, c));
-        for (int q = 0; q < h->n_markers - h->n0; q += 128) tails.push_back(make_int2(t, q));
-        for (long long wd = 0; wd < h->mask_words; wd += tdlb::kMaskCopyWords) copies.push_back(make_int2(t, (int)wd));
-        for (int s = 0; s < h->n_small; s++) small.push_back(make_int2(t, h->h_plane_list[(size_t)s]));
-        for (int s = 0; s < h->n_big; s++) big.push_back(make_int2(t, h->h_plane_list[(size_t)(h->n_small + s)]));
-        small_tile = std::max(small_tile, h->smem_cells);
-        if (h->n_big) big_tile = std::max(big_tile, h->big_tile_cells);
+    TDLB_BCK(cudaDeviceSynchronize());
+    int small_all = 0, big_all = 0;
+    for (BatchGroup& G : b->grp) {
+        std::vector<int2> cells, tails, copies, small, big;
+        int small_tile = 0, big_tile = 0;
+        for (int t : G.tanks) {
+            const tdlb_lattice* h = b->tanks[(size_t)t];
+            if (!h->markers_set) continue;
+            const int ncell = (int)h->cells.cell_e.size();
+            for (int c = 0; c < ncell; c += 256) cells.push_back(make_int2(t, c));
+            for (int q = 0; q < h->n_markers - h->n0; q += 128) tails.push_back(make_int2(t, q));
+            for (long long wd = 0; wd < h->mask_words; wd += tdlb::kMaskCopyWords) copies.push_back(make_int2(t, (int)wd));
+            for (int s = 0; s < h->n_small; s++) small.push_back(make_int2(t, h->h_plane_list[(size_t)s]));
+            for (int s = 0; s < h->n_big; s++) big.push_back(make_int2(t, h->h_plane_list[(size_t)(h->n_small + s)]));
+            small_tile = std::max(small_tile, h->smem_cells);
+            if (h->n_big) big_tile = std::max(big_tile, h->big_tile_cells);
+        }
+        put(G.cells, cells);
+        put(G.tails, tails);
+        put(G.copies, copies);
+        put(G.small, small);
+        put(G.big, big);
+        G.small_tile = small_tile;
+        G.big_tile = big_tile;
+        small_all = std::max(small_all, small_tile);
+        big_all = std::max(big_all, big_tile);
     }
-    TDLB_BCK(cudaStreamSynchronize(b->stream));
-    put(b->cells, cells);
-    put(b->tails, tails);
-    put(b->copies, copies);
-    put(b->small, small);
-    put(b->big, big);
-    b->small_tile = small_tile;
-    b->big_tile = big_tile;
-    TDLB_BCK(tdlb::ibm_batch_prepare_smem(tdlb::ibm_smem_bytes(Dims{}, small_tile), tdlb::ibm_smem_bytes(Dims{}, big_tile)));
+    TDLB_BCK(tdlb::ibm_batch_prepare_smem(tdlb::ibm_smem_bytes(Dims{}, small_all), tdlb::ibm_smem_bytes(Dims{}, big_all)));
     for (size_t t = 0; t < b->tanks.size(); t++) b->ibm_gen[t] = b->tanks[t]->marker_gen;
 }
 
@@ -296,43 +337,65 @@ void advance_step_state(tdlb_lattice* h) {
     h->holds_moments = false;
 }
 
-void launch_fused(tdlb_batch_s* b, const TankStep* d_views, int* counter, cudaStream_t st) {
+// The fused launch over `work`: one block per item (no persistence), so
+// that the block scheduler fills the SMs the other group's forcing pass
+// leaves free.
+void launch_fused(tdlb_batch_s* b, const TankStep* d_views, const WorkList& work, int* counter, cudaStream_t st) {
+    if (work.n == 0) return;
     const tdlb::BatchFn fn = tdlb::batch_kernel(storage_of(b), eso_of(b), b->vec, b->threads);
-    fn<<<b->grid, b->threads, 0, st>>>(d_views, b->work.d, b->work.n, counter);
+    fn<<<work.n, b->threads, 0, st>>>(d_views, work.d, work.n, counter);
     TDLB_BCK(cudaGetLastError());
 }
 
-// One batched step on b->stream (also used inside capture). `k` selects the
-// uploaded views (0: first step of the pair, 1: second). Returns the number
-// of kernels it queued.
-int queue_step(tdlb_batch_s* b, int k) {
+// One batched step of both groups (also used inside capture). `k` selects
+// the uploaded views (0: first step of the pair, 1: second); `first`: no
+// earlier step of this sequence, so group 0 need not wait for group 1.
+// Returns the number of kernels it queued.
+int queue_step(tdlb_batch_s* b, int k, bool first) {
     const size_t n = b->tanks.size();
     int kernels = 0;
-    if (b->rot_work.n) {
-        tdlb::k_rotate_batch<<<b->rot_work.n, 256, 0, b->stream>>>(b->d_rotors, b->rot_work.d, b->d_step);
-        TDLB_BCK(cudaGetLastError());
+    for (int gi = 0; gi < 2; gi++) {
+        BatchGroup& G = b->grp[gi];
+        BatchGroup& other = b->grp[gi ^ 1];
+        if (G.tanks.empty()) continue;
+        if (G.rot_work.n) {
+            tdlb::k_rotate_batch<<<G.rot_work.n, 256, 0, G.stream>>>(b->d_rotors, G.rot_work.d, b->d_step + gi);
+            TDLB_BCK(cudaGetLastError());
+            kernels++;
+        }
+        // the fused steps of the two groups take turns
+        if (!other.tanks.empty() && (gi == 1 || !first)) TDLB_BCK(cudaStreamWaitEvent(G.stream, other.ev_fused, 0));
+        launch_fused(b, b->d_steps + (size_t)k * n, G.work, b->d_step + gi, G.stream);
+        TDLB_BCK(cudaEventRecord(G.ev_fused, G.stream));
         kernels++;
+        tdlb::IbmBatch ib{};
+        ib.args = b->d_ibm + (size_t)k * n;
+        ib.cells = G.cells.d; ib.n_cells = G.cells.n;
+        ib.tails = G.tails.d; ib.n_tails = G.tails.n;
+        ib.copies = G.copies.d; ib.n_copies = G.copies.n;
+        ib.small = G.small.d; ib.n_small = G.small.n;
+        ib.big = G.big.d; ib.n_big = G.big.n;
+        ib.small_tile = G.small_tile;
+        ib.big_tile = G.big_tile;
+        ib.storage = storage_of(b);
+        TDLB_BCK(tdlb::launch_ibm_batch(ib, G.stream, G.side, G.ev_fork, G.ev_join));
+        kernels += (ib.n_cells > 0) + (ib.n_tails > 0) + (ib.n_copies > 0) + (ib.n_small > 0) + (ib.n_big > 0);
     }
-    launch_fused(b, b->d_steps + (size_t)k * n, b->d_step, b->stream);
-    kernels++;
-    for (tdlb_lattice* h : b->tanks) advance_step_state(h);
-    tdlb::IbmBatch ib{};
-    ib.args = b->d_ibm + (size_t)k * n;
-    ib.cells = b->cells.d; ib.n_cells = b->cells.n;
-    ib.tails = b->tails.d; ib.n_tails = b->tails.n;
-    ib.copies = b->copies.d; ib.n_copies = b->copies.n;
-    ib.small = b->small.d; ib.n_small = b->small.n;
-    ib.big = b->big.d; ib.n_big = b->big.n;
-    ib.small_tile = b->small_tile;
-    ib.big_tile = b->big_tile;
-    ib.storage = storage_of(b);
-    TDLB_BCK(tdlb::launch_ibm_batch(ib, b->stream, b->side, b->ev_fork, b->ev_join));
-    kernels += (ib.n_cells > 0) + (ib.n_tails > 0) + (ib.n_copies > 0) + (ib.n_small > 0) + (ib.n_big > 0);
     for (tdlb_lattice* h : b->tanks) {
-        if (!h->markers_set) continue;
-        h->pass++;
+        advance_step_state(h);
+        if (h->markers_set) h->pass++;
     }
     return kernels;
+}
+
+// Group 1's stream joins the batch's stream (fork) and leaves it (merge).
+void split_streams(tdlb_batch_s* b) {
+    TDLB_BCK(cudaEventRecord(b->ev_split, b->stream));
+    TDLB_BCK(cudaStreamWaitEvent(b->grp[1].stream, b->ev_split, 0));
+}
+void merge_streams(tdlb_batch_s* b) {
+    TDLB_BCK(cudaEventRecord(b->ev_merge, b->grp[1].stream));
+    TDLB_BCK(cudaStreamWaitEvent(b->stream, b->ev_merge, 0));
 }
 
 // Views and forcing arguments of the next two steps, uploaded in stream
@@ -368,7 +431,6 @@ void upload_views(tdlb_batch_s* b, float alpha, float beta) {
 // and the rotation launch's tank table.
 void build_tables(tdlb_batch_s* b, int steps) {
     std::vector<TankRotor> rot(b->tanks.size());
-    std::vector<int2> items;
     for (size_t t = 0; t < b->tanks.size(); t++) {
         tdlb_lattice* h = b->tanks[t];
         rot[t] = TankRotor{};
@@ -395,10 +457,14 @@ void build_tables(tdlb_batch_s* b, int steps) {
         TDLB_BCK(cudaMemcpy(b->d_table[t], tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
         const int nr = h->n_markers - h->n0;
         rot[t] = TankRotor{h->d_rot_xz, h->d_markers + h->n0, b->d_table[t], h->rot_ci, h->rot_ck, nr, h->g.nx, h->g.nz, 0};
-        for (int q = 0; q < nr; q += 256) items.push_back(make_int2((int)t, q));
     }
     TDLB_BCK(cudaMemcpy(b->d_rotors, rot.data(), rot.size() * sizeof(TankRotor), cudaMemcpyHostToDevice));
-    put(b->rot_work, items);
+    for (BatchGroup& G : b->grp) {
+        std::vector<int2> items;
+        for (int t : G.tanks)
+            for (int q = 0; q < rot[(size_t)t].n; q += 256) items.push_back(make_int2(t, q));
+        put(G.rot_work, items);
+    }
 }
 
 void finish_tables(tdlb_batch_s* b, int steps) {
@@ -436,6 +502,7 @@ void ensure_capacity(tdlb_batch_s* b) {
 void sync_members(tdlb_batch_s* b) {
     if (!b->members_changed) return;
     ensure_capacity(b);
+    assign_groups(b);
     build_work(b);
     for (auto& g : b->ibm_gen) g = ~0u;
     b->members_changed = false;
@@ -474,34 +541,52 @@ void check_ready(tdlb_batch_s* b) {
         if (!h->initialised) throw BFail{TDLB_ESTATE, "every tank must be initialised first"};
 }
 
+// Pairs of steps per captured graph: the two groups' pipeline drains at the
+// end of each replay.
+constexpr int kPairsPerGraph = 4;
+
+// One eager step: uploads follow every queued launch of both groups.
+void eager_step(tdlb_batch_s* b, float alpha, float beta) {
+    merge_streams(b);
+    upload_views(b, alpha, beta);
+    split_streams(b);
+    b->launches += queue_step(b, 0, true);
+}
+
 // `steps` steps, eager or graph-replayed. A step whose state still holds
 // moments (right after initialise) runs eagerly: its views differ from the
 // repeating pair's.
 void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
     if (b->tanks.empty()) return;
     check_ready(b);
-    TDLB_BCK(cudaStreamSynchronize(b->stream));   // the previous run may still read the tables and lists
+    TDLB_BCK(cudaDeviceSynchronize());   // the previous run may still read the tables and lists
     sync_members(b);
     build_ibm_work(b);
     build_tables(b, steps);
-    TDLB_BCK(cudaMemsetAsync(b->d_step, 0, sizeof(int), b->stream));
+    TDLB_BCK(cudaMemsetAsync(b->d_step, 0, 2 * sizeof(int), b->stream));
     int done = 0;
     bool any_moments = false;
     for (tdlb_lattice* h : b->tanks) any_moments = any_moments || h->holds_moments;
     while (done < steps && (any_moments || !graph || steps - done < 2)) {
-        upload_views(b, alpha, beta);
-        b->launches += queue_step(b, 0);
+        eager_step(b, alpha, beta);
         done++;
         any_moments = false;
     }
-    if (done < steps) {
+    const int pairs = (steps - done) / 2;
+    if (pairs > 0) {
+        const int P = std::min(pairs, kPairsPerGraph);
+        merge_streams(b);
         upload_views(b, alpha, beta);
         cudaGraph_t g = nullptr;
-        int per_pair = 0;
+        int per_graph = 0;
         TDLB_BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            per_pair += queue_step(b, 0);
-            per_pair += queue_step(b, 1);
+            split_streams(b);
+            for (int p = 0; p < P; p++) {
+                per_graph += queue_step(b, 0, p == 0);
+                per_graph += queue_step(b, 1, false);
+            }
+            merge_streams(b);
         } catch (...) {
             cudaStreamEndCapture(b->stream, &g);
             if (g) cudaGraphDestroy(g);
@@ -512,11 +597,11 @@ void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
         const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
         cudaGraphDestroy(g);
         TDLB_BCK(ie);
-        // the capture advanced the host state by the pair; the replays run it
-        const int pairs = (steps - done) / 2;
+        // the capture advanced the host state by 2P steps; the replays run them
         for (tdlb_lattice* h : b->tanks)
-            if (h->markers_set) h->pass -= 2;
-        for (int r = 0; r < pairs; r++) {
+            if (h->markers_set) h->pass -= 2 * P;
+        const int replays = pairs / P;
+        for (int r = 0; r < replays; r++) {
             const cudaError_t le = cudaGraphLaunch(ge, b->stream);
             if (le != cudaSuccess) {
                 cudaGraphExecDestroy(ge);
@@ -525,15 +610,15 @@ void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
         }
         cudaGraphExecDestroy(ge);
         for (tdlb_lattice* h : b->tanks)
-            if (h->markers_set) h->pass += 2 * pairs;
-        b->launches += (long long)per_pair * pairs;
-        done += 2 * pairs;
-        if (done < steps) {   // an odd step left
-            upload_views(b, alpha, beta);
-            b->launches += queue_step(b, 0);
+            if (h->markers_set) h->pass += 2 * P * replays;
+        b->launches += (long long)per_graph * replays;
+        done += 2 * P * replays;
+        while (done < steps) {   // fewer than 2P steps left
+            eager_step(b, alpha, beta);
             done++;
         }
     }
+    merge_streams(b);
     finish_tables(b, steps);
     for (tdlb_lattice* h : b->tanks)
         if (h->markers_set) h->last_beta = beta;   // for tdlb_impeller_load
@@ -541,18 +626,43 @@ void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
 
 void release(tdlb_batch_s* b) {
     cudaSetDevice(b->device);
-    if (b->stream) cudaStreamSynchronize(b->stream);
+    cudaDeviceSynchronize();
     for (tdlb_lattice* h : b->tanks) tdlb_destroy(h);
     for (double* p : b->d_table) cudaFree(p);
-    for (WorkList* w : {&b->work, &b->rot_work, &b->cells, &b->tails, &b->copies, &b->small, &b->big}) drop(*w);
+    drop(b->work);
+    for (BatchGroup& G : b->grp) {
+        for (WorkList* w : {&G.work, &G.rot_work, &G.cells, &G.tails, &G.copies, &G.small, &G.big}) drop(*w);
+        if (G.ev_fork) cudaEventDestroy(G.ev_fork);
+        if (G.ev_join) cudaEventDestroy(G.ev_join);
+        if (G.ev_fused) cudaEventDestroy(G.ev_fused);
+        if (G.side) cudaStreamDestroy(G.side);
+        if (G.stream && G.stream != b->stream) cudaStreamDestroy(G.stream);
+    }
     cudaFree(b->d_steps);
     cudaFree(b->d_ibm);
     cudaFree(b->d_rotors);
     cudaFree(b->d_step);
-    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
-    if (b->ev_join) cudaEventDestroy(b->ev_join);
-    if (b->side) cudaStreamDestroy(b->side);
+    if (b->ev_split) cudaEventDestroy(b->ev_split);
+    if (b->ev_merge) cudaEventDestroy(b->ev_merge);
     if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+// Streams, events and the step counters of a new batch.
+void init_streams(tdlb_batch_s* b) {
+    TDLB_BCK(cudaSetDevice(b->device));
+    TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    TDLB_BCK(cudaEventCreateWithFlags(&b->ev_split, cudaEventDisableTiming));
+    TDLB_BCK(cudaEventCreateWithFlags(&b->ev_merge, cudaEventDisableTiming));
+    for (int gi = 0; gi < 2; gi++) {
+        BatchGroup& G = b->grp[gi];
+        if (gi == 0) G.stream = b->stream;
+        else TDLB_BCK(cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking));
+        TDLB_BCK(cudaStreamCreateWithFlags(&G.side, cudaStreamNonBlocking));
+        TDLB_BCK(cudaEventCreateWithFlags(&G.ev_fork, cudaEventDisableTiming));
+        TDLB_BCK(cudaEventCreateWithFlags(&G.ev_join, cudaEventDisableTiming));
+        TDLB_BCK(cudaEventCreateWithFlags(&G.ev_fused, cudaEventDisableTiming));
+    }
+    TDLB_BCK(cudaMalloc(&b->d_step, 2 * sizeof(int)));
 }
 
 }  // namespace
@@ -571,12 +681,7 @@ int tdlb_batch_create(const tdlb_config* cfgs, int n, int device, tdlb_batch* ou
     b->streaming = cfgs[0].streaming;
     b->vec = 1;
     try {
-        TDLB_BCK(cudaSetDevice(device));
-        TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-        TDLB_BCK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
-        TDLB_BCK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
-        TDLB_BCK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
-        TDLB_BCK(cudaMalloc(&b->d_step, sizeof(int)));
+        init_streams(b);
         for (int t = 0; t < n; t++) add_tank(b, cfgs[t]);
         sync_members(b);
     } catch (const BFail& f) {
@@ -602,12 +707,7 @@ int tdlb_batch_create_empty(int device, int streaming, int storage, tdlb_batch* 
     b->streaming = streaming;
     b->vec = 1;
     try {
-        TDLB_BCK(cudaSetDevice(device));
-        TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-        TDLB_BCK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
-        TDLB_BCK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
-        TDLB_BCK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
-        TDLB_BCK(cudaMalloc(&b->d_step, sizeof(int)));
+        init_streams(b);
     } catch (const BFail& f) {
         g_batch_create_error = f.msg;
         release(b);
@@ -691,13 +791,9 @@ int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms) {
         const bool h16 = storage_of(b) != TDLB_STORAGE_FP32;
         for (int v : {1, 2, 4}) {
             if (h16 && v == 2) continue;
-            for (int nt : {128, 256})
-                for (int bps : {2, 4, 8}) {
-                    if (nt == 256 && bps == 8) continue;
-                    cands.push_back({v, nt, bps});
-                }
+            for (int nt : {128, 256}) cands.push_back({v, nt, b->bps});
         }
-        TDLB_BCK(cudaStreamSynchronize(b->stream));
+        TDLB_BCK(cudaDeviceSynchronize());
         upload_views(b, 0.f, 0.f);
         cudaEvent_t e0, e1;
         TDLB_BCK(cudaEventCreate(&e0));
@@ -708,9 +804,9 @@ int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms) {
             for (const Cand& c : cands) {
                 b->vec = c.v; b->threads = c.nt; b->bps = c.bps;
                 build_work(b);
-                launch_fused(b, b->d_steps, nullptr, b->stream);   // warm-up
+                launch_fused(b, b->d_steps, b->work, nullptr, b->stream);   // warm-up
                 TDLB_BCK(cudaEventRecord(e0, b->stream));
-                for (int r = 0; r < trials; r++) launch_fused(b, b->d_steps, nullptr, b->stream);
+                for (int r = 0; r < trials; r++) launch_fused(b, b->d_steps, b->work, nullptr, b->stream);
                 TDLB_BCK(cudaEventRecord(e1, b->stream));
                 TDLB_BCK(cudaEventSynchronize(e1));
                 float ms = 0.f;
@@ -754,7 +850,10 @@ int tdlb_batch_kernel_launches(tdlb_batch b, long long* n) {
 }
 
 int tdlb_batch_synchronize(tdlb_batch b) {
-    return bguard(b, [&] { TDLB_BCK(cudaStreamSynchronize(b->stream)); });
+    return bguard(b, [&] {
+        TDLB_BCK(cudaStreamSynchronize(b->stream));
+        TDLB_BCK(cudaStreamSynchronize(b->grp[1].stream));
+    });
 }
 
 int tdlb_batch_get_stream(tdlb_batch b, void** stream) {
