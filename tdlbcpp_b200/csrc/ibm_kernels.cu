@@ -280,6 +280,7 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
     const Dims g = a.g;
     const float* s = a.tail;
     const long long cap = a.tail_cap;
+    const bool distinct = g.nx >= 3 && g.nz >= 3;   // the 9 stencil cells of a marker differ
 
     for (int h = threadIdx.x; h < H; h += THREADS) keys[h] = -1;
     __syncthreads();
@@ -315,14 +316,19 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
             const int t = p - a.n0;
             const int* rf = ref + 9 * (p - q0);
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
+            float w[9], ox[9], oy[9], oz[9];
+            int hh[9];
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                const float w = s[(TF_W + c) * cap + t];
-                const int h = rf[c];
-                rhoSum = fmaf(w, s[(TF_RHO + c) * cap + t], rhoSum);
-                xSum = fmaf(w, fmaf(0.5f, hx[h], s[(TF_MX + c) * cap + t]), xSum);
-                ySum = fmaf(w, fmaf(0.5f, hy[h], s[(TF_MY + c) * cap + t]), ySum);
-                zSum = fmaf(w, fmaf(0.5f, hz[h], s[(TF_MZ + c) * cap + t]), zSum);
+                w[c] = s[(TF_W + c) * cap + t];
+                hh[c] = rf[c];
+                ox[c] = hx[hh[c]];
+                oy[c] = hy[hh[c]];
+                oz[c] = hz[hh[c]];
+                rhoSum = fmaf(w[c], s[(TF_RHO + c) * cap + t], rhoSum);
+                xSum = fmaf(w[c], fmaf(0.5f, ox[c], s[(TF_MX + c) * cap + t]), xSum);
+                ySum = fmaf(w[c], fmaf(0.5f, oy[c], s[(TF_MY + c) * cap + t]), ySum);
+                zSum = fmaf(w[c], fmaf(0.5f, oz[c], s[(TF_MZ + c) * cap + t]), zSum);
             }
             xSum = fmaf(-rhoSum, s[TF_U * cap + t], xSum);
             ySum = fmaf(-rhoSum, s[TF_V * cap + t], ySum);
@@ -330,13 +336,22 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
             a.sums[p] = xSum;
             a.sums[a.n + p] = ySum;
             a.sums[2 * a.n + p] = zSum;
+            if (distinct) {   // 9 different cells: independent updates
 #pragma unroll
-            for (int c = 0; c < 9; c++) {   // sequential: a wrapped stencil sees its own update
-                const int h = rf[c];
-                const float bw = a.beta * s[(TF_W + c) * cap + t];
-                hx[h] = fmaf(a.alpha, hx[h], -bw * xSum);
-                hy[h] = fmaf(a.alpha, hy[h], -bw * ySum);
-                hz[h] = fmaf(a.alpha, hz[h], -bw * zSum);
+                for (int c = 0; c < 9; c++) {
+                    const float bw = a.beta * w[c];
+                    hx[hh[c]] = fmaf(a.alpha, ox[c], -bw * xSum);
+                    hy[hh[c]] = fmaf(a.alpha, oy[c], -bw * ySum);
+                    hz[hh[c]] = fmaf(a.alpha, oz[c], -bw * zSum);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 9; c++) {   // sequential: a wrapped stencil sees its own update
+                    const float bw = a.beta * w[c];
+                    hx[hh[c]] = fmaf(a.alpha, hx[hh[c]], -bw * xSum);
+                    hy[hh[c]] = fmaf(a.alpha, hy[hh[c]], -bw * ySum);
+                    hz[hh[c]] = fmaf(a.alpha, hz[hh[c]], -bw * zSum);
+                }
             }
         }
         __syncthreads();
@@ -380,7 +395,10 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
     __syncthreads();
 
     // ---- first segment: each marker in list order relative to every marker
-    //      it shares a cell with (level walk)
+    //      it shares a cell with (level walk). With x and z at least 3 the 9
+    //      stencil cells of a marker differ (the stencil wraps onto itself
+    //      only on a narrower lattice).
+    const bool distinct = a.g.nx >= 3 && a.g.nz >= 3;
     const long long n0 = a.n0;
     const float* rho = a.cell_m + c0;
     const float* mx = a.cell_m + C + c0;
@@ -390,14 +408,22 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
         for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
+            float w[9], ox[9], oy[9], oz[9];
+            int li[9];
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                const float w = a.prep[(PF_W + c) * n0 + p];
-                const int li = __float_as_int(a.prep[(PF_CELL + c) * n0 + p]);
-                rhoSum = fmaf(w, rho[li], rhoSum);
-                xSum = fmaf(w, fmaf(0.5f, fx[li], mx[li]), xSum);
-                ySum = fmaf(w, fmaf(0.5f, fy[li], my[li]), ySum);
-                zSum = fmaf(w, fmaf(0.5f, fz[li], mz[li]), zSum);
+                w[c] = a.prep[(PF_W + c) * n0 + p];
+                li[c] = __float_as_int(a.prep[(PF_CELL + c) * n0 + p]);
+            }
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                ox[c] = fx[li[c]];
+                oy[c] = fy[li[c]];
+                oz[c] = fz[li[c]];
+                rhoSum = fmaf(w[c], rho[li[c]], rhoSum);
+                xSum = fmaf(w[c], fmaf(0.5f, ox[c], mx[li[c]]), xSum);
+                ySum = fmaf(w[c], fmaf(0.5f, oy[c], my[li[c]]), ySum);
+                zSum = fmaf(w[c], fmaf(0.5f, oz[c], mz[li[c]]), zSum);
             }
             xSum = fmaf(-rhoSum, a.prep[PF_U * n0 + p], xSum);
             ySum = fmaf(-rhoSum, a.prep[PF_V * n0 + p], ySum);
@@ -405,13 +431,24 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
             a.sums[p] = xSum;
             a.sums[a.n + p] = ySum;
             a.sums[2 * a.n + p] = zSum;
+            if (distinct) {
+                // 9 different cells: each update starts from the value read
+                // above, so the 27 stores are independent
 #pragma unroll
-            for (int c = 0; c < 9; c++) {   // sequential: a wrapped stencil sees its own update
-                const float bw = a.beta * a.prep[(PF_W + c) * n0 + p];
-                const int li = __float_as_int(a.prep[(PF_CELL + c) * n0 + p]);
-                fx[li] = fmaf(a.alpha, fx[li], -bw * xSum);
-                fy[li] = fmaf(a.alpha, fy[li], -bw * ySum);
-                fz[li] = fmaf(a.alpha, fz[li], -bw * zSum);
+                for (int c = 0; c < 9; c++) {
+                    const float bw = a.beta * w[c];
+                    fx[li[c]] = fmaf(a.alpha, ox[c], -bw * xSum);
+                    fy[li[c]] = fmaf(a.alpha, oy[c], -bw * ySum);
+                    fz[li[c]] = fmaf(a.alpha, oz[c], -bw * zSum);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 9; c++) {   // sequential: a wrapped stencil sees its own update
+                    const float bw = a.beta * w[c];
+                    fx[li[c]] = fmaf(a.alpha, fx[li[c]], -bw * xSum);
+                    fy[li[c]] = fmaf(a.alpha, fy[li[c]], -bw * ySum);
+                    fz[li[c]] = fmaf(a.alpha, fz[li[c]], -bw * zSum);
+                }
             }
         }
         __syncthreads();
@@ -431,7 +468,7 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
 }
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes,
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes,
                                                                        int tile_cells) {
     extern __shared__ float tile[];                             // [3][tile_cells]
     ibm_spread_plane<THREADS>(a, planes[blockIdx.x], tile_cells, tile);
@@ -601,7 +638,7 @@ cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
 }
 
 cudaError_t ibm_prepare_smem(size_t bytes) {
-    cudaError_t e = raise_smem_limit((const void*)k_ibm_spread<256>, bytes);
+    cudaError_t e = raise_smem_limit((const void*)k_ibm_spread<128>, bytes);
     if (e != cudaSuccess) return e;
     return raise_smem_limit((const void*)k_ibm_spread<512>, bytes);
 }
@@ -644,7 +681,7 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
         if (err != cudaSuccess) return err;
     }
     if (a.n_small > 0)
-        k_ibm_spread<256><<<a.n_small, 256, ibm_smem_bytes(a.g, a.smem_cells), st>>>(a, a.plane_list, a.smem_cells);
+        k_ibm_spread<128><<<a.n_small, 128, ibm_smem_bytes(a.g, a.smem_cells), st>>>(a, a.plane_list, a.smem_cells);
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     if (a.n_big > 0) return cudaStreamWaitEvent(st, a.ev_join, 0);
@@ -699,7 +736,7 @@ __global__ void __launch_bounds__(256) k_mask_copy_batch(const IbmArgs* __restri
 }
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread_batch(const IbmArgs* __restrict__ args,
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1) k_ibm_spread_batch(const IbmArgs* __restrict__ args,
                                                                              const int2* __restrict__ work, int big) {
     extern __shared__ float tile[];
     __shared__ IbmArgs sa;
@@ -710,7 +747,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 256 ? 3 : 1) k_ibm_spread_
 }
 
 cudaError_t ibm_batch_prepare_smem(size_t small_bytes, size_t big_bytes) {
-    cudaError_t e = raise_smem_limit((const void*)k_ibm_spread_batch<256>, small_bytes);
+    cudaError_t e = raise_smem_limit((const void*)k_ibm_spread_batch<128>, small_bytes);
     if (e != cudaSuccess) return e;
     return raise_smem_limit((const void*)k_ibm_spread_batch<512>, big_bytes);
 }
@@ -740,7 +777,7 @@ cudaError_t launch_ibm_batch(const IbmBatch& b, cudaStream_t st, cudaStream_t si
         err = cudaEventRecord(join, side);
         if (err != cudaSuccess) return err;
     }
-    if (b.n_small > 0) k_ibm_spread_batch<256><<<b.n_small, 256, ibm_smem_bytes(Dims{}, b.small_tile), st>>>(b.args, b.small, 0);
+    if (b.n_small > 0) k_ibm_spread_batch<128><<<b.n_small, 128, ibm_smem_bytes(Dims{}, b.small_tile), st>>>(b.args, b.small, 0);
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     if (b.n_big > 0) return cudaStreamWaitEvent(st, join, 0);

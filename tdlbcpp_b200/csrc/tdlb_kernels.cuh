@@ -113,7 +113,7 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st);
 // Immersed-boundary passes of many lattices in one set of launches: device
 // IbmArgs per lattice and work lists of (lattice, first index) items --
 // cells: 256 first-segment cells; tails: 128 blade markers; copies: 1024
-// touched-flag words; small / big: one j-plane (256 / 512 threads).
+// touched-flag words; small / big: one j-plane (128 / 512 threads).
 struct IbmBatch {
     const IbmArgs* args;
     const int2* cells; int n_cells;
