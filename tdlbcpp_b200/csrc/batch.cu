@@ -68,11 +68,16 @@ __device__ __forceinline__ void tank_quad(const TankStep& ts, unsigned t) {
     }
 }
 
-// Persistent batched step: block b takes work items b, b + grid, ...; an
-// item is `NT` consecutive quads of one tank, whose step view is staged in
-// shared memory. 16-bit storage never holds moments, so its from-moments
-// bodies are not built. `counter` (may be NULL) is advanced once: this
-// launch runs after the step's rotation, which reads it.
+// Quads of `NT` threads a work item covers: the tank's view is staged in
+// shared memory once per item.
+constexpr int kBatchChunks = 4;
+
+// Batched step: block b takes work items b, b + grid, ...; an item is
+// kBatchChunks x NT consecutive quads of one tank (fewer at the end of a
+// tank), whose step view is staged in shared memory. 16-bit storage never
+// holds moments, so its from-moments bodies are not built. `counter` (may be
+// NULL) is advanced once: this launch runs after the step's rotation, which
+// reads it.
 template <typename S, int V, int NT, bool ESO>
 __global__ void __launch_bounds__(NT, (ESO ? kEsotwistBlocksPerSM<V> : 4) * 128 / NT) k_batch_step(const TankStep* __restrict__ tanks, const int2* __restrict__ work,
                                                    int nwork, int* counter) {
@@ -84,13 +89,18 @@ __global__ void __launch_bounds__(NT, (ESO ? kEsotwistBlocksPerSM<V> : 4) * 128 
         __syncthreads();
         stage<NT>(ts, tanks + wk.x);
         __syncthreads();
-        const unsigned t = (unsigned)wk.y + threadIdx.x;
-        if (ts.les) {
-            if (kFM && ts.from_moments) tank_quad<S, V, ESO, true, kFM>(ts, t);
-            else tank_quad<S, V, ESO, true, false>(ts, t);
-        } else {
-            if (kFM && ts.from_moments) tank_quad<S, V, ESO, false, kFM>(ts, t);
-            else tank_quad<S, V, ESO, false, false>(ts, t);
+        const unsigned nquads = (unsigned)ts.g.nx * (unsigned)ts.g.ny * (unsigned)(ts.g.kp / V);
+        for (int c = 0; c < kBatchChunks; c++) {
+            const unsigned t0 = (unsigned)wk.y + (unsigned)(c * NT);
+            if (t0 >= nquads) break;   // uniform over the block
+            const unsigned t = t0 + threadIdx.x;
+            if (ts.les) {
+                if (kFM && ts.from_moments) tank_quad<S, V, ESO, true, kFM>(ts, t);
+                else tank_quad<S, V, ESO, true, false>(ts, t);
+            } else {
+                if (kFM && ts.from_moments) tank_quad<S, V, ESO, false, kFM>(ts, t);
+                else tank_quad<S, V, ESO, false, false>(ts, t);
+            }
         }
     }
 }
@@ -265,7 +275,7 @@ void build_work(tdlb_batch_s* b) {
         for (int t : ts) {
             const Dims& g = b->tanks[(size_t)t]->g;
             const long long nq = g.rows() * (g.kp / b->vec);
-            for (long long q = 0; q < nq; q += b->threads) w.push_back(make_int2(t, (int)q));
+            for (long long q = 0; q < nq; q += (long long)b->threads * tdlb::kBatchChunks) w.push_back(make_int2(t, (int)q));
         }
         return w;
     };
