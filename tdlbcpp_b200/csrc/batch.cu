@@ -70,7 +70,7 @@ __device__ __forceinline__ void tank_quad(const TankStep& ts, unsigned t) {
 
 // Quads of `NT` threads a work item covers: the tank's view is staged in
 // shared memory once per item.
-constexpr int kBatchChunks = 4;
+constexpr int kBatchChunks = 8;
 
 // Batched step: block b takes work items b, b + grid, ...; an item is
 // kBatchChunks x NT consecutive quads of one tank (fewer at the end of a
