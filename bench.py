@@ -764,8 +764,14 @@ def host_threads(edge=EDGE, height=16):
 _PG = None
 
 
-def init_dist(args):
-    global _PG
+_DEVICE = "cuda"
+
+
+def init_dist(args, backend=None):
+    """One process per GPU (RANK / LOCAL_RANK / WORLD_SIZE from torchrun):
+    NCCL on GPUs; gloo where no GPU is visible (the CPU tests of the
+    multi-rank helpers)."""
+    global _PG, _DEVICE
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -773,8 +779,12 @@ def init_dist(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        _DEVICE = "cuda" if backend == "nccl" else "cpu"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         _PG = dist
     return rank, world, local
 
@@ -785,9 +795,11 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The slowest rank's time: every multi-GPU number is timed on each
+    device and reduced with MAX."""
     if world > 1 and _PG is not None:
         import torch
-        t = torch.tensor([float(x)], device="cuda")
+        t = torch.tensor([float(x)], device=_DEVICE)
         _PG.all_reduce(t, op=_PG.ReduceOp.MAX)
         return float(t.item())
     return float(x)
