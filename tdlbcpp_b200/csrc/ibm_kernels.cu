@@ -22,12 +22,13 @@
 // only where the bit is set, and the next pass treats F as zero where neither
 // the previous pass (mask_old) nor the current one has touched the cell.
 //
-// Per pass (launch_ibm): k_ibm_cells (moments and starting F of every unique
-// stencil cell of the static markers), k_ibm_gather_tail (weights and
-// stencil moments of every blade marker, which no marker changes), a copy of
-// the static touched flags into mask_new, then k_ibm_spread, one CTA per
-// j-plane: the static markers' levels on an F tile in shared memory, then
-// the blade levels on a shared-memory hash table of the plane's blade cells.
+// Per pass (launch_ibm): a copy of the static touched flags into mask_new,
+// k_ibm_cells (moments and starting F of every unique stencil cell of the
+// static markers; the big planes' cells first), k_ibm_gather_tail (weights
+// and stencil moments of every blade marker, which no marker changes), then
+// k_ibm_spread, one CTA per j-plane: the static markers' levels on an F tile
+// in shared memory, then the blade levels on a shared-memory hash table of
+// the plane's blade cells.
 #include "tdlb_kernels.cuh"
 #include "tdlb_rotate.hpp"
 
@@ -154,10 +155,13 @@ __device__ __forceinline__ void ibm_cell(const IbmArgs& a, int c) {
     a.cell_F[2 * C + c] = live ? a.Fz[e] : 0.f;
 }
 
+// Cells [first, first + count) of a.cell_order (of the cell list itself
+// when there is no order).
 template <typename S>
-__global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < a.ncell) ibm_cell<S>(a, c);
+__global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a, int first, int count) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    ibm_cell<S>(a, a.cell_order ? a.cell_order[first + t] : first + t);
 }
 
 // Second segment (the blades): weights and the moments of the 9 stencil
@@ -651,23 +655,27 @@ cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, 
 }
 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
-    if (a.ncell > 0) {
-        const unsigned b = (a.ncell + 255) / 256;
-        with_storage(a.storage, [&](auto s) { k_ibm_cells<decltype(s)><<<b, 256, 0, st>>>(a); });
-        cudaError_t err = cudaGetLastError();
-        if (err != cudaSuccess) return err;
-    }
-    if (a.n > a.n0) {
-        const unsigned b = (a.n - a.n0 + 127) / 128;
-        with_storage(a.storage, [&](auto s) { k_ibm_gather_tail<decltype(s)><<<b, 128, 0, st>>>(a); });
-        cudaError_t err = cudaGetLastError();
-        if (err != cudaSuccess) return err;
-    }
+    auto cells = [&](int first, int count) {
+        if (count <= 0) return;
+        with_storage(a.storage,
+                     [&](auto s) { k_ibm_cells<decltype(s)><<<(count + 255) / 256, 256, 0, st>>>(a, first, count); });
+    };
     // mask_new starts as the first segment's (static) touched cells
     cudaError_t err = cudaMemcpyAsync(a.mask_new, a.mask_static, a.mask_bytes, cudaMemcpyDeviceToDevice, st);
     if (err != cudaSuccess) return err;
-    // planes with many cells (an impeller disk) run on a side stream with a
-    // full-size tile and 512 threads, concurrently with the other planes
+    const bool split = a.n_big > 0 && a.cell_order;
+    // Planes with many cells (an impeller disk) run on a side stream with a
+    // full-size tile and 512 threads. Their cells are prepared first, so that
+    // their spread starts while the other planes' cells are prepared: a
+    // big-plane block needs a whole SM's shared memory, which it would not
+    // find once the small-plane spread has spread its blocks over the SMs.
+    cells(0, split ? a.ncell_big : a.ncell);
+    if (a.n > a.n0) {
+        const unsigned b = (a.n - a.n0 + 127) / 128;
+        with_storage(a.storage, [&](auto s) { k_ibm_gather_tail<decltype(s)><<<b, 128, 0, st>>>(a); });
+    }
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
     if (a.n_big > 0) {
         err = cudaEventRecord(a.ev_fork, st);
         if (err != cudaSuccess) return err;
@@ -680,6 +688,7 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
         err = cudaEventRecord(a.ev_join, a.side);
         if (err != cudaSuccess) return err;
     }
+    if (split) cells(a.ncell_big, a.ncell - a.ncell_big);
     if (a.n_small > 0)
         k_ibm_spread<128><<<a.n_small, 128, ibm_smem_bytes(a.g, a.smem_cells), st>>>(a, a.plane_list, a.smem_cells);
     err = cudaGetLastError();

@@ -156,6 +156,8 @@ int tdlb_double_resolution(tdlb_handle h) {
     drop(h->d_plane_lv1);
     drop(h->d_plane_cell);
     drop(h->d_plane_list);
+    drop(h->d_cell_order);
+    h->ncell_big = 0;
     drop(h->d_mask_static);
     drop(h->d_exclude);
     h->h_exclude.clear();

@@ -58,6 +58,7 @@ void release(tdlb_lattice* h) {
     cudaFree(h->d_plane_lv0);
     cudaFree(h->d_plane_lv1);
     cudaFree(h->d_cell_e);
+    cudaFree(h->d_cell_order);
     cudaFree(h->d_plane_cell);
     cudaFree(h->d_prep);
     cudaFree(h->d_cell_m);
@@ -567,6 +568,24 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
         h->big_tile_cells = tdlb::ibm_smem_bytes(g, big_max) <= 220 * 1024 ? big_max : 0;
         const size_t bytes = std::max(tdlb::ibm_smem_bytes(g, h->smem_cells), tdlb::ibm_smem_bytes(g, h->big_tile_cells));
         if (bytes > 48 * 1024) TDLB_CK(tdlb::ibm_prepare_smem(bytes));
+        // cell order of the pass: the big planes' cells, then the others
+        cudaFree(h->d_cell_order);
+        h->d_cell_order = nullptr;
+        h->ncell_big = 0;
+        if (!big.empty() && C0) {
+            std::vector<char> is_big((size_t)g.ny, 0);
+            for (int j : big) is_big[(size_t)j] = 1;
+            std::vector<int> order;
+            order.reserve((size_t)C0);
+            for (int pass = 1; pass >= 0; pass--)
+                for (int j = 0; j < g.ny; j++)
+                    if (is_big[(size_t)j] == pass)
+                        for (int c = h->cells.plane_cell[(size_t)j]; c < h->cells.plane_cell[(size_t)j + 1]; c++)
+                            order.push_back(c);
+            for (int j : big) h->ncell_big += h->cells.plane_cell[(size_t)j + 1] - h->cells.plane_cell[(size_t)j];
+            TDLB_CK(cudaMalloc(&h->d_cell_order, order.size() * sizeof(int)));
+            TDLB_CK(cudaMemcpy(h->d_cell_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+        }
         small.insert(small.end(), big.begin(), big.end());
         if (!h->d_plane_list) TDLB_CK(cudaMalloc(&h->d_plane_list, (size_t)g.ny * sizeof(int)));
         TDLB_CK(cudaMemcpy(h->d_plane_list, small.data(), (size_t)g.ny * sizeof(int), cudaMemcpyHostToDevice));
@@ -622,6 +641,8 @@ tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     a.cell_e = h->d_cell_e;
     a.plane_cell = h->d_plane_cell;
     a.ncell = (int)h->cells.cell_e.size();
+    a.cell_order = h->d_cell_order;
+    a.ncell_big = h->ncell_big;
     a.prep = h->d_prep;
     a.cell_m = h->d_cell_m;
     a.cell_F = h->d_cell_F;

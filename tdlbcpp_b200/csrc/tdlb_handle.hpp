@@ -45,6 +45,8 @@ struct tdlb_lattice {
     // first-segment cell lists and per-pass IBM buffers
     tdlb::CellList cells;
     int* d_cell_e = nullptr;
+    int* d_cell_order = nullptr;  // the big planes' cells first (NULL without big planes)
+    int ncell_big = 0;
     int* d_plane_cell = nullptr;
     float* d_prep = nullptr;      // PF_COUNT * n0
     float* d_cell_m = nullptr;    // 4 * C0

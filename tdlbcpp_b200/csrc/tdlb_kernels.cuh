@@ -82,6 +82,8 @@ struct IbmArgs {
     const int* cell_e;          // [C0] element index of each cell
     const int* plane_cell;      // [ny+1] cell range of each plane
     int ncell;                  // C0
+    const int* cell_order;      // [C0] the big planes' cells, then the others (NULL: no big plane)
+    int ncell_big;              // cells of the big planes
     const float* prep;          // PF_COUNT * n0 (slot-major fields)
     float* cell_m;              // 4 * C0: rho, jx, jy, jz of each cell this pass
     float* cell_F;              // 3 * C0: F of each cell at the start of this pass
