@@ -199,34 +199,51 @@ def run_ours(args, rank, world, device):
     ms = max_over_ranks(ms, world)
     kernel_ms_max = max_over_ranks(kernel_ms, world)
 
-    # ---- e2e: host-driven steps through the C ABI
+    # ---- e2e: host-driven steps through the C ABI. Per step the host
+    # generates the blades at the step's angle into pinned memory and uploads
+    # them (tdlb_set_rotating_markers), the step runs, and its FP64 impeller
+    # load comes back to pinned host memory. The host prepares step s+1's
+    # blades while the device runs step s (their upload is queued after the
+    # load of step s, which still needs step s's blades).
     pinned = torch.empty(n_rot * tb.MARKER_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
     host_rot = np.frombuffer(pinned.numpy(), dtype=tb.MARKER_DTYPE)
-    load = torch.empty(5 * 8, dtype=torch.uint8, pin_memory=True)
-    load_np = np.frombuffer(load.numpy(), dtype=np.float64)
+    load = torch.empty(5, dtype=torch.float64, pin_memory=True)
+    load_np = load.numpy()
+    got = torch.cuda.Event()
     spec = rt.spec
     k_e2e = max(3, args.steps // 5)
+    loads = []
 
-    def e2e_step():
+    def upload_next():
         nonlocal angle
         angle += dth
         n = tb.ctypes.c_size_t()
         rc = cu.lib.tdlb_rushton_rotating(tb.ctypes.byref(spec), angle, dth, tb._p(host_rot), n_rot, tb.ctypes.byref(n))
         assert rc == 0 and n.value == n_rot
         cu.set_rotating_markers(host_rot)
-        cu.collision()
-        cu.forcing_resident(ALPHA, BETA)
-        cu.impeller_load(load_np)
 
-    e2e_step()
+    def e2e_steps(k):
+        upload_next()
+        for s in range(k):
+            cu.collision()
+            cu.forcing_resident(ALPHA, BETA)
+            cu.impeller_load_async(load.data_ptr())
+            got.record(stream)
+            if s + 1 < k:
+                upload_next()
+            got.synchronize()
+            loads.append(load_np.copy())
+
+    e2e_steps(2)
     barrier(world)
     cu.synchronize()
+    loads.clear()
     w0 = time.perf_counter()
-    for _ in range(k_e2e):
-        e2e_step()
+    e2e_steps(k_e2e)
     cu.synchronize()
     w1 = time.perf_counter()
     barrier(world)
+    load_np = loads[-1]
     e2e_s = max_over_ranks(w1 - w0, world)
     red = cu.reduce_fp64()
     cu.close()

@@ -342,6 +342,13 @@ int tdlb_set_rotating_markers(tdlb_handle h, const tdlb_marker* markers, size_t 
  * momentum; out[3] = its torque about the tank axis (j); out[4] = markers
  * summed. A project-defined diagnostic: the reference computes none. */
 int tdlb_impeller_load(tdlb_handle h, double* out5);
+/* The same load, queued on the handle's stream with its copy into out5
+ * (pinned host memory or device memory), without waiting: out5 holds it once
+ * the stream has reached this point (tdlb_synchronize, or an event recorded
+ * on the stream after this call). Lets a caller prepare the next step on the
+ * host while the device finishes this one. The first call allocates the
+ * reduction's device scratch. */
+int tdlb_impeller_load_async(tdlb_handle h, double* out5);
 
 /* The same FP64 impeller load for callers that may not allocate device
  * memory while they run (inside CUDA graph capture, under their own memory

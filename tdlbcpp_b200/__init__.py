@@ -202,6 +202,7 @@ def load_library() -> ctypes.CDLL:
         "tdlb_set_rotating_markers": (i32, [H, vp, sz]),
         "tdlb_impeller_load": (i32, [H, vp]),
         "tdlb_impeller_load_noalloc": (i32, [H, vp]),
+        "tdlb_impeller_load_async": (i32, [H, vp]),
         "tdlb_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "tdlb_set_cells_per_thread": (i32, [H, i32]),
         "tdlb_set_overlap": (i32, [H, i32]),
@@ -481,6 +482,11 @@ class ComputeUnit:
         n = ctypes.c_int64()
         self._check(self.lib.tdlb_kernel_launches(self.h, ctypes.byref(n)))
         return n.value
+
+    def impeller_load_async(self, ptr: int):
+        """Queue the impeller load and its copy into 5 doubles at `ptr`
+        (pinned host or device memory) on this unit's stream; no wait."""
+        self._check(self.lib.tdlb_impeller_load_async(self.h, ctypes.c_void_p(ptr)))
 
     def impeller_load_noalloc(self, device_ptr: int):
         """Allocation-free impeller load into a caller-owned device buffer of

@@ -80,7 +80,10 @@ void release(tdlb_lattice* h) {
     cudaFree(h->d_red);
     cudaFree(h->d_rot_xz);
     cudaFree(h->d_load);
-    cudaFreeHost(h->h_stage);
+    for (auto& st : h->pin) {
+        cudaFreeHost(st.p);
+        if (st.ev) cudaEventDestroy(st.ev);
+    }
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     else if (h->stream) cudaStreamDestroy(h->stream);
 }
@@ -474,13 +477,23 @@ void validate_markers(const Dims& g, const tdlb_marker* m, size_t n, size_t base
     }
 }
 
+// Grow the level-pointer array, keeping its contents (the first segment's
+// levels stay valid when only the blade schedule grows).
 void ensure_level_cap(tdlb_lattice* h, long long need) {
     if (need <= h->level_cap && h->d_level_ptr) return;
     TDLB_CK(cudaStreamSynchronize(h->stream));
-    cudaFree(h->d_level_ptr);
-    h->d_level_ptr = nullptr;
     const long long cap = std::max<long long>(round_up(need * 2, 1024), 1024);
-    TDLB_CK(cudaMalloc(&h->d_level_ptr, cap * sizeof(int)));
+    int* p = nullptr;
+    TDLB_CK(cudaMalloc(&p, cap * sizeof(int)));
+    if (h->d_level_ptr) {
+        const cudaError_t e = cudaMemcpy(p, h->d_level_ptr, (size_t)h->level_cap * sizeof(int), cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(p);
+            TDLB_CK(e);
+        }
+        cudaFree(h->d_level_ptr);
+    }
+    h->d_level_ptr = p;
     h->level_cap = cap;
 }
 
@@ -1111,20 +1124,43 @@ int tdlb_set_rotating_markers(tdlb_handle h, const tdlb_marker* markers, size_t 
         if (n != (size_t)(h->n_markers - h->n0)) throw Fail{TDLB_EINVAL, "rotating marker count differs from the attached blades"};
         if (n && !markers) throw Fail{TDLB_EINVAL, "markers is NULL"};
         validate_markers(h->g, markers, n, (size_t)h->n0);
-        TDLB_CK(cudaStreamSynchronize(h->stream));   // previous tail copies read h_markers / seg1
+        // Host copies and the blade schedule for these positions; the uploads
+        // go through a pinned buffer and are queued after the work already on
+        // the stream (the previous forcing pass still reads the old blades),
+        // so this call does not wait for the device.
         std::copy(markers, markers + n, h->h_markers.begin() + h->n0);
         const auto* mk = reinterpret_cast<const tdlb::Marker*>(h->h_markers.data());
         h->seg1.build(mk, h->n0, h->n_markers, h->g.nx, h->g.ny, h->g.nz, h->n0, h->seg0.nlevels, nullptr);
-        if (n > h->stage_cap) {
-            cudaFreeHost(h->h_stage);
-            h->h_stage = nullptr;
-            TDLB_CK(cudaHostAlloc((void**)&h->h_stage, n * sizeof(tdlb_marker), cudaHostAllocDefault));
-            h->stage_cap = n;
+        const int L0 = h->seg0.nlevels;
+        ensure_level_cap(h, (long long)L0 + h->seg1.nlevels + 1);
+        const size_t b_mk = n * sizeof(tdlb::Marker);
+        const size_t b_order = n * sizeof(int);
+        const size_t b_lv = h->seg1.level_ptr.size() * sizeof(int);
+        const size_t b_pl = (size_t)(h->g.ny + 1) * sizeof(int);
+        const size_t need = b_mk + b_order + b_lv + b_pl;
+        auto& st = h->pin[h->pin_cur];
+        h->pin_cur ^= 1;
+        if (st.ev) TDLB_CK(cudaEventSynchronize(st.ev));   // the copies of two calls ago read this buffer
+        else TDLB_CK(cudaEventCreateWithFlags(&st.ev, cudaEventDisableTiming));
+        if (need > st.cap) {
+            cudaFreeHost(st.p);
+            st.p = nullptr;
+            st.cap = 0;
+            TDLB_CK(cudaHostAlloc((void**)&st.p, need, cudaHostAllocDefault));
+            st.cap = need;
         }
-        std::copy(markers, markers + n, h->h_stage);
-        if (n) TDLB_CK(cudaMemcpyAsync(h->d_markers + h->n0, h->h_stage, n * sizeof(tdlb::Marker),
-                                       cudaMemcpyHostToDevice, h->stream));
-        upload_seg1(h);
+        char* q = st.p;
+        std::memcpy(q, markers, b_mk);
+        std::memcpy(q + b_mk, h->seg1.order.data(), b_order);
+        std::memcpy(q + b_mk + b_order, h->seg1.level_ptr.data(), b_lv);
+        std::memcpy(q + b_mk + b_order + b_lv, h->seg1.plane_lv.data(), b_pl);
+        if (n) {
+            TDLB_CK(cudaMemcpyAsync(h->d_markers + h->n0, q, b_mk, cudaMemcpyHostToDevice, h->stream));
+            TDLB_CK(cudaMemcpyAsync(h->d_sched + h->n0, q + b_mk, b_order, cudaMemcpyHostToDevice, h->stream));
+        }
+        TDLB_CK(cudaMemcpyAsync(h->d_level_ptr + L0, q + b_mk + b_order, b_lv, cudaMemcpyHostToDevice, h->stream));
+        TDLB_CK(cudaMemcpyAsync(h->d_plane_lv1, q + b_mk + b_order + b_lv, b_pl, cudaMemcpyHostToDevice, h->stream));
+        TDLB_CK(cudaEventRecord(st.ev, h->stream));
         h->rot_device = false;   // the blades now follow the host's list
         // a split step needs every blade stencil cell inside the zone
         if (h->zone_gen == h->marker_gen)
@@ -1132,19 +1168,28 @@ int tdlb_set_rotating_markers(tdlb_handle h, const tdlb_marker* markers, size_t 
     });
 }
 
+// Queue the impeller load of the last forcing pass and its copy into out5.
+void queue_impeller_load(tdlb_lattice* h, double* out5) {
+    if (!out5) throw Fail{TDLB_EINVAL, "out is NULL"};
+    if (h->impeller_begin < 0) throw Fail{TDLB_ESTATE, "no impeller attached (tdlb_attach_rushton)"};
+    if (h->pass == 0) throw Fail{TDLB_ESTATE, "no forcing pass yet"};
+    if (!h->d_load) TDLB_CK(cudaMalloc(&h->d_load, (size_t)(tdlb::kLoadBlocks * 5 + 5) * sizeof(double)));
+    tdlb::IbmArgs a = ibm_args(h, 0.f, h->last_beta);
+    TDLB_CK(tdlb::launch_marker_load(a, h->impeller_begin, h->rot_ci, h->rot_ck, h->d_load,
+                                     h->d_load + tdlb::kLoadBlocks * 5, h->stream));
+    TDLB_CK(cudaMemcpyAsync(out5, h->d_load + tdlb::kLoadBlocks * 5, 5 * sizeof(double), cudaMemcpyDefault,
+                            h->stream));
+}
+
 int tdlb_impeller_load(tdlb_handle h, double* out5) {
     return guarded(h, [&] {
-        if (!out5) throw Fail{TDLB_EINVAL, "out is NULL"};
-        if (h->impeller_begin < 0) throw Fail{TDLB_ESTATE, "no impeller attached (tdlb_attach_rushton)"};
-        if (h->pass == 0) throw Fail{TDLB_ESTATE, "no forcing pass yet"};
-        if (!h->d_load) TDLB_CK(cudaMalloc(&h->d_load, (size_t)(tdlb::kLoadBlocks * 5 + 5) * sizeof(double)));
-        tdlb::IbmArgs a = ibm_args(h, 0.f, h->last_beta);
-        TDLB_CK(tdlb::launch_marker_load(a, h->impeller_begin, h->rot_ci, h->rot_ck, h->d_load,
-                                         h->d_load + tdlb::kLoadBlocks * 5, h->stream));
-        TDLB_CK(cudaMemcpyAsync(out5, h->d_load + tdlb::kLoadBlocks * 5, 5 * sizeof(double), cudaMemcpyDeviceToHost,
-                                h->stream));
+        queue_impeller_load(h, out5);
         TDLB_CK(cudaStreamSynchronize(h->stream));
     });
+}
+
+int tdlb_impeller_load_async(tdlb_handle h, double* out5) {
+    return guarded(h, [&] { queue_impeller_load(h, out5); });
 }
 
 int tdlb_read_markers(tdlb_handle h, tdlb_marker* out, size_t cap, size_t* n) {

@@ -82,8 +82,15 @@ struct tdlb_lattice {
     double angle = 0.0;           // impeller angle of the last rotation
     unsigned long long rstep = 1; // main-loop step the angle belongs to (main.cpp:336 starts at 1)
     double* d_load = nullptr;     // kLoadBlocks*5 partials + 5 results
-    tdlb_marker* h_stage = nullptr;   // pinned staging of the blade upload
-    size_t stage_cap = 0;
+    // pinned staging of the per-step blade upload (markers and their
+    // schedule), two buffers used in turn; each buffer's event marks the end
+    // of the copies that read it
+    struct PinStage {
+        char* p = nullptr;
+        size_t cap = 0;
+        cudaEvent_t ev = nullptr;
+    } pin[2];
+    int pin_cur = 0;
     std::vector<double> h_rot_xz; // host copy of d_rot_xz
 
     // Split steps: the outer chunks of a step run on `stream` while the
