@@ -396,10 +396,12 @@ int tdlb_batch_add(tdlb_batch b, const tdlb_config* cfg, int* index);
 int tdlb_batch_remove(tdlb_batch b, int index);
 int tdlb_batch_tank(tdlb_batch b, int t, tdlb_handle* out);
 /* Shape of the fused batched launch: cells per thread (1, 2, 4; 16-bit
- * storage 1 or 4) and threads per block (128 or 256). The launch runs one
- * block per work item (threads x cells per thread cells of one tank), so
- * the block scheduler balances it against the other group's forcing pass;
- * blocks_per_sm (1..16) is kept for callers and no longer shapes the grid. */
+ * storage 1 or 4), threads per block (128 or 256) and blocks per SM: 1..16
+ * makes the launch persistent (grid = min(work items, SMs x blocks_per_sm),
+ * each block taking items b, b + grid, ...); 0 (the default) runs one block
+ * per work item, which the block scheduler balances against the other
+ * group's forcing pass. A work item is eight chunks of `threads` quads of
+ * one tank. */
 int tdlb_batch_set_shape(tdlb_batch b, int cells_per_thread, int threads, int blocks_per_sm);
 int tdlb_batch_get_shape(tdlb_batch b, int* cells_per_thread, int* threads, int* blocks_per_sm);
 /* Times every shape on the initialised batch and keeps the fastest

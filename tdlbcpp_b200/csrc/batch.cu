@@ -192,7 +192,8 @@ struct tdlb_batch_s {
     std::vector<int> table_cap;
     TankRotor* d_rotors = nullptr;     // [n]
     std::vector<unsigned> ibm_gen;     // marker generation the IBM lists were built for
-    int vec = 1, threads = 128, bps = 4;   // fused-launch shape
+    int vec = 1, threads = 128, bps = 0;   // fused-launch shape (bps 0: one block per work item)
+    int sms = 0;                           // SMs of the device
     long long launches = 0;            // kernels run by tdlb_batch_run* so far
     std::string err = "no error";
 };
@@ -347,13 +348,14 @@ void advance_step_state(tdlb_lattice* h) {
     h->holds_moments = false;
 }
 
-// The fused launch over `work`: one block per item (no persistence), so
-// that the block scheduler fills the SMs the other group's forcing pass
-// leaves free.
+// The fused launch over `work`: persistent blocks (bps per SM, each taking
+// items b, b + grid, ...) or, with bps = 0, one block per item, so that the
+// block scheduler fills the SMs the other group's forcing pass leaves free.
 void launch_fused(tdlb_batch_s* b, const TankStep* d_views, const WorkList& work, int* counter, cudaStream_t st) {
     if (work.n == 0) return;
     const tdlb::BatchFn fn = tdlb::batch_kernel(storage_of(b), eso_of(b), b->vec, b->threads);
-    fn<<<work.n, b->threads, 0, st>>>(d_views, work.d, work.n, counter);
+    const int grid = b->bps > 0 ? std::min(work.n, b->sms * b->bps) : work.n;
+    fn<<<grid, b->threads, 0, st>>>(d_views, work.d, work.n, counter);
     TDLB_BCK(cudaGetLastError());
 }
 
@@ -660,6 +662,7 @@ void release(tdlb_batch_s* b) {
 // Streams, events and the step counters of a new batch.
 void init_streams(tdlb_batch_s* b) {
     TDLB_BCK(cudaSetDevice(b->device));
+    TDLB_BCK(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
     TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     TDLB_BCK(cudaEventCreateWithFlags(&b->ev_split, cudaEventDisableTiming));
     TDLB_BCK(cudaEventCreateWithFlags(&b->ev_merge, cudaEventDisableTiming));
@@ -770,7 +773,7 @@ int tdlb_batch_set_shape(tdlb_batch b, int cells_per_thread, int threads, int bl
         if (cells_per_thread == 2 && storage_of(b) != TDLB_STORAGE_FP32)
             throw BFail{TDLB_EINVAL, "16-bit storage runs 1 or 4 cells per thread"};
         if (threads != 128 && threads != 256) throw BFail{TDLB_EINVAL, "threads must be 128 or 256"};
-        if (blocks_per_sm < 1 || blocks_per_sm > 16) throw BFail{TDLB_EINVAL, "blocks per SM must be 1..16"};
+        if (blocks_per_sm < 0 || blocks_per_sm > 16) throw BFail{TDLB_EINVAL, "blocks per SM must be 0..16"};
         b->vec = cells_per_thread;
         b->threads = threads;
         b->bps = blocks_per_sm;
@@ -801,7 +804,8 @@ int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms) {
         const bool h16 = storage_of(b) != TDLB_STORAGE_FP32;
         for (int v : {1, 2, 4}) {
             if (h16 && v == 2) continue;
-            for (int nt : {128, 256}) cands.push_back({v, nt, b->bps});
+            for (int nt : {128, 256})
+                for (int bps : {0, 4, 8}) cands.push_back({v, nt, bps});
         }
         TDLB_BCK(cudaDeviceSynchronize());
         upload_views(b, 0.f, 0.f);

@@ -103,7 +103,7 @@ def test_graph_replay_equals_eager(gpu, streaming):
 def test_batch_shapes_agree(gpu, streaming):
     tb = gpu
     res = []
-    for shape in [(1, 128, 4), (2, 256, 2), (4, 128, 8), (4, 256, 1)]:
+    for shape in [(1, 128, 4), (2, 256, 2), (4, 128, 8), (4, 256, 1), (1, 128, 0)]:
         with make_batch(tb, streaming, "fp32") as b:
             b.set_shape(*shape)
             assert b.shape() == shape
