@@ -472,7 +472,7 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
 }
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes,
+__global__ void __launch_bounds__(THREADS, 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes,
                                                                        int tile_cells) {
     extern __shared__ float tile[];                             // [3][tile_cells]
     ibm_spread_plane<THREADS>(a, planes[blockIdx.x], tile_cells, tile);
@@ -642,8 +642,6 @@ cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
 }
 
 cudaError_t ibm_prepare_smem(size_t bytes) {
-    cudaError_t e = raise_smem_limit((const void*)k_ibm_spread<128>, bytes);
-    if (e != cudaSuccess) return e;
     return raise_smem_limit((const void*)k_ibm_spread<512>, bytes);
 }
 
@@ -690,7 +688,7 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
     }
     if (split) cells(a.ncell_big, a.ncell - a.ncell_big);
     if (a.n_small > 0)
-        k_ibm_spread<128><<<a.n_small, 128, ibm_smem_bytes(a.g, a.smem_cells), st>>>(a, a.plane_list, a.smem_cells);
+        k_ibm_spread<512><<<a.n_small, 512, ibm_smem_bytes(a.g, a.smem_cells), st>>>(a, a.plane_list, a.smem_cells);
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     if (a.n_big > 0) return cudaStreamWaitEvent(st, a.ev_join, 0);

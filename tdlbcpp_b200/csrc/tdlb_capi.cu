@@ -556,8 +556,8 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
     }
     if (n0) TDLB_CK(cudaMalloc(&h->d_prep, (size_t)tdlb::PF_COUNT * n0 * sizeof(float)));
     {
-        // F tiles of the 128-thread launch: 3 CTAs per SM fit 3 tiles of up
-        // to 6144 cells (72 KB) in shared memory;
+        // F tiles of the ordinary planes' launch: up to 6144 cells (72 KB)
+        // of shared memory;
         // the tile is sized for the most crowded ordinary plane, at least
         // 4608 cells. Planes with more cells (an impeller disk) go to a
         // second, 512-thread launch with a tile for the largest of them
