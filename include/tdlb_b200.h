@@ -393,6 +393,15 @@ int tdlb_batch_size(tdlb_batch b, int* n);
 /* A tank joins (index: its position) or leaves the batch between runs; a
  * removed tank's handle is destroyed and later tanks move down by one. */
 int tdlb_batch_add(tdlb_batch b, const tdlb_config* cfg, int* index);
+/* A lattice created with tdlb_create* and prepared on its own stream
+ * (markers attached, initialised, first forcing pass) joins the batch as its
+ * last tank: its stream is drained, it runs on the batch's streams from then
+ * on and the batch owns it (tdlb_batch_remove or tdlb_batch_destroy destroys
+ * it; the caller must not). Its streaming scheme, storage and device must be
+ * the batch's. Setting a tank up this way overlaps a running batch, where
+ * tdlb_batch_add's tank is set up on the batch's stream after it. No
+ * counterpart in the reference, which runs one lattice per process. */
+int tdlb_batch_adopt(tdlb_batch b, tdlb_handle h, int* index);
 int tdlb_batch_remove(tdlb_batch b, int index);
 int tdlb_batch_tank(tdlb_batch b, int t, tdlb_handle* out);
 /* Shape of the fused batched launch: cells per thread (1, 2, 4; 16-bit

@@ -225,6 +225,7 @@ def load_library() -> ctypes.CDLL:
         "tdlb_batch_size": (i32, [H, ctypes.POINTER(i32)]),
         "tdlb_batch_tank": (i32, [H, i32, ctypes.POINTER(H)]),
         "tdlb_batch_add": (i32, [H, ctypes.POINTER(Config), ctypes.POINTER(i32)]),
+        "tdlb_batch_adopt": (i32, [H, H, ctypes.POINTER(i32)]),
         "tdlb_batch_remove": (i32, [H, i32]),
         "tdlb_batch_set_shape": (i32, [H, i32, i32, i32]),
         "tdlb_batch_get_shape": (i32, [H, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
@@ -617,6 +618,18 @@ class Batch:
         th = ctypes.c_void_p()
         self._check(self.lib.tdlb_batch_tank(self.h, idx.value, ctypes.byref(th)))
         cu = ComputeUnit._borrowed(self.lib, th)
+        self.tanks.append(cu)
+        return cu
+
+    def adopt(self, cu: "ComputeUnit") -> "ComputeUnit":
+        """A standalone ComputeUnit, already set up on its own stream, joins
+        the batch as its last tank; the batch owns it from then on (closing
+        `cu` no longer destroys it). Returns `cu`, now a view."""
+        if not getattr(cu, "_owned", False) or not getattr(cu, "h", None):
+            raise TdlbError(-5, "only a standalone, open ComputeUnit can be adopted")
+        idx = ctypes.c_int()
+        self._check(self.lib.tdlb_batch_adopt(self.h, cu.h, ctypes.byref(idx)))
+        cu._owned = False
         self.tanks.append(cu)
         return cu
 

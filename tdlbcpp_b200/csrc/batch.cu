@@ -268,6 +268,14 @@ void assign_groups(tdlb_batch_s* b) {
     for (BatchGroup& G : b->grp) std::sort(G.tanks.begin(), G.tanks.end());
 }
 
+// Waits for the batch's own two streams, not the whole device: tanks set up on
+// their own streams (for tdlb_batch_adopt) keep running meanwhile.
+cudaError_t quiesce(tdlb_batch_s* b) {
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess && b->grp[1].stream && b->grp[1].stream != b->stream) e = cudaStreamSynchronize(b->grp[1].stream);
+    return e;
+}
+
 // Fused-step work lists for the current shape: (tank, first quad) per item,
 // for every tank and per group.
 void build_work(tdlb_batch_s* b) {
@@ -282,7 +290,7 @@ void build_work(tdlb_batch_s* b) {
     };
     std::vector<int> all(b->tanks.size());
     for (size_t t = 0; t < all.size(); t++) all[t] = (int)t;
-    TDLB_BCK(cudaDeviceSynchronize());   // queued launches may still read the old lists
+    TDLB_BCK(quiesce(b));   // queued launches may still read the old lists
     put(b->work, items(all));
     for (BatchGroup& G : b->grp) put(G.work, items(G.tanks));
 }
@@ -292,7 +300,7 @@ void build_ibm_work(tdlb_batch_s* b) {
     bool same = true;
     for (size_t t = 0; t < b->tanks.size(); t++) same = same && b->ibm_gen[t] == b->tanks[t]->marker_gen;
     if (same) return;
-    TDLB_BCK(cudaDeviceSynchronize());
+    TDLB_BCK(quiesce(b));
     int small_all = 0, big_all = 0;
     for (BatchGroup& G : b->grp) {
         std::vector<int2> cells, tails, copies, small, big;
@@ -536,6 +544,24 @@ tdlb_lattice* add_tank(tdlb_batch_s* b, const tdlb_config& cfg) {
     return h;
 }
 
+// A lattice created and prepared on its own stream joins the batch: its
+// stream is drained and replaced by the batch's (as for add_tank), and the
+// batch owns it from then on.
+void adopt_tank(tdlb_batch_s* b, tdlb_lattice* h) {
+    if (!h) throw BFail{TDLB_EINVAL, "handle is NULL"};
+    if (h->own_stream) throw BFail{TDLB_ESTATE, "the lattice already belongs to a batch"};
+    if (h->cfg.streaming != b->streaming || h->cfg.storage != b->storage)
+        throw BFail{TDLB_EINVAL, "all tanks of a batch share one streaming scheme and one storage precision"};
+    if (h->device != b->device) throw BFail{TDLB_EINVAL, "the lattice lives on another device"};
+    tdlb_rt::borrow_stream(h, b->stream);
+    h->vec = b->vec;
+    b->tanks.push_back(h);
+    b->d_table.push_back(nullptr);
+    b->table_cap.push_back(0);
+    b->ibm_gen.push_back(~0u);
+    b->members_changed = true;
+}
+
 void remove_tank(tdlb_batch_s* b, int t) {
     if (t < 0 || t >= (int)b->tanks.size()) throw BFail{TDLB_EINVAL, "tank index out of range"};
     TDLB_BCK(cudaStreamSynchronize(b->stream));
@@ -571,7 +597,7 @@ void eager_step(tdlb_batch_s* b, float alpha, float beta) {
 void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
     if (b->tanks.empty()) return;
     check_ready(b);
-    TDLB_BCK(cudaDeviceSynchronize());   // the previous run may still read the tables and lists
+    TDLB_BCK(quiesce(b));   // the previous run may still read the tables and lists
     sync_members(b);
     build_ibm_work(b);
     build_tables(b, steps);
@@ -739,6 +765,13 @@ int tdlb_batch_add(tdlb_batch b, const tdlb_config* cfg, int* index) {
     });
 }
 
+int tdlb_batch_adopt(tdlb_batch b, tdlb_handle h, int* index) {
+    return bguard(b, [&] {
+        adopt_tank(b, h);
+        if (index) *index = (int)b->tanks.size() - 1;
+    });
+}
+
 int tdlb_batch_remove(tdlb_batch b, int index) {
     return bguard(b, [&] { remove_tank(b, index); });
 }
@@ -807,7 +840,7 @@ int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms) {
             for (int nt : {128, 256})
                 for (int bps : {0, 4, 8}) cands.push_back({v, nt, bps});
         }
-        TDLB_BCK(cudaDeviceSynchronize());
+        TDLB_BCK(quiesce(b));
         upload_views(b, 0.f, 0.f);
         cudaEvent_t e0, e1;
         TDLB_BCK(cudaEventCreate(&e0));

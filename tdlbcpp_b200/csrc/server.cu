@@ -185,22 +185,25 @@ bool admit_one(tdlb_server_s* s, const Pending& p, long long need) {
         push_result(s, failed(r, TDLB_ECUDA, p.t_submit, s->now()));
         return false;
     }
-    int idx = -1;
-    int rc = tdlb_batch_add(b, &c, &idx);
-    if (rc != TDLB_OK) {
-        note(s, std::string("admission: ") + tdlb_batch_last_error(b));
-        push_result(s, failed(r, rc, p.t_submit, s->now()));
-        return false;
-    }
+    // The tank is set up on its own stream, so this overlaps a running chunk;
+    // adopting it drains that stream and moves it onto the batch's.
     tdlb_handle h = nullptr;
-    tdlb_batch_tank(b, idx, &h);
+    int rc = tdlb_create_config(&c, s->device, &h);
     const double d1 = tdlb_rushton_impeller_increment(&spec, 1);
-    rc = tdlb_attach_rushton(h, &spec, d1, d1, d1);
+    if (rc == TDLB_OK) rc = tdlb_attach_rushton(h, &spec, d1, d1, d1);
     if (rc == TDLB_OK) rc = tdlb_initialise(h, 1.0f);
     if (rc == TDLB_OK) rc = tdlb_forcing_resident(h, s->alpha, s->beta);
     if (rc != TDLB_OK) {
         note(s, std::string("tank setup: ") + tdlb_last_error(h));
-        tdlb_batch_remove(b, idx);
+        if (h) tdlb_destroy(h);
+        push_result(s, failed(r, rc, p.t_submit, s->now()));
+        return false;
+    }
+    int idx = -1;
+    rc = tdlb_batch_adopt(b, h, &idx);
+    if (rc != TDLB_OK) {
+        note(s, std::string("admission: ") + tdlb_batch_last_error(b));
+        tdlb_destroy(h);
         push_result(s, failed(r, rc, p.t_submit, s->now()));
         return false;
     }
@@ -301,6 +304,10 @@ void step_chunk(tdlb_server_s* s) {
             if (rc != TDLB_OK) why = tdlb_batch_last_error(kv.second);
         }
     }
+    // Requests admitted now are set up while the chunk runs; they join the
+    // next chunk.
+    const size_t running = s->active.size();
+    if (rc == TDLB_OK) admit(s);
     for (auto& kv : s->batches)
         if (tdlb_batch_synchronize(kv.second) != TDLB_OK && rc == TDLB_OK) {
             rc = TDLB_ECUDA;
@@ -333,12 +340,13 @@ void step_chunk(tdlb_server_s* s) {
     }
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        for (Active& a : s->active) {
+        for (size_t k = 0; k < running; k++) {
+            Active& a = s->active[k];
             a.remaining -= chunk;
             s->lattice_updates += (double)a.req.x * a.req.y * a.req.z * (double)chunk;
         }
     }
-    for (size_t k = s->active.size(); k-- > 0;)
+    for (size_t k = running; k-- > 0;)
         if (s->active[k].remaining <= 0) retire(s, k);
 }
 

@@ -120,13 +120,38 @@ def test_autotune_then_run(gpu):
         ms = b.autotune(trials=2)
         assert ms > 0
         v, t, bps = b.shape()
-        assert v in (1, 2, 4) and t in (128, 256) and 1 <= bps <= 16
+        assert v in (1, 2, 4) and t in (128, 256) and 0 <= bps <= 16
         for cu in b.tanks:   # the timed launches changed the fields
             cu.initialise(1.0)
             cu.forcing_resident(ALPHA, BETA)
         b.run(4, ALPHA, BETA)
         rho, u = b.tanks[0].read_velocity_density()
         assert np.isfinite(u).all() and np.isfinite(rho).all()
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_adopted_tank_matches_tank_alone(gpu, streaming):
+    """A tank set up on its own stream while a batch is running (the serving
+    form's admission) joins the batch and then follows the trajectory it
+    follows alone; the tanks already there carry on."""
+    tb = gpu
+    with make_batch(tb, streaming, "fp32", TANKS[:2]) as b:
+        b.run(3, ALPHA, BETA)
+        rt, cfg = tank_config(tb, TANKS[2], streaming, "fp32")
+        cu = tb.ComputeUnit(**cfg)
+        prepare(cu, rt)
+        assert b.adopt(cu) is cu and len(b) == 3
+        b.run(5, ALPHA, BETA)
+        (rho, u), F = cu.read_velocity_density(), cu.read_force()
+        with pytest.raises(tb.TdlbError):
+            b.adopt(cu)               # already the batch's
+        cu.close()                    # a view now: the batch still owns the tank
+        assert len(b) == 3
+        b.run(1, ALPHA, BETA)
+    (rho0, u0), F0, _ = run_alone(tb, TANKS[2], streaming, "fp32", 5)
+    assert rel_l2(u, u0) <= 1e-6
+    assert rel_l2(rho, rho0) <= 1e-6
+    assert rel_l2(F, F0) <= 1e-5
 
 
 def test_batch_rejects_mixed_schemes(gpu):
