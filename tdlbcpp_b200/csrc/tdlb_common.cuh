@@ -221,17 +221,36 @@ __device__ __forceinline__ void moments4_of(const float* q, float* m) {
 // each group of opposite directions. alpha[M17] = alpha[M18] = 0, so the
 // fourth-order columns drop out.
 //
+// FAST: hardware-approximate reciprocals and square root (16-bit forms).
 // DEV (16-bit deviation storage): the populations in and out are deviations
 // f - w rho0. The moments of the rest populations are (rho0, 0, ..., 0) and
 // the inverse filter maps alpha0 = rho0 / 24 back to them, so m[0] holds
 // rho - rho0 and alpha0 is taken as (rho - rho0) / 24: every output is then
 // the deviation itself, without adding and removing the rest weights.
 // ---------------------------------------------------------------------------
-template <bool LES, bool DEV = false>
+// Hardware approximations (PTX rcp.approx / sqrt.approx, flush-to-zero):
+// one instruction each instead of the IEEE-rounded sequences. Only for the
+// 16-bit storage forms, whose state is rounded to 11 significant bits on
+// every store, far above the approximations' few-ulp FP32 error; the FP32
+// form keeps IEEE rounding.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+template <bool FAST>
+__device__ __forceinline__ float rcp_of(float x) { return FAST ? rcp_approx(x) : __frcp_rn(x); }
+
+template <bool LES, bool DEV = false, bool FAST = false>
 __device__ __forceinline__ void collide(const float* m, float fx, float fy, float fz, float& nu,
                                         const CollideParams& p, float* out) {
     const float rho = DEV ? m[0] + p.rho0 : m[0];
-    const float inv_rho = __frcp_rn(rho);
+    const float inv_rho = rcp_of<FAST>(rho);
     const float jx = fmaf(0.5f, fx, m[1]);
     const float jy = fmaf(0.5f, fy, m[2]);
     const float jz = fmaf(0.5f, fz, m[3]);
@@ -240,7 +259,7 @@ __device__ __forceinline__ void collide(const float* m, float fx, float fy, floa
     float b = p.b0, c = p.c0;
     if (LES) {
         // fct = 3 / (rho (1 + 6 (Nu + nu)))       (:52)
-        const float fct = 3.f * __frcp_rn(rho * fmaf(6.f, nu + p.nu, 1.f));
+        const float fct = 3.f * rcp_of<FAST>(rho * fmaf(6.f, nu + p.nu, 1.f));
         // literal grouping of :55-65: m + 0.5*F*u - m
         const float dudx = fct * (fmaf(0.5f * fx, ux, m[1]) - m[4]);
         const float dvdy = fct * (fmaf(0.5f * fy, uy, m[2]) - m[6]);
@@ -251,9 +270,9 @@ __device__ __forceinline__ void collide(const float* m, float fx, float fy, floa
         const float syz = 2.f * fct * (fmaf(0.5f * fz, uy, m[3]) - m[8]);
         const float sh = 2.f * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + sxy * sxy + sxz * sxz + syz * syz
                        - (2.f / 3.f) * divv * divv;
-        nu = p.cs0sq * sqrtf(fabsf(sh));            // (:74)
+        nu = p.cs0sq * (FAST ? sqrt_approx(fabsf(sh)) : sqrtf(fabsf(sh)));   // (:74)
         const float nut = nu + p.nu;
-        b = __frcp_rn(fmaf(6.f, nut, 1.f));
+        b = rcp_of<FAST>(fmaf(6.f, nut, 1.f));
         c = fmaf(-6.f, nut, 1.f);
     }
 
