@@ -436,9 +436,10 @@ int tdlb_batch_get_stream(tdlb_batch b, void** stream);
  * admits submitted requests in arrival order while a slot is free and the
  * tank's device bytes (tdlb_lattice_bytes) fit the free HBM (less 1 GiB)
  * and the budget; builds each admitted tank (a Rushton turbine filling the
- * lattice, tip speed and Re as requested, LES with Cs = 0.1, rho = 1),
- * forces it once (main.cpp:305) and adds it to the resident batch of its
- * precision and scheme; advances every resident tank in chunks of
+ * lattice, tip speed and Re as requested, LES with Cs = 0.1, rho = 1) and
+ * forces it once (main.cpp:305) on the tank's own stream, overlapping the
+ * chunk that is running, then adopts it into the resident batch of its
+ * precision and scheme (tdlb_batch_adopt); advances every resident tank in chunks of
  * min(chunk_steps, smallest remaining step count) with alpha = 0.97,
  * beta = 1.9; and retires finished tanks, freeing their memory. A tank's
  * result does not depend on what else is resident. */
