@@ -421,7 +421,9 @@ int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms);
  * (main.cpp:409-454): impeller rotation (tanks with tdlb_attach_rushton, the
  * angle advanced by tdlb_rushton_impeller_increment of the step), fused
  * collision + streaming, immersed-boundary forcing (tanks with markers) with
- * alpha, beta. Pairs of steps replay one captured CUDA graph. */
+ * alpha, beta. Pairs of steps replay captured CUDA graphs (four pairs, then
+ * single pairs), kept between runs while the batch's tanks and shape stay
+ * the same. */
 int tdlb_batch_run(tdlb_batch b, int steps, float alpha, float beta);
 /* Same steps, every launch issued eagerly (no graph). */
 int tdlb_batch_run_eager(tdlb_batch b, int steps, float alpha, float beta);

@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -167,6 +168,7 @@ struct BatchGroup {
     std::vector<int> tanks;            // indices into tdlb_batch_s::tanks
     WorkList work;                     // fused-step items (tank, first quad)
     WorkList rot_work;                 // (tank, first blade)
+    std::vector<int2> rot_items;       // host copy of rot_work
     WorkList cells, tails, copies, small, big;   // immersed-boundary items
     int small_tile = 0, big_tile = 0;
     cudaStream_t stream = nullptr;     // group 0: the batch's stream
@@ -188,9 +190,16 @@ struct tdlb_batch_s {
     WorkList work;                     // fused-step items of every tank (autotuner)
     BatchGroup grp[2];
     int* d_step = nullptr;             // [2] device step counters of a run (one per group)
-    std::vector<double*> d_table;      // per tank: [steps][3] cos, sin, delta
-    std::vector<int> table_cap;
+    double* d_tables = nullptr;        // per rotating tank: [steps][3] cos, sin, delta, back to back
+    size_t tables_cap = 0;             // doubles d_tables holds
     TankRotor* d_rotors = nullptr;     // [n]
+    // Instantiated graphs of kPairsPerGraph step pairs (0) and of one pair
+    // (1), kept while everything their launches name stays the same (key).
+    struct CachedGraph {
+        cudaGraphExec_t ge = nullptr;
+        std::vector<uintptr_t> key;
+        int kernels = 0;
+    } graphs[2];
     std::vector<unsigned> ibm_gen;     // marker generation the IBM lists were built for
     int vec = 1, threads = 128, bps = 0;   // fused-launch shape (bps 0: one block per work item)
     int sms = 0;                           // SMs of the device
@@ -448,42 +457,61 @@ void upload_views(tdlb_batch_s* b, float alpha, float beta) {
 }
 
 // Per-step (cos, sin, delta) of every attached impeller for `steps` steps,
-// and the rotation launch's tank table.
+// and the rotation launch's tank table: one allocation and two asynchronous
+// copies on the batch's stream (run() has waited for the previous run, the
+// only reader). The rotation work lists are rebuilt only when they change.
 void build_tables(tdlb_batch_s* b, int steps) {
-    std::vector<TankRotor> rot(b->tanks.size());
-    for (size_t t = 0; t < b->tanks.size(); t++) {
+    const size_t n = b->tanks.size();
+    std::vector<TankRotor> rot(n);
+    std::vector<size_t> off(n, 0);
+    size_t total = 0;
+    for (size_t t = 0; t < n; t++) {
+        const tdlb_lattice* h = b->tanks[t];
+        if (!h->rot_device || h->n_markers == h->n0) continue;
+        off[t] = total;
+        total += (size_t)3 * steps;
+    }
+    if (total > b->tables_cap) {
+        cudaFree(b->d_tables);
+        b->d_tables = nullptr;
+        b->tables_cap = 0;
+        TDLB_BCK(cudaMalloc(&b->d_tables, total * sizeof(double)));
+        b->tables_cap = total;
+    }
+    std::vector<double> tab(total);
+    for (size_t t = 0; t < n; t++) {
         tdlb_lattice* h = b->tanks[t];
         rot[t] = TankRotor{};
         if (!h->rot_device || h->n_markers == h->n0) continue;
-        if (b->table_cap[t] < steps) {
-            cudaFree(b->d_table[t]);
-            b->d_table[t] = nullptr;
-            b->table_cap[t] = 0;
-            TDLB_BCK(cudaMalloc(&b->d_table[t], (size_t)3 * steps * sizeof(double)));
-            b->table_cap[t] = steps;
-        }
         const tdlb::RushtonGeom G = tdlb::RushtonGeom::from(h->rspec);
-        std::vector<double> tab((size_t)3 * steps);
+        double* tt = tab.data() + off[t];
         double angle = h->angle;
         unsigned long long st = h->rstep;
         for (int s = 0; s < steps; s++) {
             st++;
             const double d = G.increment(st);
             angle += d;
-            tab[(size_t)3 * s] = std::cos(angle);
-            tab[(size_t)3 * s + 1] = std::sin(angle);
-            tab[(size_t)3 * s + 2] = d;
+            tt[(size_t)3 * s] = std::cos(angle);
+            tt[(size_t)3 * s + 1] = std::sin(angle);
+            tt[(size_t)3 * s + 2] = d;
         }
-        TDLB_BCK(cudaMemcpy(b->d_table[t], tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
         const int nr = h->n_markers - h->n0;
-        rot[t] = TankRotor{h->d_rot_xz, h->d_markers + h->n0, b->d_table[t], h->rot_ci, h->rot_ck, nr, h->g.nx, h->g.nz, 0};
+        rot[t] = TankRotor{h->d_rot_xz, h->d_markers + h->n0, b->d_tables + off[t], h->rot_ci, h->rot_ck, nr, h->g.nx,
+                           h->g.nz, 0};
     }
-    TDLB_BCK(cudaMemcpy(b->d_rotors, rot.data(), rot.size() * sizeof(TankRotor), cudaMemcpyHostToDevice));
+    if (total) TDLB_BCK(cudaMemcpyAsync(b->d_tables, tab.data(), total * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    // (copies from pageable memory are staged before the calls return)
+    TDLB_BCK(cudaMemcpyAsync(b->d_rotors, rot.data(), n * sizeof(TankRotor), cudaMemcpyHostToDevice, b->stream));
     for (BatchGroup& G : b->grp) {
         std::vector<int2> items;
         for (int t : G.tanks)
             for (int q = 0; q < rot[(size_t)t].n; q += 256) items.push_back(make_int2(t, q));
-        put(G.rot_work, items);
+        const bool same = items.size() == G.rot_items.size() &&
+                          (items.empty() || std::memcmp(items.data(), G.rot_items.data(), items.size() * sizeof(int2)) == 0);
+        if (!same) {
+            put(G.rot_work, items);
+            G.rot_items = items;
+        }
     }
 }
 
@@ -537,8 +565,6 @@ tdlb_lattice* add_tank(tdlb_batch_s* b, const tdlb_config& cfg) {
     tdlb_rt::borrow_stream(h, b->stream);
     h->vec = b->vec;
     b->tanks.push_back(h);
-    b->d_table.push_back(nullptr);
-    b->table_cap.push_back(0);
     b->ibm_gen.push_back(~0u);
     b->members_changed = true;
     return h;
@@ -556,8 +582,6 @@ void adopt_tank(tdlb_batch_s* b, tdlb_lattice* h) {
     tdlb_rt::borrow_stream(h, b->stream);
     h->vec = b->vec;
     b->tanks.push_back(h);
-    b->d_table.push_back(nullptr);
-    b->table_cap.push_back(0);
     b->ibm_gen.push_back(~0u);
     b->members_changed = true;
 }
@@ -566,10 +590,7 @@ void remove_tank(tdlb_batch_s* b, int t) {
     if (t < 0 || t >= (int)b->tanks.size()) throw BFail{TDLB_EINVAL, "tank index out of range"};
     TDLB_BCK(cudaStreamSynchronize(b->stream));
     tdlb_destroy(b->tanks[(size_t)t]);
-    cudaFree(b->d_table[(size_t)t]);
     b->tanks.erase(b->tanks.begin() + t);
-    b->d_table.erase(b->d_table.begin() + t);
-    b->table_cap.erase(b->table_cap.begin() + t);
     b->ibm_gen.erase(b->ibm_gen.begin() + t);
     b->members_changed = true;
 }
@@ -591,6 +612,72 @@ void eager_step(tdlb_batch_s* b, float alpha, float beta) {
     b->launches += queue_step(b, 0, true);
 }
 
+// Everything a captured step pair names on the host side: launch shapes,
+// work lists, device arrays, streams. A cached graph is replayed only while
+// its key is unchanged (the views, tables and rotors it reads are device
+// arrays rewritten before every run).
+std::vector<uintptr_t> graph_key(const tdlb_batch_s* b, int P) {
+    std::vector<uintptr_t> k = {(uintptr_t)P, b->tanks.size(), (uintptr_t)b->vec, (uintptr_t)b->threads,
+                                (uintptr_t)b->bps, (uintptr_t)b->d_steps, (uintptr_t)b->d_ibm,
+                                (uintptr_t)b->d_rotors, (uintptr_t)b->d_step};
+    for (const BatchGroup& G : b->grp) {
+        k.push_back(G.tanks.size());
+        k.push_back((uintptr_t)G.stream);
+        k.push_back((uintptr_t)G.side);
+        for (const WorkList* w : {&G.work, &G.rot_work, &G.cells, &G.tails, &G.copies, &G.small, &G.big}) {
+            k.push_back((uintptr_t)w->d);
+            k.push_back((uintptr_t)w->n);
+        }
+        k.push_back((uintptr_t)G.small_tile);
+        k.push_back((uintptr_t)G.big_tile);
+    }
+    return k;
+}
+
+// The instantiated graph of P step pairs for the current batch: the cached
+// one while its key holds, else a new capture (the old one is destroyed).
+cudaGraphExec_t graph_for(tdlb_batch_s* b, int P, int& kernels) {
+    tdlb_batch_s::CachedGraph& c = b->graphs[P == 1 ? 1 : 0];
+    std::vector<uintptr_t> key = graph_key(b, P);
+    if (c.ge && c.key == key) {
+        kernels = c.kernels;
+        return c.ge;
+    }
+    if (c.ge) {
+        cudaGraphExecDestroy(c.ge);
+        c.ge = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    int per_graph = 0;
+    TDLB_BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        split_streams(b);
+        for (int p = 0; p < P; p++) {
+            per_graph += queue_step(b, 0, p == 0);
+            per_graph += queue_step(b, 1, false);
+        }
+        merge_streams(b);
+    } catch (...) {
+        cudaStreamEndCapture(b->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    TDLB_BCK(cudaStreamEndCapture(b->stream, &g));
+    // the capture advanced the host state by 2P steps (the parity is back
+    // where it was); the replays run them
+    for (tdlb_lattice* h : b->tanks)
+        if (h->markers_set) h->pass -= 2 * P;
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    TDLB_BCK(ie);
+    c.ge = ge;
+    c.key = std::move(key);
+    c.kernels = per_graph;
+    kernels = per_graph;
+    return ge;
+}
+
 // `steps` steps, eager or graph-replayed. A step whose state still holds
 // moments (right after initialise) runs eagerly: its views differ from the
 // repeating pair's.
@@ -610,51 +697,26 @@ void run(tdlb_batch_s* b, int steps, float alpha, float beta, bool graph) {
         done++;
         any_moments = false;
     }
-    const int pairs = (steps - done) / 2;
+    int pairs = (steps - done) / 2;
     if (pairs > 0) {
-        const int P = std::min(pairs, kPairsPerGraph);
         merge_streams(b);
         upload_views(b, alpha, beta);
-        cudaGraph_t g = nullptr;
-        int per_graph = 0;
-        TDLB_BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        try {
-            split_streams(b);
-            for (int p = 0; p < P; p++) {
-                per_graph += queue_step(b, 0, p == 0);
-                per_graph += queue_step(b, 1, false);
-            }
-            merge_streams(b);
-        } catch (...) {
-            cudaStreamEndCapture(b->stream, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
+        // graphs of kPairsPerGraph pairs, then of one pair; both read the
+        // views just uploaded (an even number of steps ends on the parity it
+        // started from)
+        for (int P : {kPairsPerGraph, 1}) {
+            const int replays = pairs / P;
+            if (replays == 0) continue;
+            int kernels = 0;
+            const cudaGraphExec_t ge = graph_for(b, P, kernels);
+            for (int r = 0; r < replays; r++) TDLB_BCK(cudaGraphLaunch(ge, b->stream));
+            for (tdlb_lattice* h : b->tanks)
+                if (h->markers_set) h->pass += 2 * P * replays;
+            b->launches += (long long)kernels * replays;
+            done += 2 * P * replays;
+            pairs -= P * replays;
         }
-        TDLB_BCK(cudaStreamEndCapture(b->stream, &g));
-        cudaGraphExec_t ge = nullptr;
-        const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
-        cudaGraphDestroy(g);
-        TDLB_BCK(ie);
-        // the capture advanced the host state by 2P steps; the replays run them
-        for (tdlb_lattice* h : b->tanks)
-            if (h->markers_set) h->pass -= 2 * P;
-        const int replays = pairs / P;
-        for (int r = 0; r < replays; r++) {
-            const cudaError_t le = cudaGraphLaunch(ge, b->stream);
-            if (le != cudaSuccess) {
-                cudaGraphExecDestroy(ge);
-                TDLB_BCK(le);
-            }
-        }
-        cudaGraphExecDestroy(ge);
-        for (tdlb_lattice* h : b->tanks)
-            if (h->markers_set) h->pass += 2 * P * replays;
-        b->launches += (long long)per_graph * replays;
-        done += 2 * P * replays;
-        while (done < steps) {   // fewer than 2P steps left
-            eager_step(b, alpha, beta);
-            done++;
-        }
+        if (done < steps) eager_step(b, alpha, beta);   // an odd last step
     }
     merge_streams(b);
     finish_tables(b, steps);
@@ -666,7 +728,9 @@ void release(tdlb_batch_s* b) {
     cudaSetDevice(b->device);
     cudaDeviceSynchronize();
     for (tdlb_lattice* h : b->tanks) tdlb_destroy(h);
-    for (double* p : b->d_table) cudaFree(p);
+    for (auto& c : b->graphs)
+        if (c.ge) cudaGraphExecDestroy(c.ge);
+    cudaFree(b->d_tables);
     drop(b->work);
     for (BatchGroup& G : b->grp) {
         for (WorkList* w : {&G.work, &G.rot_work, &G.cells, &G.tails, &G.copies, &G.small, &G.big}) drop(*w);
