@@ -173,7 +173,8 @@ struct BatchGroup {
     int small_tile = 0, big_tile = 0;
     cudaStream_t stream = nullptr;     // group 0: the batch's stream
     cudaStream_t side = nullptr;       // large-plane spreads
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fused = nullptr;
+    cudaStream_t ibm = nullptr;        // the forcing pass (high priority, as `side`)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fused = nullptr, ev_ibm = nullptr;
 };
 
 struct tdlb_batch_s {
@@ -203,6 +204,7 @@ struct tdlb_batch_s {
     std::vector<unsigned> ibm_gen;     // marker generation the IBM lists were built for
     int vec = 1, threads = 128, bps = 0;   // fused-launch shape (bps 0: one block per work item)
     int sms = 0;                           // SMs of the device
+    int ibm_priority = 0;                  // the device's highest stream priority
     long long launches = 0;            // kernels run by tdlb_batch_run* so far
     std::string err = "no error";
 };
@@ -397,6 +399,10 @@ int queue_step(tdlb_batch_s* b, int k, bool first) {
         launch_fused(b, b->d_steps + (size_t)k * n, G.work, b->d_step + gi, G.stream);
         TDLB_BCK(cudaEventRecord(G.ev_fused, G.stream));
         kernels++;
+        // the forcing pass runs on a high-priority stream, so that its
+        // latency-bound blocks get SM slots ahead of the other group's fused
+        // launch; the group's next rotation waits for it
+        TDLB_BCK(cudaStreamWaitEvent(G.ibm, G.ev_fused, 0));
         tdlb::IbmBatch ib{};
         ib.args = b->d_ibm + (size_t)k * n;
         ib.cells = G.cells.d; ib.n_cells = G.cells.n;
@@ -407,8 +413,10 @@ int queue_step(tdlb_batch_s* b, int k, bool first) {
         ib.small_tile = G.small_tile;
         ib.big_tile = G.big_tile;
         ib.storage = storage_of(b);
-        TDLB_BCK(tdlb::launch_ibm_batch(ib, G.stream, G.side, G.ev_fork, G.ev_join));
+        TDLB_BCK(tdlb::launch_ibm_batch(ib, G.ibm, G.side, G.ev_fork, G.ev_join));
         kernels += (ib.n_cells > 0) + (ib.n_tails > 0) + (ib.n_copies > 0) + (ib.n_small > 0) + (ib.n_big > 0);
+        TDLB_BCK(cudaEventRecord(G.ev_ibm, G.ibm));
+        TDLB_BCK(cudaStreamWaitEvent(G.stream, G.ev_ibm, 0));
     }
     for (tdlb_lattice* h : b->tanks) {
         advance_step_state(h);
@@ -634,6 +642,31 @@ std::vector<uintptr_t> graph_key(const tdlb_batch_s* b, int P) {
     return k;
 }
 
+// Sets the launch priority of every kernel node of g except those of `keep`.
+cudaError_t prioritise_nodes(cudaGraph_t g, const void* keep, int priority) {
+    size_t n = 0;
+    cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
+    if (e != cudaSuccess) return e;
+    std::vector<cudaGraphNode_t> nodes(n);
+    e = cudaGraphGetNodes(g, nodes.data(), &n);
+    if (e != cudaSuccess) return e;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType type;
+        e = cudaGraphNodeGetType(nd, &type);
+        if (e != cudaSuccess) return e;
+        if (type != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp{};
+        e = cudaGraphKernelNodeGetParams(nd, &kp);
+        if (e != cudaSuccess) return e;
+        if (kp.func == keep) continue;
+        cudaLaunchAttributeValue v{};
+        v.priority = priority;
+        e = cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // The instantiated graph of P step pairs for the current batch: the cached
 // one while its key holds, else a new capture (the old one is destroyed).
 cudaGraphExec_t graph_for(tdlb_batch_s* b, int P, int& kernels) {
@@ -667,8 +700,12 @@ cudaGraphExec_t graph_for(tdlb_batch_s* b, int P, int& kernels) {
     // where it was); the replays run them
     for (tdlb_lattice* h : b->tanks)
         if (h->markers_set) h->pass -= 2 * P;
+    // every kernel but the fused launch (forcing passes, rotations) keeps the
+    // high priority of the streams it was captured from
+    cudaError_t pe = prioritise_nodes(g, (const void*)tdlb::batch_kernel(storage_of(b), eso_of(b), b->vec, b->threads),
+                                      b->ibm_priority);
     cudaGraphExec_t ge = nullptr;
-    const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    const cudaError_t ie = pe != cudaSuccess ? pe : cudaGraphInstantiateWithFlags(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     TDLB_BCK(ie);
     c.ge = ge;
@@ -737,7 +774,9 @@ void release(tdlb_batch_s* b) {
         if (G.ev_fork) cudaEventDestroy(G.ev_fork);
         if (G.ev_join) cudaEventDestroy(G.ev_join);
         if (G.ev_fused) cudaEventDestroy(G.ev_fused);
+        if (G.ev_ibm) cudaEventDestroy(G.ev_ibm);
         if (G.side) cudaStreamDestroy(G.side);
+        if (G.ibm) cudaStreamDestroy(G.ibm);
         if (G.stream && G.stream != b->stream) cudaStreamDestroy(G.stream);
     }
     cudaFree(b->d_steps);
@@ -753,6 +792,8 @@ void release(tdlb_batch_s* b) {
 void init_streams(tdlb_batch_s* b) {
     TDLB_BCK(cudaSetDevice(b->device));
     TDLB_BCK(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
+    int least = 0;
+    TDLB_BCK(cudaDeviceGetStreamPriorityRange(&least, &b->ibm_priority));
     TDLB_BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     TDLB_BCK(cudaEventCreateWithFlags(&b->ev_split, cudaEventDisableTiming));
     TDLB_BCK(cudaEventCreateWithFlags(&b->ev_merge, cudaEventDisableTiming));
@@ -760,10 +801,12 @@ void init_streams(tdlb_batch_s* b) {
         BatchGroup& G = b->grp[gi];
         if (gi == 0) G.stream = b->stream;
         else TDLB_BCK(cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking));
-        TDLB_BCK(cudaStreamCreateWithFlags(&G.side, cudaStreamNonBlocking));
+        TDLB_BCK(cudaStreamCreateWithPriority(&G.side, cudaStreamNonBlocking, b->ibm_priority));
+        TDLB_BCK(cudaStreamCreateWithPriority(&G.ibm, cudaStreamNonBlocking, b->ibm_priority));
         TDLB_BCK(cudaEventCreateWithFlags(&G.ev_fork, cudaEventDisableTiming));
         TDLB_BCK(cudaEventCreateWithFlags(&G.ev_join, cudaEventDisableTiming));
         TDLB_BCK(cudaEventCreateWithFlags(&G.ev_fused, cudaEventDisableTiming));
+        TDLB_BCK(cudaEventCreateWithFlags(&G.ev_ibm, cudaEventDisableTiming));
     }
     TDLB_BCK(cudaMalloc(&b->d_step, 2 * sizeof(int)));
 }

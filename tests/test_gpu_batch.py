@@ -100,6 +100,23 @@ def test_graph_replay_equals_eager(gpu, streaming):
 
 
 @pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_chunked_runs_equal_one_run(gpu, streaming):
+    """Runs of 10, 10, 3 and 10 steps (graphs captured by the first run and
+    replayed by the later ones, one-pair graphs and an odd last step) leave
+    every tank where one run of 33 steps does, bit for bit."""
+    tb = gpu
+    res = []
+    for chunks in ([10, 10, 3, 10], [33]):
+        with make_batch(tb, streaming, "fp32") as b:
+            for c in chunks:
+                b.run(c, ALPHA, BETA)
+            res.append([(cu.read_moments(), cu.read_force()) for cu in b.tanks])
+    for (m0, f0), (m1, f1) in zip(*res):
+        assert np.array_equal(m0, m1)
+        assert np.array_equal(f0, f1)
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
 def test_batch_shapes_agree(gpu, streaming):
     tb = gpu
     res = []
