@@ -402,6 +402,12 @@ int tdlb_batch_add(tdlb_batch b, const tdlb_config* cfg, int* index);
  * tdlb_batch_add's tank is set up on the batch's stream after it. No
  * counterpart in the reference, which runs one lattice per process. */
 int tdlb_batch_adopt(tdlb_batch b, tdlb_handle h, int* index);
+/* The inverse of tdlb_batch_adopt: tank `index` leaves the batch without
+ * being destroyed (after the batch's queued work), runs on its own stream
+ * again and belongs to the caller (tdlb_destroy). Later tanks move down by
+ * one. Lets a caller read a finished tank and free it while the batch runs
+ * on. No counterpart in the reference. */
+int tdlb_batch_detach(tdlb_batch b, int index, tdlb_handle* out);
 int tdlb_batch_remove(tdlb_batch b, int index);
 int tdlb_batch_tank(tdlb_batch b, int t, tdlb_handle* out);
 /* Shape of the fused batched launch: cells per thread (1, 2, 4; 16-bit
@@ -434,17 +440,19 @@ int tdlb_batch_synchronize(tdlb_batch b);
 int tdlb_batch_get_stream(tdlb_batch b, void** stream);
 
 /* ---- serving form: a request loop over resident, batched tanks ----
- * No counterpart in the reference. A server runs one worker thread that
+ * No counterpart in the reference. A server runs two threads. A helper
  * admits submitted requests in arrival order while a slot is free and the
  * tank's device bytes (tdlb_lattice_bytes) fit the free HBM (less 1 GiB)
- * and the budget; builds each admitted tank (a Rushton turbine filling the
- * lattice, tip speed and Re as requested, LES with Cs = 0.1, rho = 1) and
- * forces it once (main.cpp:305) on the tank's own stream, overlapping the
- * chunk that is running, then adopts it into the resident batch of its
- * precision and scheme (tdlb_batch_adopt); advances every resident tank in chunks of
- * min(chunk_steps, smallest remaining step count) with alpha = 0.97,
- * beta = 1.9; and retires finished tanks, freeing their memory. A tank's
- * result does not depend on what else is resident. */
+ * and the budget, and builds each admitted tank (a Rushton turbine filling
+ * the lattice, tip speed and Re as requested, LES with Cs = 0.1, rho = 1,
+ * forced once as main.cpp:305 does) on the tank's own stream while the
+ * resident tanks step. The worker adopts built tanks into the resident
+ * batch of their precision and scheme (tdlb_batch_adopt) between chunks,
+ * advances every resident tank in chunks of min(chunk_steps, smallest
+ * remaining step count) with alpha = 0.97, beta = 1.9, and detaches
+ * finished tanks (tdlb_batch_detach), which the helper reads out and frees
+ * while the next chunk runs. A tank's result does not depend on what else
+ * is resident. */
 typedef struct tdlb_server_s* tdlb_server;
 
 typedef struct tdlb_request {

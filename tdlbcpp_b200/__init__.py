@@ -226,6 +226,7 @@ def load_library() -> ctypes.CDLL:
         "tdlb_batch_tank": (i32, [H, i32, ctypes.POINTER(H)]),
         "tdlb_batch_add": (i32, [H, ctypes.POINTER(Config), ctypes.POINTER(i32)]),
         "tdlb_batch_adopt": (i32, [H, H, ctypes.POINTER(i32)]),
+        "tdlb_batch_detach": (i32, [H, i32, ctypes.POINTER(H)]),
         "tdlb_batch_remove": (i32, [H, i32]),
         "tdlb_batch_set_shape": (i32, [H, i32, i32, i32]),
         "tdlb_batch_get_shape": (i32, [H, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
@@ -631,6 +632,16 @@ class Batch:
         self._check(self.lib.tdlb_batch_adopt(self.h, cu.h, ctypes.byref(idx)))
         cu._owned = False
         self.tanks.append(cu)
+        return cu
+
+    def detach(self, index: int) -> "ComputeUnit":
+        """Tank `index` leaves the batch without being destroyed; the returned
+        ComputeUnit owns it again (closing it destroys the tank)."""
+        th = ctypes.c_void_p()
+        self._check(self.lib.tdlb_batch_detach(self.h, index, ctypes.byref(th)))
+        cu = self.tanks.pop(index)
+        cu.h = th
+        cu._owned = True
         return cu
 
     def remove(self, index: int):

@@ -594,6 +594,21 @@ void adopt_tank(tdlb_batch_s* b, tdlb_lattice* h) {
     b->members_changed = true;
 }
 
+// The inverse of adopt_tank: tank t leaves the batch without being
+// destroyed, once the batch's streams are idle, and runs on its own stream
+// again; the caller owns it. Later tanks move down by one.
+tdlb_lattice* detach_tank(tdlb_batch_s* b, int t) {
+    if (t < 0 || t >= (int)b->tanks.size()) throw BFail{TDLB_EINVAL, "tank index out of range"};
+    TDLB_BCK(quiesce(b));
+    tdlb_lattice* h = b->tanks[(size_t)t];
+    tdlb_rt::return_stream(h);
+    h->vec = 1;
+    b->tanks.erase(b->tanks.begin() + t);
+    b->ibm_gen.erase(b->ibm_gen.begin() + t);
+    b->members_changed = true;
+    return h;
+}
+
 void remove_tank(tdlb_batch_s* b, int t) {
     if (t < 0 || t >= (int)b->tanks.size()) throw BFail{TDLB_EINVAL, "tank index out of range"};
     TDLB_BCK(cudaStreamSynchronize(b->stream));
@@ -876,6 +891,13 @@ int tdlb_batch_adopt(tdlb_batch b, tdlb_handle h, int* index) {
     return bguard(b, [&] {
         adopt_tank(b, h);
         if (index) *index = (int)b->tanks.size() - 1;
+    });
+}
+
+int tdlb_batch_detach(tdlb_batch b, int index, tdlb_handle* out) {
+    return bguard(b, [&] {
+        if (!out) throw BFail{TDLB_EINVAL, "out is NULL"};
+        *out = detach_tank(b, index);
     });
 }
 

@@ -1,24 +1,26 @@
 // Serving form: a request loop over resident, continuously batched tanks.
 //
 // Callers submit tank-solve requests (tank size, impeller tip speed,
-// Reynolds number, step count, storage precision) from any thread. One
-// worker thread owns the GPU work:
-//   * admission -- requests are taken in arrival order while a slot is free
-//     and the tank's device bytes (tdlb_lattice_bytes) fit both the free HBM
-//     (less a reserve) and the server's budget; an admitted tank is built,
-//     gets its Rushton turbine, is initialised and forced once
-//     (main.cpp:305), and joins the resident batch of its precision and
-//     streaming scheme;
-//   * stepping -- all resident tanks advance together in chunks: every
-//     batch runs the same number of steps (the smallest remaining count,
-//     capped by chunk_steps) through tdlb_batch_run, the batches of different
-//     precisions on their own streams at the same time;
-//   * retirement -- a finished tank's FP64 diagnostics (mass, momentum,
-//     impeller force and torque, power number) and, if asked, its density
-//     and velocity fields are copied out, it leaves its batch and its memory
-//     is freed, so a waiting request can be admitted at the next chunk.
-// Requests that arrive while others run are admitted at the next chunk
-// boundary, so their work overlaps with the tanks already on the GPU.
+// Reynolds number, step count, storage precision) from any thread. Two
+// server threads share the GPU work:
+//   * admission (helper thread) -- requests are taken in arrival order while
+//     a slot is free and the tank's device bytes (tdlb_lattice_bytes) fit
+//     both the free HBM (less a reserve) and the server's budget; an
+//     admitted tank is built on its own stream, gets its Rushton turbine, is
+//     initialised and forced once (main.cpp:305), all while the resident
+//     tanks keep stepping;
+//   * stepping (worker thread) -- between two chunks the built tanks join
+//     the resident batch of their precision and streaming scheme
+//     (tdlb_batch_adopt); all resident tanks advance together in chunks:
+//     every batch runs the same number of steps (the smallest remaining
+//     count, capped by chunk_steps) through tdlb_batch_run, the batches of
+//     different precisions on their own streams at the same time;
+//   * retirement -- a finished tank leaves its batch (tdlb_batch_detach) and
+//     the helper copies out its FP64 diagnostics (mass, momentum, impeller
+//     force and torque, power number) and, if asked, its density and
+//     velocity fields, and frees its memory, while the next chunk runs.
+// Requests that arrive while others run join at a chunk boundary, so their
+// work overlaps with the tanks already on the GPU.
 // A tank's arithmetic does not depend on its batch neighbours: its result
 // equals the same request run alone.
 #include "tdlb_b200.h"
@@ -76,7 +78,13 @@ struct tdlb_server_s {
     std::string err = "no error";
     long long submitted = 0, completed = 0;
 
-    // worker-owned
+    // shared with the helper thread (under mu)
+    std::thread helper;
+    std::vector<Active> ready;      // built tanks waiting to join a batch (own streams)
+    std::vector<Active> finished;   // finished tanks detached from their batches
+    int holding = 0;                // tanks holding device memory: building, ready, resident, finished
+
+    // stepping-thread-owned
     std::thread worker;
     std::map<int, tdlb_batch> batches;   // key: storage * 2 + streaming
     std::vector<Active> active;
@@ -174,42 +182,71 @@ int index_in(tdlb_batch b, tdlb_handle h) {
     return -1;
 }
 
-// Build, initialise and force a request's tank; false (result pushed) on failure.
-bool admit_one(tdlb_server_s* s, const Pending& p, long long need) {
+// ---------------------------------------------------------------------------
+// Helper thread: admission and retirement, off the stepping thread, so that
+// building a tank (allocation, geometry, marker schedule: about 0.1 s for a
+// 256^3 tank) and freeing one never leave the GPU idle between chunks.
+// ---------------------------------------------------------------------------
+
+// Takes the next request if a slot is free and its bytes fit: 1 taken (slot
+// and bytes reserved), 0 nothing to take now, 2 the request failed (result
+// pushed).
+int take_request(tdlb_server_s* s, Pending& p, long long& need) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->queue.empty() || s->stop) return 0;
+    if (s->holding >= s->max_active) return 0;
+    p = s->queue.front();
+    need = need_of(p.req);
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    long long avail = (long long)free_b - s->reserve;
+    if (s->budget > 0) avail = std::min(avail, s->budget - s->bytes_in_use);
+    if (need >= 0 && need <= avail) {
+        s->queue.pop_front();
+        s->holding++;
+        s->bytes_in_use += need;
+        return 1;
+    }
+    if (s->holding > 0 && need >= 0) return 0;   // wait for memory to free up
+    s->queue.pop_front();
+    s->done.push_back(failed(p.req, need < 0 ? TDLB_EINVAL : TDLB_ENOMEM, p.t_submit, s->now()));
+    s->completed++;
+    s->idle_cv.notify_all();
+    return 2;
+}
+
+// Gives back a slot and its bytes.
+void release_slot(tdlb_server_s* s, long long bytes) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->holding--;
+    s->bytes_in_use -= bytes;
+    s->cv.notify_all();
+}
+
+// Builds a taken request's tank on its own stream: created, impeller
+// attached, initialised and forced once (main.cpp:305), then handed to the
+// stepping thread, which adopts it into its batch between two chunks.
+void build(tdlb_server_s* s, const Pending& p, long long need) {
     const tdlb_request& r = p.req;
     const tdlb_rushton spec = spec_of(r);
     const int radius = tdlb_rushton_blade_outer_radius(&spec);
     const tdlb_config c = config_of(r, radius < 1 ? 1 : radius);
-    tdlb_batch b = batch_for(s, r);
-    if (!b) {
-        push_result(s, failed(r, TDLB_ECUDA, p.t_submit, s->now()));
-        return false;
-    }
-    // The tank is set up on its own stream, so this overlaps a running chunk;
-    // adopting it drains that stream and moves it onto the batch's.
     tdlb_handle h = nullptr;
     int rc = tdlb_create_config(&c, s->device, &h);
     const double d1 = tdlb_rushton_impeller_increment(&spec, 1);
     if (rc == TDLB_OK) rc = tdlb_attach_rushton(h, &spec, d1, d1, d1);
     if (rc == TDLB_OK) rc = tdlb_initialise(h, 1.0f);
     if (rc == TDLB_OK) rc = tdlb_forcing_resident(h, s->alpha, s->beta);
+    if (rc == TDLB_OK) rc = tdlb_synchronize(h);
     if (rc != TDLB_OK) {
         note(s, std::string("tank setup: ") + tdlb_last_error(h));
         if (h) tdlb_destroy(h);
+        release_slot(s, need);
         push_result(s, failed(r, rc, p.t_submit, s->now()));
-        return false;
-    }
-    int idx = -1;
-    rc = tdlb_batch_adopt(b, h, &idx);
-    if (rc != TDLB_OK) {
-        note(s, std::string("admission: ") + tdlb_batch_last_error(b));
-        tdlb_destroy(h);
-        push_result(s, failed(r, rc, p.t_submit, s->now()));
-        return false;
+        return;
     }
     Active a{};
     a.req = r;
-    a.batch = b;
     a.h = h;
     a.remaining = r.steps;
     a.t_submit = p.t_submit;
@@ -219,43 +256,14 @@ bool admit_one(tdlb_server_s* s, const Pending& p, long long need) {
     a.D = G.D;
     a.omega = G.increment(1000000000ULL);
     std::lock_guard<std::mutex> lk(s->mu);
-    s->active.push_back(a);
-    s->bytes_in_use += need;
+    s->ready.push_back(a);
     s->admitted++;
-    return true;
+    s->cv.notify_all();
 }
 
-void admit(tdlb_server_s* s) {
-    for (;;) {
-        Pending p;
-        long long need = 0;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            if (s->queue.empty() || s->stop) return;
-            if ((int)s->active.size() >= s->max_active) return;
-            p = s->queue.front();
-            need = need_of(p.req);
-            size_t free_b = 0, total_b = 0;
-            cudaMemGetInfo(&free_b, &total_b);
-            long long avail = (long long)free_b - s->reserve;
-            if (s->budget > 0) avail = std::min(avail, s->budget - s->bytes_in_use);
-            if (need < 0 || need > avail) {
-                if (!s->active.empty() && need >= 0) return;   // wait for memory to free up
-                s->queue.pop_front();
-                tdlb_result res = failed(p.req, need < 0 ? TDLB_EINVAL : TDLB_ENOMEM, p.t_submit, s->now());
-                s->done.push_back(res);
-                s->completed++;
-                s->idle_cv.notify_all();
-                continue;
-            }
-            s->queue.pop_front();
-        }
-        admit_one(s, p, need);
-    }
-}
-
-void retire(tdlb_server_s* s, size_t k) {
-    Active& a = s->active[k];
+// A finished tank, detached from its batch and on its own stream again: its
+// FP64 diagnostics and optional fields are read, its memory freed.
+void retire(tdlb_server_s* s, Active& a) {
     tdlb_result res{};
     res.id = a.req.id;
     res.t_submit = a.t_submit;
@@ -279,14 +287,75 @@ void retire(tdlb_server_s* s, size_t k) {
     // power number P / (rho N^3 D^5), P = torque * omega, N = omega / (2 pi)
     const double N = a.omega / (2.0 * M_PI);
     res.power_number = N > 0 ? std::fabs(res.torque * a.omega) / (N * N * N * std::pow(a.D, 5)) : 0.0;
-    const int idx = index_in(a.batch, a.h);
-    if (idx >= 0) tdlb_batch_remove(a.batch, idx);
+    tdlb_destroy(a.h);
+    a.h = nullptr;
+    release_slot(s, a.bytes);
     res.t_done = s->now();
+    push_result(s, res);
+}
+
+void helper_loop(tdlb_server_s* s) {
+    cudaSetDevice(s->device);
+    for (;;) {
+        std::vector<Active> fin;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            fin.swap(s->finished);
+        }
+        for (Active& a : fin) retire(s, a);
+        Pending p;
+        long long need = 0;
+        const int took = take_request(s, p, need);
+        if (took == 1) build(s, p, need);
+        if (took != 0 || !fin.empty()) continue;
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (s->stop && s->finished.empty()) break;
+        // wake for finished tanks, new requests or freed slots
+        const long long sub0 = s->submitted;
+        const int hold0 = s->holding;
+        s->cv.wait_for(lk, std::chrono::milliseconds(20), [&] {
+            return s->stop || !s->finished.empty() || s->submitted != sub0 || s->holding != hold0;
+        });
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stepping thread.
+// ---------------------------------------------------------------------------
+
+// Tanks the helper has built join the batch of their precision and scheme.
+void adopt_ready(tdlb_server_s* s) {
+    std::vector<Active> rd;
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        s->bytes_in_use -= a.bytes;
-        s->active.erase(s->active.begin() + (long)k);
+        rd.swap(s->ready);
     }
+    for (Active& a : rd) {
+        tdlb_batch b = batch_for(s, a.req);
+        int idx = -1;
+        const int rc = b ? tdlb_batch_adopt(b, a.h, &idx) : TDLB_ECUDA;
+        if (rc != TDLB_OK) {
+            note(s, std::string("admission: ") + (b ? tdlb_batch_last_error(b) : "no batch"));
+            tdlb_destroy(a.h);
+            release_slot(s, a.bytes);
+            push_result(s, failed(a.req, rc, a.t_submit, s->now()));
+            continue;
+        }
+        a.batch = b;
+        s->active.push_back(a);
+    }
+}
+
+// A resident tank that will not finish: it leaves its batch (destroyed)
+// with `code` as its result.
+void drop_active(tdlb_server_s* s, size_t k, int code) {
+    Active& a = s->active[k];
+    tdlb_result res = failed(a.req, code, a.t_submit, s->now());
+    res.t_admit = a.t_admit;
+    const int idx = index_in(a.batch, a.h);
+    if (idx >= 0) tdlb_batch_remove(a.batch, idx);
+    release_slot(s, a.bytes);
+    s->active.erase(s->active.begin() + (long)k);
     push_result(s, res);
 }
 
@@ -304,83 +373,63 @@ void step_chunk(tdlb_server_s* s) {
             if (rc != TDLB_OK) why = tdlb_batch_last_error(kv.second);
         }
     }
-    // Requests admitted now are set up while the chunk runs; they join the
-    // next chunk.
-    const size_t running = s->active.size();
-    if (rc == TDLB_OK) admit(s);
     for (auto& kv : s->batches)
         if (tdlb_batch_synchronize(kv.second) != TDLB_OK && rc == TDLB_OK) {
             rc = TDLB_ECUDA;
             why = tdlb_batch_last_error(kv.second);
         }
-    if (rc != TDLB_OK) {
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->err = "chunk failed: " + why;
-    }
     {
         std::lock_guard<std::mutex> lk(s->mu);
+        if (rc != TDLB_OK) s->err = "chunk failed: " + why;
         s->busy_s += s->now() - t;
         s->chunks++;
     }
     if (rc != TDLB_OK) {   // every resident tank fails with the error
-        for (size_t k = s->active.size(); k-- > 0;) {
-            Active& a = s->active[k];
-            tdlb_result res = failed(a.req, rc, a.t_submit, s->now());
-            res.t_admit = a.t_admit;
-            const int idx = index_in(a.batch, a.h);
-            if (idx >= 0) tdlb_batch_remove(a.batch, idx);
-            {
-                std::lock_guard<std::mutex> lk(s->mu);
-                s->bytes_in_use -= a.bytes;
-                s->active.erase(s->active.begin() + (long)k);
-            }
-            push_result(s, res);
-        }
+        for (size_t k = s->active.size(); k-- > 0;) drop_active(s, k, rc);
         return;
     }
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        for (size_t k = 0; k < running; k++) {
-            Active& a = s->active[k];
+        for (Active& a : s->active) {
             a.remaining -= chunk;
             s->lattice_updates += (double)a.req.x * a.req.y * a.req.z * (double)chunk;
         }
     }
-    for (size_t k = running; k-- > 0;)
-        if (s->active[k].remaining <= 0) retire(s, k);
+    // finished tanks leave their batches (not destroyed) and go to the
+    // helper, which reads and frees them while the next chunk runs
+    for (size_t k = s->active.size(); k-- > 0;) {
+        Active& a = s->active[k];
+        if (a.remaining > 0) continue;
+        const int idx = index_in(a.batch, a.h);
+        tdlb_handle h = nullptr;
+        if (idx < 0 || tdlb_batch_detach(a.batch, idx, &h) != TDLB_OK) {
+            drop_active(s, k, TDLB_ECUDA);
+            continue;
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->finished.push_back(a);
+        s->active.erase(s->active.begin() + (long)k);
+        s->cv.notify_all();
+    }
 }
 
 void loop(tdlb_server_s* s) {
     cudaSetDevice(s->device);
     for (;;) {
-        admit(s);
+        adopt_ready(s);
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->n_active_snapshot = (int)s->active.size();
             if (s->stop) break;
             if (s->active.empty()) {
-                s->cv.wait_for(lk, std::chrono::milliseconds(20), [&] { return s->stop || !s->queue.empty(); });
+                s->cv.wait_for(lk, std::chrono::milliseconds(20), [&] { return s->stop || !s->ready.empty(); });
                 continue;
             }
         }
         step_chunk(s);
     }
-    // stopping: resident and queued requests end unfinished
-    for (size_t k = s->active.size(); k-- > 0;) {
-        Active& a = s->active[k];
-        tdlb_result res = failed(a.req, TDLB_ESTATE, a.t_submit, s->now());
-        const int idx = index_in(a.batch, a.h);
-        if (idx >= 0) tdlb_batch_remove(a.batch, idx);
-        s->active.erase(s->active.begin() + (long)k);
-        push_result(s, res);
-    }
-    std::lock_guard<std::mutex> lk(s->mu);
-    while (!s->queue.empty()) {
-        s->done.push_back(failed(s->queue.front().req, TDLB_ESTATE, s->queue.front().t_submit, s->now()));
-        s->completed++;
-        s->queue.pop_front();
-    }
-    s->idle_cv.notify_all();
+    // stopping: resident tanks end unfinished
+    for (size_t k = s->active.size(); k-- > 0;) drop_active(s, k, TDLB_ESTATE);
 }
 
 thread_local std::string g_server_error = "no error";
@@ -412,8 +461,15 @@ int tdlb_server_create(int device, int64_t hbm_budget_bytes, int max_active, int
     s->t0 = Clock::now();
     try {
         s->worker = std::thread(loop, s);
+        s->helper = std::thread(helper_loop, s);
     } catch (const std::exception& e) {
         g_server_error = e.what();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stop = true;
+            s->cv.notify_all();
+        }
+        if (s->worker.joinable()) s->worker.join();
         delete s;
         return TDLB_EINVAL;
     }
@@ -493,7 +549,19 @@ int tdlb_server_destroy(tdlb_server s) {
         s->cv.notify_all();
     }
     if (s->worker.joinable()) s->worker.join();
+    if (s->helper.joinable()) s->helper.join();
     cudaSetDevice(s->device);
+    // what the threads left: finished tanks are read out, built ones and
+    // queued requests end unfinished
+    for (Active& a : s->finished) retire(s, a);
+    for (Active& a : s->ready) {
+        tdlb_destroy(a.h);
+        push_result(s, failed(a.req, TDLB_ESTATE, a.t_submit, s->now()));
+    }
+    while (!s->queue.empty()) {
+        push_result(s, failed(s->queue.front().req, TDLB_ESTATE, s->queue.front().t_submit, s->now()));
+        s->queue.pop_front();
+    }
     for (auto& kv : s->batches) tdlb_batch_destroy(kv.second);
     delete s;
     return TDLB_OK;

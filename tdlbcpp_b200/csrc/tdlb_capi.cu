@@ -1261,6 +1261,12 @@ void borrow_stream(tdlb_lattice* h, cudaStream_t s) {
     h->stream = s;
 }
 
+void return_stream(tdlb_lattice* h) {
+    if (!h->own_stream) return;
+    h->stream = h->own_stream;
+    h->own_stream = nullptr;
+}
+
 cudaError_t join_side(tdlb_lattice* h) {
     if (!h->pending) return cudaSuccess;
     cudaError_t e = cudaEventRecord(h->ev_sync, h->ibm);

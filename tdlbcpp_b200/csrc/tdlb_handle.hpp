@@ -146,6 +146,8 @@ tdlb::StepArgs step_args(tdlb_lattice* h, bool collide);
 tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta);
 // Queue h's work on `s` instead of its own stream (batches share one).
 void borrow_stream(tdlb_lattice* h, cudaStream_t s);
+// Undo borrow_stream: h's work goes to its own stream again.
+void return_stream(tdlb_lattice* h);
 // Make `stream` wait for the forcing pass and inner launches queued on the
 // split-step stream (every entry point other than the step loop calls it).
 cudaError_t join_side(tdlb_lattice* h);

@@ -171,6 +171,37 @@ def test_adopted_tank_matches_tank_alone(gpu, streaming):
     assert rel_l2(F, F0) <= 1e-5
 
 
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_detached_tank_continues_alone(gpu, streaming):
+    """A tank detached from a batch after 5 steps (the serving form's
+    retirement) keeps its state, continues through the single-lattice entry
+    points for 2 more steps and ends where 7 steps alone end; the batch
+    carries on with the other tanks."""
+    tb = gpu
+    spec = TANKS[1]
+    with make_batch(tb, streaming, "fp32", TANKS[:3]) as b:
+        b.run(5, ALPHA, BETA)
+        cu = b.detach(1)
+        assert len(b) == 2
+        b.run(3, ALPHA, BETA)
+        rt, _ = tank_config(tb, spec, streaming, "fp32")
+        angle = rt.increment(1)
+        for s in range(2, 7):
+            angle += rt.increment(s)
+        for s in range(7, 9):
+            d = rt.increment(s)
+            angle += d
+            cu.rotate_impeller(angle, d)
+            cu.collision()
+            cu.forcing_resident(ALPHA, BETA)
+        (rho, u), F = cu.read_velocity_density(), cu.read_force()
+        cu.close()                    # owned again: destroys the tank
+    (rho0, u0), F0, _ = run_alone(tb, spec, streaming, "fp32", 7)
+    assert rel_l2(u, u0) <= 1e-6
+    assert rel_l2(rho, rho0) <= 1e-6
+    assert rel_l2(F, F0) <= 1e-5
+
+
 def test_batch_rejects_mixed_schemes(gpu):
     tb = gpu
     cfgs = [dict(x=8, y=8, z=8, nu=1e-3), dict(x=8, y=8, z=8, nu=1e-3, streaming="Esotwist")]
