@@ -204,12 +204,13 @@ def run_ours(args, rank, world, device):
     # them (tdlb_set_rotating_markers), the step runs, and its FP64 impeller
     # load comes back to pinned host memory. The host prepares step s+1's
     # blades while the device runs step s (their upload is queued after the
-    # load of step s, which still needs step s's blades).
+    # load of step s, which still needs step s's blades) and reads step s's
+    # load after queueing step s+1, so the device never waits for the host.
     pinned = torch.empty(n_rot * tb.MARKER_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
     host_rot = np.frombuffer(pinned.numpy(), dtype=tb.MARKER_DTYPE)
-    load = torch.empty(5, dtype=torch.float64, pin_memory=True)
+    load = torch.empty((2, 5), dtype=torch.float64, pin_memory=True)   # steps alternate between the rows
     load_np = load.numpy()
-    got = torch.cuda.Event()
+    got = [torch.cuda.Event(), torch.cuda.Event()]
     spec = rt.spec
     k_e2e = max(3, args.steps // 5)
     loads = []
@@ -223,16 +224,23 @@ def run_ours(args, rank, world, device):
         cu.set_rotating_markers(host_rot)
 
     def e2e_steps(k):
+        # the device always has the next step queued: step s is queued, the
+        # host prepares step s+1's blades, and only then waits for the load
+        # of step s-1 (two pinned rows, so no step's copy overwrites a load
+        # the host has not read)
         upload_next()
         for s in range(k):
             cu.collision()
             cu.forcing_resident(ALPHA, BETA)
-            cu.impeller_load_async(load.data_ptr())
-            got.record(stream)
+            cu.impeller_load_async(load[s % 2].data_ptr())
+            got[s % 2].record(stream)
             if s + 1 < k:
                 upload_next()
-            got.synchronize()
-            loads.append(load_np.copy())
+            if s >= 1:
+                got[(s - 1) % 2].synchronize()
+                loads.append(load_np[(s - 1) % 2].copy())
+        got[(k - 1) % 2].synchronize()
+        loads.append(load_np[(k - 1) % 2].copy())
 
     e2e_steps(2)
     barrier(world)

@@ -535,12 +535,28 @@ __global__ void __launch_bounds__(256) k_marker_load(IbmArgs a, int begin, doubl
         for (int c = 0; c < 5; c++) partial[blockIdx.x * 5 + c] = red[c][0];
 }
 
-__global__ void k_marker_load_final(const double* partial, int nblocks, double* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double acc[5] = {0, 0, 0, 0, 0};
+// Ordered sum of the block partials: the warp stages them in shared memory
+// (coalesced, all loads in flight at once), then one thread adds them in
+// block order, so the result does not depend on the launch.
+template <int NC, int NB>
+__device__ __forceinline__ void ordered_final(const double* __restrict__ partial, int nblocks, double* out) {
+    __shared__ double v[NB * NC];
+    const int n = nblocks * NC;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) v[q] = partial[q];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] = 0.0;
     for (int b = 0; b < nblocks; b++)
-        for (int c = 0; c < 5; c++) acc[c] += partial[b * 5 + c];
-    for (int c = 0; c < 5; c++) out[c] = acc[c];
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] += v[b * NC + c];
+#pragma unroll
+    for (int c = 0; c < NC; c++) out[c] = acc[c];
+}
+
+__global__ void k_marker_load_final(const double* partial, int nblocks, double* out) {
+    ordered_final<5, kLoadBlocks>(partial, nblocks, out);
 }
 
 cudaError_t launch_marker_load(const IbmArgs& a, int begin, double ci, double ck, double* partial, double* out,
@@ -585,11 +601,7 @@ __global__ void __launch_bounds__(256) k_reduce_fp64(IbmArgs a, const uint32_t* 
 }
 
 __global__ void k_reduce_fp64_final(const double* partial, int nblocks, double* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double acc[4] = {0, 0, 0, 0};
-    for (int b = 0; b < nblocks; b++)
-        for (int c = 0; c < 4; c++) acc[c] += partial[b * 4 + c];
-    for (int c = 0; c < 4; c++) out[c] = acc[c];
+    ordered_final<4, kReduceBlocks>(partial, nblocks, out);
 }
 
 cudaError_t launch_reduce_fp64(const IbmArgs& a, const uint32_t* mask, double* partial, double* out, cudaStream_t st) {
