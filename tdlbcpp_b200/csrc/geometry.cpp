@@ -126,25 +126,56 @@ double RushtonGeom::increment(unsigned long long step) const {
 }
 
 std::vector<tdlb_marker> RushtonGeom::fixed() const {
-    std::vector<P> v;
-    for (long long j = 0; j < y; j++) ring(*this, R_wall, j, 0.0, v);
+    // The wall ring and the baffle points are the same in every plane: they
+    // are computed once, grouped by colour, and emitted colour by colour --
+    // the wall in (plane, ring position) order, then the baffles in
+    // (baffle, plane, radius) order, which is the order a stable sort by
+    // colour of the plane-by-plane list gives.
+    std::vector<P> wall;
+    ring(*this, R_wall, 0, 0.0, wall);
+    std::vector<std::vector<P>> baffle((size_t)std::max(n_baffles, 0));
     for (int b = 0; b < n_baffles; b++) {
         const double phi = M_PI / 4.0 + 2.0 * M_PI * b / n_baffles;
-        for (long long j = 0; j < y; j++)
-            for (double r = R_wall - 1.0; r >= R_wall - baffle_w - 1e-9; r -= 1.0) {
-                P p;
-                p.r = r; p.theta = phi;
-                p.pi = ci + r * std::cos(phi);
-                p.pk = ck + r * std::sin(phi);
-                p.j = j;
-                p.seq = (long long)v.size();
-                v.push_back(p);
-            }
+        for (double r = R_wall - 1.0; r >= R_wall - baffle_w - 1e-9; r -= 1.0) {
+            P p;
+            p.r = r; p.theta = phi;
+            p.pi = ci + r * std::cos(phi);
+            p.pk = ck + r * std::sin(phi);
+            p.j = 0;
+            p.seq = 0;
+            baffle[(size_t)b].push_back(p);
+        }
     }
-    color_by_cell(v);
+    auto colour = [](const P& p) {
+        const long long i = (long long)std::floor(p.pi + 0.5), k = (long long)std::floor(p.pk + 0.5);
+        return (int)(((i % 3) + 3) % 3 * 3 + ((k % 3) + 3) % 3);
+    };
+    size_t per_plane = wall.size();
+    for (const auto& bv : baffle) per_plane += bv.size();
     std::vector<tdlb_marker> out;
-    out.reserve(v.size());
-    for (const auto& p : v) out.push_back(to_marker(*this, p, 0.0));
+    out.reserve(per_plane * (size_t)std::max<long long>(y, 0));
+    for (int c = 0; c < 9; c++) {
+        std::vector<const P*> w;
+        for (const P& p : wall)
+            if (colour(p) == c) w.push_back(&p);
+        for (long long j = 0; j < y; j++)
+            for (const P* p : w) {
+                P q = *p;
+                q.j = j;
+                out.push_back(to_marker(*this, q, 0.0));
+            }
+        for (const auto& bv : baffle) {
+            std::vector<const P*> bb;
+            for (const P& p : bv)
+                if (colour(p) == c) bb.push_back(&p);
+            for (long long j = 0; j < y; j++)
+                for (const P* p : bb) {
+                    P q = *p;
+                    q.j = j;
+                    out.push_back(to_marker(*this, q, 0.0));
+                }
+        }
+    }
     return out;
 }
 
