@@ -118,6 +118,26 @@ def test_rushton_geometry_in_range_and_classes(tdlb, edge):
     assert rt.increment(25) == pytest.approx(full * 0.5)
 
 
+# SHA-256 prefixes of the generated marker lists (fixed, rotating-non-updating,
+# rotating at angle 0.7): the oracle and the GPU take the same list, and the
+# list order sets the level schedule, so a faster generator must give these
+# bytes exactly.
+GEOMETRY_PINS = {
+    (48, 48, 48): (7392, 443, 150, "76d4ffcc758a2111", "a2c76de5feec425a", "29c4b35af3ec1c5f"),
+    (61, 50, 47): (10150, 554, 180, "9be4de741eb34b70", "659e487721025ada", "7d4d155a98f65973"),
+}
+
+
+@pytest.mark.parametrize("dims", sorted(GEOMETRY_PINS))
+def test_rushton_geometry_bytes_pinned(tdlb, dims):
+    import hashlib
+    rt = tdlb.RushtonTurbine(*dims, tip_speed=0.1, startup_steps=0)
+    lists = (rt.fixed(), rt.rotating_nonupdating(rt.increment(1)), rt.rotating(0.7, rt.increment(1)))
+    pin = GEOMETRY_PINS[dims]
+    assert tuple(len(m) for m in lists) == pin[:3]
+    assert tuple(hashlib.sha256(m.tobytes()).hexdigest()[:16] for m in lists) == pin[3:]
+
+
 def _stencil(m, x, z):
     cells = []
     for k1 in (-1, 0, 1):
