@@ -184,7 +184,7 @@ int index_in(tdlb_batch b, tdlb_handle h) {
 
 // ---------------------------------------------------------------------------
 // Helper thread: admission and retirement, off the stepping thread, so that
-// building a tank (allocation, geometry, marker schedule: about 0.1 s for a
+// building a tank (allocation, geometry, marker schedule: tens of ms for a
 // 256^3 tank) and freeing one never leave the GPU idle between chunks.
 // ---------------------------------------------------------------------------
 
