@@ -1,21 +1,29 @@
 // Batched form: many independent tanks of uneven sizes on one GPU.
 //
-// One batched step is seven launches whatever the number of tanks:
+// The tanks are split into two groups of about equal cell count, each with
+// its own stream. One batched step is, per group, a fixed set of launches
+// whatever the number of tanks:
 //   1. k_rotate_batch   every attached impeller's blades at the step's angle,
 //                       read from a per-step (cos, sin, delta) table indexed
 //                       by a device step counter;
-//   2. k_batch_step     all tanks' fused collision + streaming: a persistent
-//                       grid of a few blocks per SM loops over work items,
-//                       each 128 or 256 consecutive quads of one tank, with
-//                       that tank's step view staged in shared memory (block
-//                       0 also advances the step counter);
-//   3-7. the immersed-boundary passes of all tanks (launch_ibm_batch): cells,
+//   2. k_batch_step     the group's fused collision + streaming: work items
+//                       of eight chunks of 128 or 256 quads of one tank, with
+//                       that tank's step view staged in shared memory once
+//                       per item; one block per item or a persistent grid of
+//                       a few blocks per SM looping over the items (block 0
+//                       also advances the step counter);
+//   3-7. the immersed-boundary passes of the group's tanks
+//                       (launch_ibm_batch) on a high-priority stream: cells,
 //                       blade gathers, touched-flag copies, small-plane and
-//                       large-plane spreads, each one launch over all tanks.
-// Two consecutive steps (one A/B and parity cycle) are captured into a CUDA
-// graph and replayed. The fused launch's shape -- cells per thread, threads
-// per block, resident blocks per SM -- is chosen by an autotuner that times
-// every candidate on the batch itself.
+//                       large-plane spreads, each one launch over the group.
+// The groups' fused launches take turns, so each group's forcing pass runs
+// while the other group's fused launch streams through HBM. Four step pairs
+// (A/B and parity cycles), and single pairs for the rest of a run, are
+// captured into CUDA graphs that stay instantiated between runs while the
+// batch's launch shapes, work lists and device arrays are unchanged. The
+// fused launch's shape -- cells per thread, threads per block, blocks per SM
+// or one block per item -- is chosen by an autotuner that times every
+// candidate on the batch itself.
 #include "tdlb_handle.hpp"
 #include "tdlb_geometry.hpp"
 #include "tdlb_rotate.hpp"
