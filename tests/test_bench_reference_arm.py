@@ -1,0 +1,30 @@
+"""bench.py's reference arm on the CPU: the reference's own step (the
+compiled oracle/_ref library) timed on the host cores prints one JSON line
+with the keys and meanings the main arm's line has, plus impl, cpu_baseline
+and an e2e figure that moves no bytes between host and device."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_one_contract_line(ref_oracle):
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                          "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600, check=True)
+    lines = [ln for ln in out.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config"):
+        assert key in d, key
+    assert d["impl"] == "reference"
+    assert d["metric"] == "MLUPS" and d["unit"] == "MLUPS" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["steps"] >= 1 and d["n_gpus"] == 1
+    assert d["config"]["workload"].startswith("rushton-400^3")
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
