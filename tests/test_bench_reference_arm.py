@@ -28,3 +28,16 @@ def test_reference_arm_prints_one_contract_line(ref_oracle):
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_main_arm_fails_loudly_without_a_gpu():
+    """No CPU fallback: without a GPU the measured arm exits non-zero and
+    prints no JSON line."""
+    import torch
+    if torch.cuda.is_available():
+        import pytest
+        pytest.skip("a GPU is visible: the measured arm would run for real")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "3", "--warmup", "3",
+                          "--no-cpu-baseline"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode != 0
+    assert not [ln for ln in out.stdout.splitlines() if ln.strip().startswith("{")]
