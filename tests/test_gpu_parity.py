@@ -282,6 +282,26 @@ def test_rushton_tank_60_cubed_20_steps_vs_reference(gpu, ref_oracle, port_oracl
 
 
 @pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_rushton_16_cubed_vs_golden_fixture(gpu, port_oracle, streaming):
+    """Against the committed fixture tests/golden/rushton16_6steps.npz (the
+    reference's own FP32 fields of a 16^3 Rushton tank after 6 steps, made by
+    tests/golden/make_golden.py): the same tolerance as the 60^3 test,
+    relative L2 <= 1e-4 for rho, u, F and Nu."""
+    import os
+    tb, po = gpu, port_oracle
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rushton16_6steps.npz"))
+    edge, steps = int(g["edge"]), int(g["steps"])
+    cu, _, _ = _rushton_run(tb, po, edge, streaming, steps, "port")
+    mg = cu.read_moments().astype(np.float64)
+    fg = cu.read_force().astype(np.float64)
+    assert rel_l2(mg[..., 0], g[f"{streaming}_rho"]) <= 1e-4
+    assert rel_l2(velocity(mg, fg), g[f"{streaming}_u"]) <= 1e-4
+    assert rel_l2(fg, g[f"{streaming}_F"]) <= 1e-4
+    assert rel_l2(cu.read_nu(), g[f"{streaming}_Nu"]) <= 1e-4
+    cu.close()
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
 def test_step_variants_bit_identical(gpu, streaming):
     """1, 2 and 4 cells per thread run the same per-cell arithmetic: the
     states after several full steps must be bit-identical."""
