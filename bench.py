@@ -17,7 +17,8 @@ forcing. Metric: MLUPS = interior cells x steps / s.
   e2e     the public C-ABI driven the way main.cpp drives the reference: per
           step the host generates the blade markers at the new angle, copies
           them from pinned memory (H2D), runs collision + forcing, and reads
-          back the FP64 impeller load (D2H); wall-clock, synchronized.
+          back the FP64 impeller load (D2H), reading step s's load after
+          queueing step s+1; wall-clock, synchronized at both ends.
   roofline  the fused step kernel: 152 algorithmic bytes per cell (18
           populations read + written, Nu read + written) / its average
           CUDA-event duration, against the measured copy bandwidth.
@@ -26,7 +27,9 @@ forcing. Metric: MLUPS = interior cells x steps / s.
 
 `--impl reference` times the reference's CPU implementation instead: every
 host thread advances its own reference ComputeUnit on a 400 x 16 x 400 slab
-through the impeller plane of the same tank, one step per "step".
+through the impeller plane of the same tank, one reference step per "step";
+it times max(1, K/25) such steps after min(W, 1) warm-up steps, so that the
+default run ends in seconds, and reports the count it timed.
 
 Multi-GPU: `torchrun --nproc-per-node N bench.py --gpus N` runs one replica
 per GPU (independent tanks, no collective: weak scaling).
