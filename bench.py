@@ -26,10 +26,12 @@ forcing. Metric: MLUPS = interior cells x steps / s.
           oracle/_ref) on a bounded sample of the same workload.
 
 `--impl reference` times the reference's CPU implementation instead: every
-host thread advances its own reference ComputeUnit on a 400 x 16 x 400 slab
-through the impeller plane of the same tank, one reference step per "step";
-it times max(1, K/25) such steps after min(W, 1) warm-up steps, so that the
-default run ends in seconds, and reports the count it timed.
+host thread advances its own reference ComputeUnit on a 400 x h x 400 slab
+through the impeller plane of the same tank (h = 16 planes, 8 when K + W
+exceeds 100, so that the run ends within a few minutes), one reference step
+per "step", K timed steps after W warm-up steps. That process loads only the
+reference harness (oracle/_ref), which also carries the project's marker
+generator.
 
 Multi-GPU: `torchrun --nproc-per-node N bench.py --gpus N` runs one replica
 per GPU (independent tanks, no collective: weak scaling).
@@ -215,7 +217,9 @@ def run_ours(args, rank, world, device):
     load_np = load.numpy()
     got = [torch.cuda.Event(), torch.cuda.Event()]
     spec = rt.spec
-    k_e2e = max(3, args.steps // 5)
+    # at least 50 steps and 0.6 s of wall clock, so that one host hiccup
+    # cannot move the figure by much
+    k_e2e = max(50, args.steps, int(math.ceil(600.0 / max(ms / args.steps, 1e-3))))
     loads = []
 
     def upload_next():
@@ -245,6 +249,12 @@ def run_ours(args, rank, world, device):
         got[(k - 1) % 2].synchronize()
         loads.append(load_np[(k - 1) % 2].copy())
 
+    # the fields after the timed steps; then the e2e run starts again from
+    # rest (initialise + forcing, main.cpp:261-305), so that it stays within
+    # the step count the Simple wall rule keeps finite
+    red_timed = cu.reduce_fp64()
+    cu.initialise(1.0)
+    cu.forcing_resident(ALPHA, BETA)
     e2e_steps(2)
     barrier(world)
     cu.synchronize()
@@ -273,6 +283,9 @@ def run_ours(args, rank, world, device):
         "nu": nu,
         "load": load_np.tolist(),
         "fields_finite": bool(np.isfinite(red).all() and np.isfinite(load_np).all()),
+        "fields_finite_after_timed": bool(np.isfinite(red_timed).all()),
+        "steps_before_timed_check": args.warmup + args.steps,
+        "e2e_steps_from_rest": k_e2e + 2,
         "mass_drift": float(red[0] / cells - 1.0),
         "launches": launches,
         "step_launches": kernel_n,
@@ -370,7 +383,7 @@ def run_batched(args, rank, world, device):
     # tank's FP64 impeller load read back to pinned host memory (queued on
     # the batch's stream, one wait per chunk)
     chunk = 10
-    n_chunks = max(1, args.steps // (5 * chunk))
+    n_chunks = max(5, args.steps // chunk, int(math.ceil(600.0 / max(chunk * ms / args.steps, 1e-3))))
     load_t = torch.empty((len(tanks), 5), dtype=torch.float64, pin_memory=True)
     load = load_t.numpy()
     b.synchronize()
@@ -728,26 +741,36 @@ def report_serving(args, rank, world, local, config):
 
 # ---------------------------------------------------------------- reference arm
 
-def slab_markers(tb, rt, j0, height, angle, dth):
+def slab_markers(rt, j0, height, angle, dth):
     m = rt.forcing_list(angle, dth, nonupdating_delta=dth)
     m = m[(m["j"] >= j0) & (m["j"] < j0 + height)].copy()
     m["j"] -= j0
     return m
 
 
+def reference_height(steps, warmup):
+    """Slab height of the reference sample: 16 planes, 8 for long runs, so
+    that --steps K --warmup W ends within a few minutes on the host cores."""
+    return 16 if steps + warmup <= 100 else 8
+
+
 def reference_sample(steps, warmup, threads, edge=EDGE, height=16):
     """Every thread advances its own reference ComputeUnit (FP32, Simple,
-    LES) on an edge x height x edge slab through the impeller plane."""
-    import tdlbcpp_b200 as tb
+    LES) on an edge x height x edge slab through the impeller plane.
+
+    Only the reference harness (oracle/_ref/libtdlb_ref.so) is loaded: the
+    marker lists come from the project's generator compiled into that
+    harness and nu from the reference's own calcNuAndRe_m, so this process
+    never maps the B200 library."""
     from oracle import pyoracle as po
 
-    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=TIP, startup_steps=0)
-    nu = tb.nu_from_reynolds(RE, TIP, rt.blade_outer_radius())
+    rt = po.RefRushton(edge, edge, edge, tip_speed=TIP, startup_steps=0)
+    nu = po.ref_nu(RE, TIP, rt.blade_outer_radius())
     dth = rt.increment(1)
     j0 = int(round(edge / 3.0)) - height // 2
     flow = po.Flow(initialRho=1.0, nu=nu, cs0=0.1, g3=0.8, alpha=ALPHA, beta=BETA, useLES=True)
     lats = [po.CpuLattice("ref", edge, height, edge, flow, "Simple", 4, tmpdir="/tmp") for _ in range(threads)]
-    mk = slab_markers(tb, rt, j0, height, 0.0, dth)
+    mk = slab_markers(rt, j0, height, 0.0, dth)
     for L in lats:
         L.initialise(1.0)
         L.forcing(mk, ALPHA, BETA)
@@ -755,7 +778,7 @@ def reference_sample(steps, warmup, threads, edge=EDGE, height=16):
     times = []
     for s in range(warmup + steps):
         angle += dth
-        mk = slab_markers(tb, rt, j0, height, angle, dth)
+        mk = slab_markers(rt, j0, height, angle, dth)
         ths = [threading.Thread(target=L.step, args=(mk, ALPHA, BETA)) for L in lats]
         t = time.perf_counter()
         for th in ths:
@@ -770,7 +793,7 @@ def reference_sample(steps, warmup, threads, edge=EDGE, height=16):
     total = sum(times)
     return {"value": cells * len(times) / total / 1e6, "cores": threads, "seconds": total,
             "sample": f"{threads} x reference ComputeUnit<float,...,Simple,CPU> on a {edge}x{height}x{edge} slab "
-                      f"through the impeller plane, {len(times)} step(s) each"}
+                      f"through the impeller plane, {len(times)} timed step(s) each after {warmup} warm-up step(s)"}
 
 
 def host_threads(edge=EDGE, height=16):
@@ -861,7 +884,7 @@ def report_batched(args, rank, world, local, config):
         "fields_finite": res["fields_finite"],
     }
     if world == 1 and not args.no_cpu_baseline:
-        r = reference_sample(1, 0, host_threads())
+        r = reference_sample(3, 1, host_threads())
         line["cpu_baseline"] = {"value": r["value"], "unit": "MLUPS", "cores": r["cores"], "kind": "reference",
                                 "sample": r["sample"] + " (per-cell rate of the same step)"}
     print(json.dumps(line), flush=True)
@@ -920,10 +943,11 @@ def main():
         if rank != 0:
             return 0
         nthr = host_threads()
-        steps = max(1, args.steps // 25)
-        r = reference_sample(steps, min(args.warmup, 1), nthr)
+        steps, warm = args.steps, args.warmup
+        h = reference_height(steps, warm)
+        r = reference_sample(steps, warm, nthr, height=h)
         line = {"metric": "MLUPS", "value": r["value"], "unit": "MLUPS", "n_gpus": args.gpus, "steps": steps,
-                "warmup": min(args.warmup, 1), "ms_per_step": r["seconds"] / steps * 1e3, "higher_is_better": True,
+                "warmup": warm, "ms_per_step": r["seconds"] / steps * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": config,
                 "impl": "reference",
                 "cpu_baseline": {"value": r["value"], "unit": "MLUPS", "cores": r["cores"], "kind": "reference",
@@ -964,10 +988,12 @@ def main():
         "split_step": {"on": res["inner_fraction"] is not None, "inner_cell_fraction": res["inner_fraction"],
                        "step_launches_per_step": res["step_launches"] / args.steps},
         "fields_finite": res["fields_finite"],
+        "fields_finite_after_timed_steps": res["fields_finite_after_timed"],
+        "steps_from_rest_at_timed_check": res["steps_before_timed_check"],
         "mass_drift": res["mass_drift"],
     }
     if world == 1 and not args.no_cpu_baseline:
-        r = reference_sample(1, 0, host_threads())
+        r = reference_sample(3, 1, host_threads())
         line["cpu_baseline"] = {"value": r["value"], "unit": "MLUPS", "cores": r["cores"], "kind": "reference",
                                 "sample": r["sample"]}
     print(json.dumps(line), flush=True)

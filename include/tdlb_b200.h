@@ -350,16 +350,21 @@ int tdlb_impeller_load(tdlb_handle h, double* out5);
  * reduction's device scratch. */
 int tdlb_impeller_load_async(tdlb_handle h, double* out5);
 
-/* The same FP64 impeller load for callers that may not allocate device
- * memory while they run (inside CUDA graph capture, under their own memory
- * pool, or in a loop that must not allocate): it calls no cudaMalloc,
- * cudaFree or other allocating routine, and writes the 5 doubles to the
- * caller's DEVICE buffer d_out5 on h's stream (nothing is synchronised).
- * No counterpart in the reference. Its scratch is a fixed 40 KiB array
- * compiled into the library, so lists of more than 1,048,576 markers are
- * rejected (TDLB_EINVAL). The first call on each device looks that array up
- * (cudaGetSymbolAddress): make it before any stream capture. All calls on a
- * device share the array; calls that overlap on the GPU race. */
+/* The same FP64 impeller load for callers that cannot allocate device
+ * memory once their run has started: a host application that hands the
+ * whole GPU to its own memory pool up front (a cudaMalloc of the library's
+ * would fail or break its accounting), or a real-time loop that forbids
+ * allocation after start-up (cudaMalloc can synchronise the device and takes
+ * unbounded time). It calls no cudaMalloc, cudaFree or other allocating
+ * routine, and writes the 5 doubles to the caller's DEVICE buffer d_out5 on
+ * h's stream (nothing is synchronised). No counterpart in the reference.
+ * Its scratch is a fixed 40 KiB array compiled into the library, so lists of
+ * more than 1,048,576 markers are rejected (TDLB_EINVAL). The first call on
+ * each device looks that array up (cudaGetSymbolAddress) and keeps the
+ * address: make that first call before any stream capture. A device reset
+ * (cudaDeviceReset) invalidates the kept address: do not call this after
+ * one in the same process. All calls on a device share the array and it
+ * keeps the last call's contents; calls that overlap on the GPU race. */
 int tdlb_impeller_load_noalloc(tdlb_handle h, double* d_out5);
 
 /* Copy of the resident marker list as the device holds it (list order). */

@@ -298,3 +298,80 @@ def coded_fill(x: int, y: int, z: int) -> np.ndarray:
     Q(i,j,k,l) = ((i*100+j)*100+k)*100+l over the ghosted grid."""
     i, j, k, l = np.meshgrid(np.arange(x + 2), np.arange(y + 2), np.arange(z + 2), np.arange(18), indexing="ij")
     return (((i * 100 + j) * 100 + k) * 100 + l).astype(np.uint64)
+
+
+class _RushtonSpec(ctypes.Structure):
+    """Same layout as tdlb_rushton (include/tdlb_b200.h)."""
+
+    _fields_ = [
+        ("x", ctypes.c_int64), ("y", ctypes.c_int64), ("z", ctypes.c_int64),
+        ("tank_diameter", ctypes.c_double), ("impeller_diameter", ctypes.c_double),
+        ("clearance", ctypes.c_double), ("blade_height", ctypes.c_double), ("disk_thickness", ctypes.c_double),
+        ("n_blades", ctypes.c_int32), ("n_baffles", ctypes.c_int32),
+        ("baffle_width", ctypes.c_double), ("wall_inset", ctypes.c_double), ("tip_speed", ctypes.c_double),
+        ("startup_steps", ctypes.c_int64),
+    ]
+
+
+class RefRushton:
+    """The project's Rushton-turbine marker generator as compiled into the
+    reference harness (oracle/_ref/libtdlb_ref.so carries
+    tdlbcpp_b200/csrc/geometry.cpp), so that a process timing the reference
+    builds its marker lists without loading the B200 library. Same methods
+    and results as tdlbcpp_b200.RushtonTurbine."""
+
+    def __init__(self, x: int, y: int, z: int, tip_speed: float = 0.1, startup_steps: int = 0):
+        lib = load("ref")
+        if not hasattr(lib, "_rushton_bound"):
+            sz, vp = ctypes.c_size_t, ctypes.c_void_p
+            sp = ctypes.POINTER(_RushtonSpec)
+            for name, extra in (("fixed", []), ("rotating_nonupdating", [ctypes.c_double]),
+                                ("rotating", [ctypes.c_double, ctypes.c_double])):
+                fn = getattr(lib, "tdlb_rushton_" + name)
+                fn.restype = ctypes.c_int
+                fn.argtypes = [sp, *extra, vp, sz, ctypes.POINTER(sz)]
+            lib.tdlb_rushton_impeller_increment.restype = ctypes.c_double
+            lib.tdlb_rushton_impeller_increment.argtypes = [sp, ctypes.c_uint64]
+            lib.tdlb_rushton_blade_outer_radius.restype = ctypes.c_int
+            lib.tdlb_rushton_blade_outer_radius.argtypes = [sp]
+            lib._rushton_bound = True
+        self.lib = lib
+        self.spec = _RushtonSpec()
+        self.spec.x, self.spec.y, self.spec.z = x, y, z
+        self.spec.tip_speed = tip_speed
+        self.spec.startup_steps = startup_steps
+
+    def _gen(self, name, *args) -> np.ndarray:
+        fn = getattr(self.lib, "tdlb_rushton_" + name)
+        n = ctypes.c_size_t()
+        if fn(ctypes.byref(self.spec), *args, None, 0, ctypes.byref(n)):
+            raise ValueError(f"tdlb_rushton_{name} failed")
+        out = np.zeros(n.value, MARKER_DTYPE)
+        if fn(ctypes.byref(self.spec), *args, _ptr(out), n.value, ctypes.byref(n)):
+            raise ValueError(f"tdlb_rushton_{name} failed")
+        return out
+
+    def fixed(self) -> np.ndarray:
+        return self._gen("fixed")
+
+    def rotating_nonupdating(self, delta_angle: float) -> np.ndarray:
+        return self._gen("rotating_nonupdating", ctypes.c_double(delta_angle))
+
+    def rotating(self, angle: float, delta_angle: float) -> np.ndarray:
+        return self._gen("rotating", ctypes.c_double(angle), ctypes.c_double(delta_angle))
+
+    def increment(self, step: int) -> float:
+        return self.lib.tdlb_rushton_impeller_increment(ctypes.byref(self.spec), step)
+
+    def blade_outer_radius(self) -> int:
+        return self.lib.tdlb_rushton_blade_outer_radius(ctypes.byref(self.spec))
+
+    def forcing_list(self, angle: float, delta_angle: float, nonupdating_delta: float = None) -> np.ndarray:
+        """fixed + rotating-non-updating + rotating, the order main.cpp:301-303 builds."""
+        nd = delta_angle if nonupdating_delta is None else nonupdating_delta
+        return np.concatenate([self.fixed(), self.rotating_nonupdating(nd), self.rotating(angle, delta_angle)])
+
+
+def ref_nu(re: float, tip_speed: float, blade_outer_radius: int) -> float:
+    """The reference's own FlowParams::calcNuAndRe_m (FlowParams.hpp:65-70)."""
+    return float(load("ref").tdlbref_calc_nu(re, tip_speed, blade_outer_radius))

@@ -96,6 +96,7 @@ void tdlbo_destroy(void* h) {
     free(h);
 }
 
+static long tdlbo_size_x(void* h) { long s; DISPATCH(h, s = (long)LAT32(h)->x, s = (long)LAT64(h)->x); return s; }
 long tdlbo_size(void* h) { long s; DISPATCH(h, s = (long)LAT32(h)->size, s = (long)LAT64(h)->size); return s; }
 int tdlbo_even_step(void* h) { int e; DISPATCH(h, e = LAT32(h)->evenStep, e = LAT64(h)->evenStep); return e; }
 void tdlbo_set_even_step(void* h, int even) { DISPATCH(h, LAT32(h)->evenStep = even != 0, LAT64(h)->evenStep = even != 0); }
@@ -141,10 +142,10 @@ void tdlbo_get_o(void* h, uint8_t* out) {
 /* Interior moments through the reference's read accessor (plain Q for
  * Simple, the esoteric read map for Esotwist), interior cells in (i, j, k)
  * order, 18 per cell. */
-#define GET_MOMENTS(L, out)                                                        \
+#define GET_MOMENTS(L, out, i_lo, i_hi)                                            \
     do {                                                                           \
         size_t c_ = 0;                                                             \
-        for (long i = 1; i <= (L)->xg - 2; i++)                                    \
+        for (long i = 1 + (i_lo); i <= (i_hi); i++)                                \
             for (long j = 1; j <= (L)->yg - 2; j++)                                \
                 for (long k = 1; k <= (L)->zg - 2; k++, c_++) {                    \
                     __typeof__((L)->Q[0]) q_[18];                                  \
@@ -158,19 +159,27 @@ void tdlbo_get_o(void* h, uint8_t* out) {
                 }                                                                  \
     } while (0)
 
-void tdlbo_get_moments(void* h, double* out) {
+/* The same for the interior slab i0 <= i < i1 (0-based interior i), so that
+ * a large lattice can be compared one slab at a time. */
+void tdlbo_get_moments_range(void* h, long i0, long i1, double* out) {
     if (((Handle*)h)->precision == 4) {
         Lattice_f32* L = LAT32(h);
+        if (i0 < 0) i0 = 0;
+        if (i1 > L->xg - 2) i1 = L->xg - 2;
 #define GET_MOMENTS_ESO(L, i, j, k, q) eso_read_f32(L, (L)->Q, i, j, k, (L)->evenStep, q)
-        GET_MOMENTS(L, out);
+        GET_MOMENTS(L, out, i0, i1);
 #undef GET_MOMENTS_ESO
     } else {
         Lattice_f64* L = LAT64(h);
+        if (i0 < 0) i0 = 0;
+        if (i1 > L->xg - 2) i1 = L->xg - 2;
 #define GET_MOMENTS_ESO(L, i, j, k, q) eso_read_f64(L, (L)->Q, i, j, k, (L)->evenStep, q)
-        GET_MOMENTS(L, out);
+        GET_MOMENTS(L, out, i0, i1);
 #undef GET_MOMENTS_ESO
     }
 }
+
+void tdlbo_get_moments(void* h, double* out) { tdlbo_get_moments_range(h, 0, tdlbo_size_x(h), out); }
 
 /* One transport-only step on the current Q: Simple push
  * (StreamingSimple.hpp:257-307) or, for Esotwist, AccessField read + write

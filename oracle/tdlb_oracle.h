@@ -62,6 +62,7 @@ void tdlbo_get_nu(void* h, double* out);
 void tdlbo_set_nu_field(void* h, const double* in);
 void tdlbo_get_o(void* h, uint8_t* out);
 void tdlbo_get_moments(void* h, double* out);
+void tdlbo_get_moments_range(void* h, long i0, long i1, double* out);
 void tdlbo_transport(void* h);
 void tdlbo_get_forcing_sums(void* h, double* out, long n);
 

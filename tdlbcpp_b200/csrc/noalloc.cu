@@ -1,13 +1,13 @@
 // tdlb_impeller_load_noalloc: the FP64 impeller load without any allocation.
 //
-// Who needs it: callers that may not allocate device memory once their
-// simulation is running -- for example code that records its per-step work
-// into a CUDA graph (cudaMalloc is not allowed while a stream is being
-// captured), hosts that hand all GPU memory to their own pool up front, or
-// real-time loops with a no-allocation rule after start-up. The allocating
-// entry point, tdlb_impeller_load, creates its reduction buffer with
-// cudaMalloc on its first call; this variant keeps that buffer in a
-// fixed-size array compiled into the library instead.
+// Who needs it: callers that cannot allocate device memory once their
+// simulation is running -- a host application that hands all GPU memory to
+// its own pool up front (a cudaMalloc from the library would fail or escape
+// the pool's accounting), or a real-time loop with a no-allocation rule after
+// start-up (cudaMalloc can synchronise the device and has no time bound).
+// The allocating entry point, tdlb_impeller_load, creates its reduction
+// buffer with cudaMalloc on its first call; this variant keeps that buffer
+// in a fixed-size array compiled into the library instead.
 //
 // The scratch: g_load_partials below, a file-scope __device__ array of
 // kNoAllocMaxBlocks * 5 doubles (40 KiB). Every GPU that loads the library
@@ -24,7 +24,9 @@
 // Set-up: the host cannot use the array's name as a device address. The
 // first call on each device looks the address up with cudaGetSymbolAddress
 // (with that device current) and keeps it; make that first call before any
-// stream capture starts.
+// stream capture starts. A device reset (cudaDeviceReset) in the same
+// process invalidates the kept address, and a later call would write through
+// it: do not call this entry point after a reset.
 #include "tdlb_handle.hpp"
 
 #include <mutex>

@@ -6,7 +6,8 @@ Markers:
           because the product has no CPU fallback.
 
 The CPU oracles (oracle/libtdlb_oracle.so, oracle/_ref/libtdlb_ref.so) are
-built on demand when missing and the sources are present.
+built on demand when missing (oracle/Makefile; the reference checkout is the
+TDLB_REFERENCE environment variable, with the default the Makefile names).
 """
 import os
 import subprocess
@@ -18,23 +19,23 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REF_SRC = "/root/reference/tdlbcpp/src"
-
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (sm_100) GPU and the built CUDA library")
 
 
 def _build(target: str):
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), target], check=True,
-                   stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+    return subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), target],
+                          stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
 
 
 @pytest.fixture(scope="session")
 def port_oracle():
     from oracle import pyoracle as po
     if not po.available("port"):
-        _build("port")
+        r = _build("port")
+        if r.returncode:
+            pytest.fail("building oracle/libtdlb_oracle.so failed:\n" + r.stdout[-2000:])
     return po
 
 
@@ -42,9 +43,10 @@ def port_oracle():
 def ref_oracle():
     from oracle import pyoracle as po
     if not po.available("ref"):
-        if not os.path.isdir(REF_SRC):
-            pytest.fail("oracle/_ref/libtdlb_ref.so is not built and the reference sources are absent")
-        _build("ref")
+        r = _build("ref")
+        if r.returncode:
+            pytest.fail("oracle/_ref/libtdlb_ref.so is not built and building it failed "
+                        "(are the reference sources present?):\n" + r.stdout[-2000:])
     return po
 
 

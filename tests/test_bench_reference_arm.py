@@ -10,12 +10,33 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+# Runs bench.py in this interpreter and, at exit, reports which of the
+# project's shared libraries the process mapped (from /proc/self/maps).
+_MAPS_WRAPPER = """
+import atexit, runpy, sys
+def _report():
+    with open("/proc/self/maps") as f:
+        maps = f.read()
+    sys.stderr.write("MAPPED_B200=%d\\n" % ("libtdlb_b200.so" in maps))
+    sys.stderr.write("MAPPED_REF=%d\\n" % ("libtdlb_ref.so" in maps))
+atexit.register(_report)
+sys.argv = ["bench.py"] + sys.argv[1:]
+runpy.run_path("bench.py", run_name="__main__")
+"""
+
+
 def test_reference_arm_prints_one_contract_line(ref_oracle):
-    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
-                          "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600, check=True)
+    out = subprocess.run([sys.executable, "-c", _MAPS_WRAPPER, "--impl", "reference", "--steps", "2",
+                          "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=600, check=True)
     lines = [ln for ln in out.stdout.splitlines() if ln.strip()]
     assert len(lines) == 1
+    # the reference arm runs the reference harness only: the B200 library is
+    # never loaded into its process
+    assert "MAPPED_REF=1" in out.stderr, out.stderr[-2000:]
+    assert "MAPPED_B200=0" in out.stderr, out.stderr[-2000:]
     d = json.loads(lines[0])
+    # it times exactly the steps and warm-up steps it was given
+    assert d["steps"] == 2 and d["warmup"] == 3
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
                 "scaling", "vs_baseline", "dtype", "data", "config"):
         assert key in d, key

@@ -103,3 +103,20 @@ def test_nu_from_reynolds_bit_exact_with_reference(ref_oracle, re, uav, radius):
     import tdlbcpp_b200 as tb
     lib = ref_oracle.load("ref")
     assert tb.nu_from_reynolds(re, uav, radius) == lib.tdlbref_calc_nu(re, uav, radius)
+
+
+@pytest.mark.parametrize("edge", [16, 60, 400])
+def test_reference_harness_geometry_equals_product_generator(ref_oracle, edge):
+    """The marker generator compiled into the reference harness (used by
+    bench.py's reference arm, which must not load the B200 library) gives the
+    product generator's lists bit for bit, and the reference's own
+    calcNuAndRe_m gives the product's nu."""
+    import tdlbcpp_b200 as tb
+    po = ref_oracle
+    a = po.RefRushton(edge, edge, edge, tip_speed=0.1)
+    b = tb.RushtonTurbine(edge, edge, edge, tip_speed=0.1)
+    d = a.increment(1)
+    assert d == b.increment(1) and a.blade_outer_radius() == b.blade_outer_radius()
+    for angle in (0.0, 0.37, 2.5):
+        assert a.forcing_list(angle, d).tobytes() == b.forcing_list(angle, d).tobytes()
+    assert po.ref_nu(20000.0, 0.1, a.blade_outer_radius()) == tb.nu_from_reynolds(20000.0, 0.1, b.blade_outer_radius())

@@ -1,13 +1,18 @@
 """tdlb_impeller_load_noalloc against tdlb_impeller_load (collected last).
 
-The allocation-free entry point is for callers that may not allocate device
-memory while running (CUDA graph capture, their own memory pool, no-alloc
-real-time loops). It writes the FP64 impeller load into a caller-owned device
-buffer, using a fixed scratch array compiled into the library instead of a
-cudaMalloc'd one. Here it must give the allocating entry point's answer on
-two calls in a row (with a time step in between), within the tolerance the
-impeller-load parity test uses. Works alone in a fresh process and after the
-other tests.
+The allocation-free entry point is for callers that cannot allocate device
+memory once their run has started: a host application that gives the whole
+GPU to its own memory pool up front, or a real-time loop that forbids
+allocation after start-up. It writes the FP64 impeller load into a
+caller-owned device buffer, using a fixed scratch array compiled into the
+library instead of a cudaMalloc'd one.
+
+Here, on a fresh handle, the first call is the allocation-free one (before
+the allocating entry point has run on that handle), and it must give the
+allocating entry point's answer on two calls in a row (with a time step in
+between), within the tolerance the impeller-load parity test uses. Around
+the second call the device's free memory must not change. Works alone in a
+fresh process and after the other tests.
 """
 import numpy as np
 import pytest
@@ -42,13 +47,21 @@ def test_impeller_load_noalloc_matches_allocating_entry_point(gpu):
         cu.collision()
         cu.forcing_resident(ALPHA, BETA)
 
+    # the caller's output buffer, allocated before the calls
     out = torch.full((5,), float("nan"), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     for call in range(2):
-        want = cu.impeller_load()
-        cu.impeller_load_noalloc(out.data_ptr())
+        free_before = torch.cuda.mem_get_info()[0]
+        cu.impeller_load_noalloc(out.data_ptr())      # on call 0: the handle's first load of any kind
         cu.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
         got = out.cpu().numpy()
+        if call == 1:
+            # the first call may load the library's module onto the device
+            # (lazy module loading, done by the driver); the second one
+            # finds everything in place and allocates nothing
+            assert free_after == free_before, f"free device memory changed by {free_before - free_after} bytes"
+        want = cu.impeller_load()
         assert np.isfinite(got).all(), f"call {call}: {got}"
         close_enough(got, want)
         # advance one step so the second call sees different data
@@ -56,4 +69,6 @@ def test_impeller_load_noalloc_matches_allocating_entry_point(gpu):
         cu.rotate_impeller(angle, d)
         cu.collision()
         cu.forcing_resident(ALPHA, BETA)
+        out.fill_(float("nan"))
+        torch.cuda.synchronize()
     cu.close()
