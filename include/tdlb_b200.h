@@ -82,10 +82,19 @@ typedef struct tdlb_config {
  * (ComputeUnit.hpp:125-133, ComputeUnitGpu.hpp:31-47) as driven by main.cpp
  * from the input JSON (main.cpp:135-164, :213-256). `params_json` is the text
  * of the reference's input file (GridParams, FlowParams, RunningParams ... ;
- * keys as in input_debug_gridx60_numSteps20.json). FlowParams.nu == 0 is
- * replaced by calcNuAndRe_m(impellerBladeOuterRadius = int(x/6))
- * (FlowParams.hpp:65-70, main.cpp:275). */
+ * keys as in input_debug_gridx60_numSteps20.json). The unit takes the
+ * FlowParams fields as the file gives them (rounded to float, the
+ * reference's FlowParams<float>), nu included: main.cpp builds its unit
+ * before calcNuAndRe_m (main.cpp:275) sets nu in main's own copy, so the
+ * reference's unit also keeps the file's nu. A caller that wants
+ * calcNuAndRe_m's nu writes it into the file or uses tdlb_create_config. */
 int tdlb_create(const char* params_json, int device, tdlb_handle* out);
+
+/* The configuration tdlb_create builds from params_json, without a GPU
+ * (host only; same errors as tdlb_create, message in tdlb_last_error(NULL)).
+ * Replaces: GridParams/FlowParams::getParamsFromJson as main.cpp:150-153
+ * calls them. */
+int tdlb_config_from_json(const char* params_json, tdlb_config* out);
 
 /* Same, from a filled tdlb_config (nu used as given). */
 int tdlb_create_config(const tdlb_config* cfg, int device, tdlb_handle* out);

@@ -92,6 +92,7 @@ def load(kind: str) -> ctypes.CDLL:
         sig["transport"] = (None, [vp])
         sig["get_forcing_sums"] = (None, [vp, vp, cl])
         sig["set_threads"] = (None, [ci])
+        sig["get_moments_range"] = (None, [vp, cl, cl, vp])
     else:
         sig["kat_simple_golden"] = (ci, [ci, vp])
         sig["checkpoint_write"] = (cl, [vp, ctypes.c_char_p, cl, ctypes.c_char_p, cl])
@@ -192,6 +193,12 @@ class CpuLattice:
         """Interior moments [x, y, z, 18] through the reference's read accessor."""
         out = np.empty((self.x, self.y, self.z, 18), np.float64)
         self._fn("get_moments")(self.h, _ptr(out))
+        return out
+
+    def get_moments_range(self, i0: int, i1: int) -> np.ndarray:
+        """Interior moments of the slab i0 <= i < i1 [i1-i0, y, z, 18] (port only)."""
+        out = np.empty((i1 - i0, self.y, self.z, 18), np.float64)
+        self._fn("get_moments_range")(self.h, i0, i1, _ptr(out))
         return out
 
     def interior(self, a: np.ndarray) -> np.ndarray:
@@ -375,3 +382,30 @@ class RefRushton:
 def ref_nu(re: float, tip_speed: float, blade_outer_radius: int) -> float:
     """The reference's own FlowParams::calcNuAndRe_m (FlowParams.hpp:65-70)."""
     return float(load("ref").tdlbref_calc_nu(re, tip_speed, blade_outer_radius))
+
+
+def reference_root() -> str:
+    """The reference checkout the oracle compiles from (oracle/Makefile's
+    REF_ROOT: the TDLB_REFERENCE environment variable or its default)."""
+    import subprocess
+    r = subprocess.run(["make", "-s", "-C", HERE, "print-ref-root"], capture_output=True, text=True, check=True)
+    return r.stdout.strip()
+
+
+def ref_read_input(path: str) -> dict:
+    """What a ComputeUnit built by main.cpp from the input file at `path`
+    holds, read by the reference's own GridParams / FlowParams parsers
+    (tdlbref_read_input)."""
+    lib = load("ref")
+    fn = lib.tdlbref_read_input
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_Flow), ctypes.c_void_p]
+    xyz = np.zeros(3, np.int64)
+    ms = np.zeros(1, np.int64)
+    st = np.zeros(1, np.int32)
+    f = _Flow()
+    if fn(path.encode(), _ptr(xyz), _ptr(ms), ctypes.byref(f), _ptr(st)):
+        raise ValueError(f"the reference could not read {path}")
+    return {"x": int(xyz[0]), "y": int(xyz[1]), "z": int(xyz[2]), "multiStep": int(ms[0]),
+            "initialRho": f.initialRho, "nu": f.nu, "cs0": f.cs0, "g3": f.g3, "alpha": f.alpha, "beta": f.beta,
+            "useLES": bool(f.useLES), "streaming": "Simple" if st[0] == 0 else "Esotwist"}

@@ -24,6 +24,7 @@
 #include <vector>
 #include <iostream>
 #include <sstream>
+#include <fstream>
 
 #include "Header.h"
 #include "ComputeUnit.h"
@@ -390,6 +391,45 @@ double tdlbref_calc_nu(double re, double uav, int radius) {
     f.uav = (float)uav;
     f.calcNuAndRe_m(radius);
     return (double)f.nu;
+}
+
+// The flow and grid a ComputeUnit built by main.cpp from an input file
+// holds: the file parsed by the reference's own GridParams / FlowParams
+// getParamsFromJson (main.cpp:133-164), FlowParams<float> as
+// useQVecPrecision is float (main.cpp:50), and the unit constructed from
+// that FlowParams before main.cpp:275 computes nu for its own copy -- so
+// the unit keeps the file's nu. xyz[3] = GridParams x, y, z; *multistep =
+// GridParams.multiStep (the ghost width, main.cpp:225); *streaming = 0 for
+// "Simple", 1 otherwise (main.cpp:242-256). Returns 0, or -1 when the file
+// cannot be read or parsed.
+int tdlbref_read_input(const char* path, long* xyz, long* multistep, FlowC* out, int* streaming) {
+    try {
+        nlohmann::json j;
+        std::ifstream in(path);
+        if (!in) return -1;
+        in >> j;
+        GridParams grid;
+        FlowParams<float> flow;
+        MuteCout mute;
+        grid.getParamsFromJson(j["GridParams"]);
+        flow.getParamsFromJson(j["FlowParams"]);
+        xyz[0] = (long)grid.x;
+        xyz[1] = (long)grid.y;
+        xyz[2] = (long)grid.z;
+        *multistep = (long)grid.multiStep;
+        out->initialRho = flow.initialRho;
+        out->nu = flow.nu;
+        out->cs0 = flow.cs0;
+        out->g3 = flow.g3;
+        out->alpha = flow.alpha;
+        out->beta = flow.beta;
+        out->useLES = flow.useLES ? 1 : 0;
+        out->pad = 0;
+        *streaming = flow.streaming == "Simple" ? 0 : 1;
+    } catch (const std::exception&) {
+        return -1;
+    }
+    return 0;
 }
 
 // setOutputExcludePoints / unsetOutputExcludePoints (ComputeUnitOutput.hpp:20-53).

@@ -147,6 +147,17 @@ def make_config(**fields) -> Config:
     return cfg
 
 
+def config_from_json(params_json: str) -> Config:
+    """The tdlb_config tdlb_create builds from a reference input file's text
+    (host only; raises TdlbError on a malformed or incomplete file)."""
+    lib = load_library()
+    cfg = Config()
+    rc = lib.tdlb_config_from_json(params_json.encode(), ctypes.byref(cfg))
+    if rc:
+        raise TdlbError(rc, lib.tdlb_last_error(None).decode())
+    return cfg
+
+
 def library_path() -> str:
     return os.path.join(HERE, _LIB_NAME)
 
@@ -168,6 +179,7 @@ def load_library() -> ctypes.CDLL:
     sigs = {
         "tdlb_create": (i32, [ctypes.c_char_p, i32, ctypes.POINTER(H)]),
         "tdlb_create_config": (i32, [ctypes.POINTER(Config), i32, ctypes.POINTER(H)]),
+        "tdlb_config_from_json": (i32, [ctypes.c_char_p, ctypes.POINTER(Config)]),
         "tdlb_destroy": (i32, [H]),
         "tdlb_last_error": (ctypes.c_char_p, [H]),
         "tdlb_initialise": (i32, [H, f32]),

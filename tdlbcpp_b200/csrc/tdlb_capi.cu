@@ -197,15 +197,16 @@ tdlb_config config_from_json(const char* text) {
         c.useLES = flow.at("useLES").get<bool>() ? 1 : 0;
         // main.cpp:242-256: "Simple" selects Simple, anything else Esotwist
         c.streaming = flow.at("streaming").get<std::string>() == "Simple" ? TDLB_STREAMING_SIMPLE : TDLB_STREAMING_ESOTWIST;
-        if (c.nu == 0.0) {
-            // calcNuAndRe_m(impellerBladeOuterRadius) (FlowParams.hpp:65-70);
-            // the blade outer radius of the Rushton geometry, D/2 = T/6.
-            const float reM = (float)flow.at("reMNonDimensional").get<double>();
-            const float uav = (float)flow.at("uav").get<double>();
-            const float Re_m = (float)(reM * M_PI / 2.0);
-            const int radius = (int)(c.x / 6);
-            c.nu = (double)(float)(uav * (float)radius / Re_m);
-        }
+        // nu as the file gives it: main.cpp constructs the ComputeUnit from
+        // its FlowParams (:242-256) before calcNuAndRe_m (:275) sets nu in
+        // main's own copy, so the reference's unit keeps the file's value.
+        // The FlowParams fields are float in the reference (useQVecPrecision).
+        c.initialRho = (double)(float)c.initialRho;
+        c.nu = (double)(float)c.nu;
+        c.cs0 = (double)(float)c.cs0;
+        c.g3 = (double)(float)c.g3;
+        c.alpha = (double)(float)c.alpha;
+        c.beta = (double)(float)c.beta;
     } catch (const Fail&) {
         throw;
     } catch (const std::exception& e) {
@@ -791,6 +792,20 @@ int tdlb_create(const char* params_json, int device, tdlb_handle* out) {
     } catch (const std::bad_alloc&) {
         g_create_error = "host allocation failed";
         return TDLB_ENOMEM;
+    }
+}
+
+int tdlb_config_from_json(const char* params_json, tdlb_config* out) {
+    if (!params_json || !out) {
+        g_create_error = "NULL argument";
+        return TDLB_EINVAL;
+    }
+    try {
+        *out = config_from_json(params_json);
+        return TDLB_OK;
+    } catch (const Fail& f) {
+        g_create_error = f.msg;
+        return f.code;
     }
 }
 

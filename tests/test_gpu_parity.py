@@ -402,3 +402,54 @@ def test_device_rotation_matches_host_generator(gpu):
         host = rt.rotating(angle, d)
         np.testing.assert_array_equal(dev.view(np.uint8), host.view(np.uint8))
     cu.close()
+
+
+def test_shipped_debug_input_vs_reference(gpu, ref_oracle):
+    """A unit made by tdlb_create from the reference's debug input
+    (input_debug_gridx60_numSteps20.json: 60^3, initialRho 8, nu 0 as main.cpp's
+    unit keeps it, cs0 0.12, LES off, Esotwist; its values are pinned against
+    the shipped file by tests/test_input_file.py) against the reference's CPU
+    unit built from the same values, with the file's impeller (uav 0.1,
+    30 start-up steps): forcing, then 20 steps of main.cpp's sequence.
+    Tolerance as the 60^3 test: relative L2 <= 1e-4 for rho, u and F."""
+    import json
+    from test_input_file import SHIPPED_DEBUG_INPUT as S
+    tb, po = gpu, ref_oracle
+    text = json.dumps({
+        "GridParams": {"x": S["x"], "y": S["y"], "z": S["z"], "multiStep": S["multiStep"]},
+        "FlowParams": {"initialRho": S["initialRho"], "reMNonDimensional": 7300.0, "uav": 0.1, "cs0": S["cs0"],
+                       "g3": S["g3"], "nu": S["nu"], "alpha": S["alpha"], "beta": S["beta"], "useLES": S["useLES"],
+                       "streaming": S["streaming"]},
+    })
+    cu = tb.ComputeUnit(params=text)
+    flow = po.Flow(initialRho=S["initialRho"], nu=S["nu"], cs0=S["cs0"], g3=S["g3"], alpha=S["alpha"],
+                   beta=S["beta"], useLES=S["useLES"])
+    lat = po.CpuLattice("ref", S["x"], S["y"], S["z"], flow, S["streaming"], 4)
+    rt = tb.RushtonTurbine(S["x"], S["y"], S["z"], tip_speed=0.1, startup_steps=30)
+    d1 = rt.increment(1)
+    fixed, nonupd = rt.fixed(), rt.rotating_nonupdating(d1)
+    angle = 0.0
+    mk = np.concatenate([fixed, nonupd, rt.rotating(angle, d1)])
+    cu.initialise(S["initialRho"])
+    lat.initialise(S["initialRho"])
+    cu.forcing(mk, S["alpha"], S["beta"])
+    lat.forcing(mk, S["alpha"], S["beta"])
+    for step in range(2, 22):
+        d = rt.increment(step)
+        angle += d
+        mk = np.concatenate([fixed, nonupd, rt.rotating(angle, d)])
+        cu.collision()
+        cu.bounceBackBoundary()
+        cu.streamingPush()
+        cu.moments()
+        cu.forcing(mk, S["alpha"], S["beta"])
+        lat.step(mk, S["alpha"], S["beta"])
+    mg = cu.read_moments().astype(np.float64)
+    fg = cu.read_force().astype(np.float64)
+    mr, fr = lat.get_moments(), lat.interior(lat.get_f())
+    assert np.isfinite(mr).all()
+    assert rel_l2(mg[..., 0], mr[..., 0]) <= 1e-4
+    assert rel_l2(velocity(mg, fg), velocity(mr, fr)) <= 1e-4
+    assert rel_l2(fg, fr) <= 1e-4
+    cu.close()
+    lat.close()

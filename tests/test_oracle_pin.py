@@ -120,3 +120,43 @@ def test_reference_harness_geometry_equals_product_generator(ref_oracle, edge):
     for angle in (0.0, 0.37, 2.5):
         assert a.forcing_list(angle, d).tobytes() == b.forcing_list(angle, d).tobytes()
     assert po.ref_nu(20000.0, 0.1, a.blade_outer_radius()) == tb.nu_from_reynolds(20000.0, 0.1, b.blade_outer_radius())
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_restatement_bit_identical_on_400_cubed_slab(ref_oracle, port_oracle, streaming):
+    """Ties the restatement to the reference at the at-scale geometry: a
+    400 x 16 x 400 slab through the impeller plane of the 400^3 tank (Re
+    20000, tip speed 0.1, LES, the slab's markers of the project generator),
+    forcing plus two time steps, FP32: moments, F and Nu bit for bit."""
+    po = ref_oracle
+    edge, height = 400, 16
+    rt = po.RefRushton(edge, edge, edge, tip_speed=0.1)
+    nu = po.ref_nu(20000.0, 0.1, rt.blade_outer_radius())
+    dth = rt.increment(1)
+    j0 = int(round(edge / 3.0)) - height // 2
+
+    def slab(angle):
+        m = rt.forcing_list(angle, dth, nonupdating_delta=dth)
+        m = m[(m["j"] >= j0) & (m["j"] < j0 + height)].copy()
+        m["j"] -= j0
+        return m
+
+    flow = po.Flow(initialRho=1.0, nu=nu, cs0=0.1, g3=0.8, useLES=True)
+    lats = [po.CpuLattice(k, edge, height, edge, flow, streaming, 4) for k in ("port", "ref")]
+    mk = slab(0.0)
+    assert len(mk) > 1000
+    for L in lats:
+        L.initialise(1.0)
+        L.forcing(mk, 0.97, 1.9)
+    angle = 0.0
+    for _ in range(2):
+        angle += dth
+        mk = slab(angle)
+        for L in lats:
+            L.step(mk, 0.97, 1.9)
+    a, b = lats
+    np.testing.assert_array_equal(a.get_moments(), b.get_moments())
+    np.testing.assert_array_equal(a.interior(a.get_f()), b.interior(b.get_f()))
+    np.testing.assert_array_equal(a.interior(a.get_nu()), b.interior(b.get_nu()))
+    for L in lats:
+        L.close()
