@@ -177,22 +177,45 @@ __device__ __forceinline__ void collide_quad(float (&f)[NQ][V], const Quad& q, f
         for (int e = 0; e < V; e++) fx[e] = fy[e] = fz[e] = 0.f;
     }
     if (LES) vload<V>(Nu + q.e0, nu);
+    if constexpr (DEV && V >= 2) {
+        // 16-bit storage, several cells per thread: two cells at a time in
+        // packed FP32x2 arithmetic (the state always holds populations)
 #pragma unroll
-    for (int e = 0; e < V; e++) {
-        float qv[NQ], m[NQ];
+        for (int e = 0; e < V; e += 2) {
+            F2 qv[NQ], m[NQ];
 #pragma unroll
-        for (int d = 0; d < NQ; d++) qv[d] = f[d][e];
-        if (from_moments) {
-#pragma unroll
-            for (int d = 0; d < NQ; d++) m[d] = qv[d];
-        } else {
+            for (int d = 0; d < NQ; d++) qv[d] = f2(f[d][e], f[d][e + 1]);
             moments_of(qv, m);
-        }
-        float n = LES ? nu[e] : 0.f;
-        collide<LES, DEV, FAST>(m, fx[e], fy[e], fz[e], n, p, qv);
-        if (LES) nu[e] = n;
+            F2 n = LES ? f2(nu[e], nu[e + 1]) : f2(0.f);
+            collide<LES, DEV, FAST>(m, f2(fx[e], fx[e + 1]), f2(fy[e], fy[e + 1]), f2(fz[e], fz[e + 1]), n, p, qv);
+            if (LES) {
+                nu[e] = n.v.x;
+                nu[e + 1] = n.v.y;
+            }
 #pragma unroll
-        for (int d = 0; d < NQ; d++) f[d][e] = qv[d];
+            for (int d = 0; d < NQ; d++) {
+                f[d][e] = qv[d].v.x;
+                f[d][e + 1] = qv[d].v.y;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            float qv[NQ], m[NQ];
+#pragma unroll
+            for (int d = 0; d < NQ; d++) qv[d] = f[d][e];
+            if (from_moments) {
+#pragma unroll
+                for (int d = 0; d < NQ; d++) m[d] = qv[d];
+            } else {
+                moments_of(qv, m);
+            }
+            float n = LES ? nu[e] : 0.f;
+            collide<LES, DEV, FAST>(m, fx[e], fy[e], fz[e], n, p, qv);
+            if (LES) nu[e] = n;
+#pragma unroll
+            for (int d = 0; d < NQ; d++) f[d][e] = qv[d];
+        }
     }
 }
 

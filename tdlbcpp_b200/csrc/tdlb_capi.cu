@@ -811,7 +811,7 @@ int tdlb_config_from_json(const char* params_json, tdlb_config* out) {
 
 int tdlb_lattice_bytes(const tdlb_config* c, int64_t* bytes) {
     if (!c || !bytes || c->x < 1 || c->y < 1 || c->z < 1) return TDLB_EINVAL;
-    const long long kp = round_up(c->z, 16), kw = (kp + 31) / 32;
+    const long long kp = round_up(c->z, tdlb::kRowPitch), kw = (kp + 31) / 32;
     const long long plane = round_up(c->x * c->y * kp, 64);
     const long long mask_words = round_up(c->x * c->y * kw, 64);
     const long long esz = c->storage == TDLB_STORAGE_FP32 ? 4 : 2;

@@ -8,7 +8,8 @@
 //   * interior cells only (the reference's ghost layer is never read by the
 //     step, so it is not stored);
 //   * cell (i, j, k), 0 <= i < nx, 0 <= j < ny, 0 <= k < nz, row r = i*ny + j,
-//     element e = r*kp + k, kp = row pitch = nz rounded up to 16 floats;
+//     element e = r*kp + k, kp = row pitch = nz rounded up to kRowPitch
+//     elements (32: every FP32 row starts on a 128-byte line);
 //   * 18 population planes (SoA), each `plane` elements long and 256-byte
 //     aligned, addressed through an 18-pointer table;
 //   * F as three SoA planes (Fx, Fy, Fz), Nu as one plane, and the IBM "touched"
@@ -54,9 +55,18 @@ __host__ inline DivU31 make_div_u31(unsigned d) {
     return r;
 }
 
+// Row pitch granule in elements: 32 FP32 elements = 128 bytes, one L2 line,
+// so that every row of every plane starts on a line. (Build parameter; 16
+// gives 64-byte rows.)
+#ifndef TDLB_ROW_PITCH
+#define TDLB_ROW_PITCH 32
+#endif
+constexpr int kRowPitch = TDLB_ROW_PITCH;
+static_assert(kRowPitch % 16 == 0, "the row pitch is a multiple of 16 elements");
+
 struct Dims {
     int nx, ny, nz;     // interior extent
-    int kp;             // row pitch in elements (multiple of 16)
+    int kp;             // row pitch in elements (multiple of kRowPitch)
     int kw;             // bitmask words per row
     long long plane;    // elements per population plane (multiple of 64)
     DivU31 by_ny;       // n / ny
@@ -70,7 +80,7 @@ __host__ inline Dims make_dims(int nx, int ny, int nz) {
     g.nx = nx;
     g.ny = ny;
     g.nz = nz;
-    g.kp = (nz + 15) / 16 * 16;
+    g.kp = (nz + kRowPitch - 1) / kRowPitch * kRowPitch;
     g.kw = (g.kp + 31) / 32;
     g.plane = ((long long)nx * ny * g.kp + 63) / 64 * 64;
     g.by_ny = make_div_u31((unsigned)ny);
@@ -155,26 +165,63 @@ __host__ inline CollideParams make_collide_params(double nu, double cs0, double 
 }
 
 // ---------------------------------------------------------------------------
+// Two cells' values in one register pair, computed with Blackwell's packed
+// FP32x2 instructions (fma/add/mul .rn.f32x2: one instruction for both
+// lanes, each lane rounded as the scalar IEEE operation). The moment and
+// collision templates below take T = float (one cell) or T = F2 (two cells);
+// with T = float they are the plain scalar code. The packed form serves the
+// 16-bit storage kernels, which are bound by instruction issue rather than
+// by memory; products and sums are not contracted into FMAs there except
+// where madd() asks for one, so its rounding differs from the scalar form's
+// by FP32 ulps, far below the 16-bit storage rounding.
+// ---------------------------------------------------------------------------
+struct F2 {
+    float2 v;
+};
+__device__ __forceinline__ F2 f2(float a, float b) { return F2{make_float2(a, b)}; }
+__device__ __forceinline__ F2 f2(float a) { return F2{make_float2(a, a)}; }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2{__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator*(float s, F2 b) { return F2{__fmul2_rn(make_float2(s, s), b.v)}; }
+__device__ __forceinline__ F2 operator*(F2 a, float s) { return F2{__fmul2_rn(a.v, make_float2(s, s))}; }
+__device__ __forceinline__ F2 operator+(F2 a, float s) { return F2{__fadd2_rn(a.v, make_float2(s, s))}; }
+__device__ __forceinline__ F2 operator-(F2 a, float s) { return F2{__fadd2_rn(a.v, make_float2(-s, -s))}; }
+
+// a * b + c with one rounding
+__device__ __forceinline__ float madd(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ F2 madd(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ F2 madd(float a, F2 b, F2 c) { return F2{__ffma2_rn(make_float2(a, a), b.v, c.v)}; }
+__device__ __forceinline__ F2 madd(float a, F2 b, float c) {
+    return F2{__ffma2_rn(make_float2(a, a), b.v, make_float2(c, c))};
+}
+
+// a per-lane function of a pair
+template <typename Fn>
+__device__ __forceinline__ F2 lanewise(F2 a, Fn fn) { return F2{make_float2(fn(a.v.x), fn(a.v.y))}; }
+
+// ---------------------------------------------------------------------------
 // Moments of 18 populations (the linear map of CollisionEgglesSomers.hpp:
 // 186-256), factored through sums/differences of opposite pairs so that each
 // moment costs a few adds. m[0] = rho, m[1..3] = momentum, m[4..9] second
 // order (M05..M10), m[10..15] third order (M11..M16), m[16..17] fourth order.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void moments_of(const float* q, float* m) {
-    const float s01 = q[0] + q[1], d01 = q[0] - q[1];
-    const float s03 = q[2] + q[3], d03 = q[2] - q[3];
-    const float s05 = q[4] + q[5], d05 = q[4] - q[5];
+template <typename T>
+__device__ __forceinline__ void moments_of(const T* q, T* m) {
+    const T s01 = q[0] + q[1], d01 = q[0] - q[1];
+    const T s03 = q[2] + q[3], d03 = q[2] - q[3];
+    const T s05 = q[4] + q[5], d05 = q[4] - q[5];
     // xy edges: Q07 (+,+) Q08 (-,-) Q13 (+,-) Q14 (-,+)
-    const float xa = q[6] + q[7], xb = q[6] - q[7], xc = q[12] + q[13], xd = q[12] - q[13];
+    const T xa = q[6] + q[7], xb = q[6] - q[7], xc = q[12] + q[13], xd = q[12] - q[13];
     // xz edges: Q09 (+,+) Q10 (-,-) Q15 (+,-) Q16 (-,+)
-    const float ya = q[8] + q[9], yb = q[8] - q[9], yc = q[14] + q[15], yd = q[14] - q[15];
+    const T ya = q[8] + q[9], yb = q[8] - q[9], yc = q[14] + q[15], yd = q[14] - q[15];
     // yz edges: Q11 (+,+) Q12 (-,-) Q17 (+,-) Q18 (-,+)
-    const float za = q[10] + q[11], zb = q[10] - q[11], zc = q[16] + q[17], zd = q[16] - q[17];
+    const T za = q[10] + q[11], zb = q[10] - q[11], zc = q[16] + q[17], zd = q[16] - q[17];
 
-    const float exy = xa + xc, exz = ya + yc, eyz = za + zc;
-    const float px = xb + xd, py = xb - xd;        // xy-edge x and y momentum
-    const float qx = yb + yd, qz = yb - yd;        // xz-edge x and z momentum
-    const float ry = zb + zd, rz = zb - zd;        // yz-edge y and z momentum
+    const T exy = xa + xc, exz = ya + yc, eyz = za + zc;
+    const T px = xb + xd, py = xb - xd;        // xy-edge x and y momentum
+    const T qx = yb + yd, qz = yb - yd;        // xz-edge x and z momentum
+    const T ry = zb + zd, rz = zb - zd;        // yz-edge y and z momentum
 
     m[0] = s01 + s03 + s05 + exy + exz + eyz;
     m[1] = d01 + px + qx;
@@ -245,83 +292,97 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 }
 template <bool FAST>
 __device__ __forceinline__ float rcp_of(float x) { return FAST ? rcp_approx(x) : __frcp_rn(x); }
+template <bool FAST>
+__device__ __forceinline__ F2 rcp_of(F2 x) { return lanewise(x, [](float a) { return rcp_of<FAST>(a); }); }
+template <bool FAST>
+__device__ __forceinline__ float sqrt_abs(float x) { return FAST ? sqrt_approx(fabsf(x)) : sqrtf(fabsf(x)); }
+template <bool FAST>
+__device__ __forceinline__ F2 sqrt_abs(F2 x) { return lanewise(x, [](float a) { return sqrt_abs<FAST>(a); }); }
+template <typename T>
+__device__ __forceinline__ T splat(float a);
+template <>
+__device__ __forceinline__ float splat<float>(float a) { return a; }
+template <>
+__device__ __forceinline__ F2 splat<F2>(float a) { return f2(a); }
 
-template <bool LES, bool DEV = false, bool FAST = false>
-__device__ __forceinline__ void collide(const float* m, float fx, float fy, float fz, float& nu,
-                                        const CollideParams& p, float* out) {
-    const float rho = DEV ? m[0] + p.rho0 : m[0];
-    const float inv_rho = rcp_of<FAST>(rho);
-    const float jx = fmaf(0.5f, fx, m[1]);
-    const float jy = fmaf(0.5f, fy, m[2]);
-    const float jz = fmaf(0.5f, fz, m[3]);
-    const float ux = inv_rho * jx, uy = inv_rho * jy, uz = inv_rho * jz;
+template <bool LES, bool DEV = false, bool FAST = false, typename T = float>
+__device__ __forceinline__ void collide(const T* m, T fx, T fy, T fz, T& nu, const CollideParams& p, T* out) {
+    const T rho = DEV ? m[0] + p.rho0 : m[0];
+    const T inv_rho = rcp_of<FAST>(rho);
+    const T jx = madd(0.5f, fx, m[1]);
+    const T jy = madd(0.5f, fy, m[2]);
+    const T jz = madd(0.5f, fz, m[3]);
+    const T ux = inv_rho * jx, uy = inv_rho * jy, uz = inv_rho * jz;
 
-    float b = p.b0, c = p.c0;
+    T b, c;
     if (LES) {
         // fct = 3 / (rho (1 + 6 (Nu + nu)))       (:52)
-        const float fct = 3.f * rcp_of<FAST>(rho * fmaf(6.f, nu + p.nu, 1.f));
+        const T fct = 3.f * rcp_of<FAST>(rho * madd(6.f, nu + p.nu, 1.f));
         // literal grouping of :55-65: m + 0.5*F*u - m
-        const float dudx = fct * (fmaf(0.5f * fx, ux, m[1]) - m[4]);
-        const float dvdy = fct * (fmaf(0.5f * fy, uy, m[2]) - m[6]);
-        const float dwdz = fct * (fmaf(0.5f * fz, uz, m[3]) - m[9]);
-        const float divv = dudx + dvdy + dwdz;
-        const float sxy = 2.f * fct * (fmaf(0.5f * fy, ux, m[2]) - m[5]);
-        const float sxz = 2.f * fct * (fmaf(0.5f * fz, ux, m[3]) - m[7]);
-        const float syz = 2.f * fct * (fmaf(0.5f * fz, uy, m[3]) - m[8]);
-        const float sh = 2.f * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + sxy * sxy + sxz * sxz + syz * syz
+        const T dudx = fct * (madd(0.5f * fx, ux, m[1]) - m[4]);
+        const T dvdy = fct * (madd(0.5f * fy, uy, m[2]) - m[6]);
+        const T dwdz = fct * (madd(0.5f * fz, uz, m[3]) - m[9]);
+        const T divv = dudx + dvdy + dwdz;
+        const T sxy = 2.f * fct * (madd(0.5f * fy, ux, m[2]) - m[5]);
+        const T sxz = 2.f * fct * (madd(0.5f * fz, ux, m[3]) - m[7]);
+        const T syz = 2.f * fct * (madd(0.5f * fz, uy, m[3]) - m[8]);
+        const T sh = 2.f * (dudx * dudx + dvdy * dvdy + dwdz * dwdz) + sxy * sxy + sxz * sxz + syz * syz
                        - (2.f / 3.f) * divv * divv;
-        nu = p.cs0sq * (FAST ? sqrt_approx(fabsf(sh)) : sqrtf(fabsf(sh)));   // (:74)
-        const float nut = nu + p.nu;
-        b = rcp_of<FAST>(fmaf(6.f, nut, 1.f));
-        c = fmaf(-6.f, nut, 1.f);
+        nu = p.cs0sq * sqrt_abs<FAST>(sh);   // (:74)
+        const T nut = nu + p.nu;
+        b = rcp_of<FAST>(madd(6.f, nut, 1.f));
+        c = madd(-6.f, nut, 1.f);
+    } else {
+        b = splat<T>(p.b0);
+        c = splat<T>(p.c0);
     }
 
     constexpr float r24 = 1.f / 24.f;
-    const float a0 = m[0] * r24;
-    const float a1 = (m[1] + fx) * r24;
-    const float a2 = (m[2] + fy) * r24;
-    const float a3 = (m[3] + fz) * r24;
-    const float br = b * r24;
-    const float a4 = (2.f * jx * ux - m[4] * c) * br;
-    const float a5 = (2.f * jx * uy - m[5] * c) * br;
-    const float a6 = (2.f * jy * uy - m[6] * c) * br;
-    const float a7 = (2.f * jx * uz - m[7] * c) * br;
-    const float a8 = (2.f * jy * uz - m[8] * c) * br;
-    const float a9 = (2.f * jz * uz - m[9] * c) * br;
-    const float g = -p.g3 * r24;
-    const float a10 = g * m[10], a11 = g * m[11], a12 = g * m[12];
-    const float a13 = g * m[13], a14 = g * m[14], a15 = g * m[15];
+    const T a0 = m[0] * r24;
+    const T a1 = (m[1] + fx) * r24;
+    const T a2 = (m[2] + fy) * r24;
+    const T a3 = (m[3] + fz) * r24;
+    const T br = b * r24;
+    const T a4 = (2.f * jx * ux - m[4] * c) * br;
+    const T a5 = (2.f * jx * uy - m[5] * c) * br;
+    const T a6 = (2.f * jy * uy - m[6] * c) * br;
+    const T a7 = (2.f * jx * uz - m[7] * c) * br;
+    const T a8 = (2.f * jy * uz - m[8] * c) * br;
+    const T a9 = (2.f * jz * uz - m[9] * c) * br;
+    const float g = -p.g3 * r24;   // scalar constant
+    const T a10 = g * m[10], a11 = g * m[11], a12 = g * m[12];
+    const T a13 = g * m[13], a14 = g * m[14], a15 = g * m[15];
 
     // faces
-    const float e01 = 2.f * a0 + 3.f * (a4 - a6 - a9);
-    const float o01 = 4.f * a1 - 2.f * (a10 + a12);
+    const T e01 = 2.f * a0 + 3.f * (a4 - a6 - a9);
+    const T o01 = 4.f * a1 - 2.f * (a10 + a12);
     out[0] = e01 + o01;
     out[1] = e01 - o01;
-    const float e03 = 2.f * a0 + 3.f * (a6 - a4 - a9);
-    const float o03 = 4.f * a2 - 2.f * (a11 + a13);
+    const T e03 = 2.f * a0 + 3.f * (a6 - a4 - a9);
+    const T o03 = 4.f * a2 - 2.f * (a11 + a13);
     out[2] = e03 + o03;
     out[3] = e03 - o03;
-    const float e05 = 2.f * a0 + 3.f * (a9 - a4 - a6);
-    const float o05 = 4.f * (a3 - a14);
+    const T e05 = 2.f * a0 + 3.f * (a9 - a4 - a6);
+    const T o05 = 4.f * (a3 - a14);
     out[4] = e05 + o05;
     out[5] = e05 - o05;
     // xy edges: Q07 (+x+y) Q14 (-x+y) Q08 (-x-y) Q13 (+x-y)
-    const float exy = a0 + 1.5f * (a4 + a6 - a9);
-    const float X = 2.f * (a1 + a10), Y = 2.f * (a2 + a11), Z = 6.f * a5;
+    const T exy = a0 + 1.5f * (a4 + a6 - a9);
+    const T X = 2.f * (a1 + a10), Y = 2.f * (a2 + a11), Z = 6.f * a5;
     out[6] = exy + X + Y + Z;
     out[13] = exy - X + Y - Z;
     out[7] = exy - X - Y + Z;
     out[12] = exy + X - Y - Z;
     // xz edges: Q09 (+x+z) Q16 (-x+z) Q10 (-x-z) Q15 (+x-z)
-    const float exz = a0 + 1.5f * (a4 - a6 + a9);
-    const float Xp = 2.f * a1 - a10 + a12, Zp = 2.f * a3 + a14 - a15, W = 6.f * a7;
+    const T exz = a0 + 1.5f * (a4 - a6 + a9);
+    const T Xp = 2.f * a1 - a10 + a12, Zp = 2.f * a3 + a14 - a15, W = 6.f * a7;
     out[8] = exz + Xp + Zp + W;
     out[15] = exz - Xp + Zp - W;
     out[9] = exz - Xp - Zp + W;
     out[14] = exz + Xp - Zp - W;
     // yz edges: Q11 (+y+z) Q18 (-y+z) Q12 (-y-z) Q17 (+y-z)
-    const float eyz = a0 + 1.5f * (a6 - a4 + a9);
-    const float Yp = 2.f * a2 - a11 + a13, Zq = 2.f * a3 + a14 + a15, Wp = 6.f * a8;
+    const T eyz = a0 + 1.5f * (a6 - a4 + a9);
+    const T Yp = 2.f * a2 - a11 + a13, Zq = 2.f * a3 + a14 + a15, Wp = 6.f * a8;
     out[10] = eyz + Yp + Zq + Wp;
     out[17] = eyz - Yp + Zq - Wp;
     out[11] = eyz - Yp - Zq + Wp;

@@ -114,3 +114,37 @@ def test_submit_from_threads_and_close_with_work_pending(gpu):
         t.join()
     time.sleep(0.02)
     s.close()                                # unfinished requests end, the worker stops
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_served_request_vs_restatement(gpu, port_oracle, streaming):
+    """One FP32 request (24^3, tip 0.1, Re 7300, 30 steps) served, against the
+    CPU restatement of the same tank with the server's set-up (nu from
+    calcNuAndRe_m of the blade radius, cs0 0.1, LES, impeller attached at
+    increment(1) and advanced by increment(s) per step): density and velocity
+    within 1e-4 relative L2, the single-tank parity tolerance."""
+    tb, po = gpu, port_oracle
+    edge, tip, re, steps = 24, 0.1, 7300.0, 30
+    with tb.Server(chunk_steps=8) as s:
+        s.submit(7, edge, tip, re, steps, storage="fp32", streaming=streaming, fields=True)
+        r = collect(s, 1)[7]
+    assert r["status"] == 0
+    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=tip, startup_steps=0)
+    nu = tb.nu_from_reynolds(re, tip, rt.blade_outer_radius())
+    lat = po.CpuLattice("port", edge, edge, edge, po.Flow(initialRho=1.0, nu=nu, cs0=0.1, g3=0.8, useLES=True),
+                        streaming, 4)
+    d1 = rt.increment(1)
+    lat.initialise(1.0)
+    lat.forcing(rt.forcing_list(d1, d1, nonupdating_delta=d1), 0.97, 1.9)
+    angle = d1
+    for st in range(2, steps + 2):
+        d = rt.increment(st)
+        angle += d
+        lat.step(rt.forcing_list(angle, d, nonupdating_delta=d1), 0.97, 1.9)
+    m, f = lat.get_moments(), lat.interior(lat.get_f())
+    lat.close()
+    rho0 = m[..., 0]
+    u0 = (m[..., 1:4] + 0.5 * f) / rho0[..., None]
+    u = np.stack([r["fields"]["ux"], r["fields"]["uy"], r["fields"]["uz"]], axis=-1)
+    assert rel_l2(r["fields"]["rho"], rho0) <= 1e-4
+    assert rel_l2(u, u0) <= 1e-4
