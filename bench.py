@@ -341,7 +341,7 @@ def run_batched(args, rank, world, device):
 
     torch.cuda.set_device(device)
     tanks = draw_batched_tanks()
-    rts, cfgs = batched_configs(tb, tanks)
+    rts, cfgs = batched_configs(tb, tanks, storage=args.storage)
     cells = sum(e ** 3 for e, _, _ in tanks)
     b = tb.Batch(cfgs, device=device)
     stream = torch.cuda.ExternalStream(b.stream(), device=device)
@@ -858,21 +858,61 @@ def max_over_ranks(x, world):
     return float(x)
 
 
+BATCH_ERROR_STEPS = 1000
+
+
+def batched_error(tb, tanks, storage, device, count=2, steps=BATCH_ERROR_STEPS):
+    """Velocity error of the `count` smallest tanks of the batched workload
+    after `steps` batched steps (the workload's step count), against the FP64
+    CPU restatement of each tank (host threads) with the batch's impeller
+    schedule: relative L2 per tank."""
+    from oracle import pyoracle as po
+    picked = sorted(range(len(tanks)), key=lambda t: tanks[t][0])[:count]
+    sub = [tanks[t] for t in picked]
+    rts, cfgs = batched_configs(tb, sub, storage=storage)
+    with tb.Batch(cfgs, device=device) as b:
+        for cu, rt in zip(b.tanks, rts):
+            prepare_tank(cu, rt)
+        b.run(steps, ALPHA, BETA)
+        got = [cu.read_velocity_density()[1].astype(np.float64) for cu in b.tanks]
+    po.load("port").tdlbo_set_threads(max(1, min(64, os.cpu_count() or 1)))
+    out = []
+    for (edge, tip, re), rt, cfg, u in zip(sub, rts, cfgs, got):
+        lat = po.CpuLattice("port", edge, edge, edge, po.Flow(initialRho=1.0, nu=cfg["nu"], cs0=0.1, g3=0.8,
+                                                              alpha=ALPHA, beta=BETA, useLES=True), "Esotwist", 8)
+        d1 = rt.increment(1)
+        lat.initialise(1.0)
+        lat.forcing(rt.forcing_list(d1, d1, nonupdating_delta=d1), ALPHA, BETA)
+        angle = d1
+        for s in range(2, steps + 2):
+            d = rt.increment(s)
+            angle += d
+            lat.step(rt.forcing_list(angle, d, nonupdating_delta=d1), ALPHA, BETA)
+        m, f = lat.get_moments(), lat.interior(lat.get_f())
+        lat.close()
+        uref = (m[..., 1:4] + 0.5 * f) / m[..., 0:1]
+        out.append({"edge": edge, "tip": tip, "re": re, "steps": steps, "u_rel_l2_vs_fp64": rel(u, uref)})
+    return out
+
+
 def report_batched(args, rank, world, local, config):
     res = run_batched(args, rank, world, local)
     if rank != 0:
         return 0
     peak, peak_kind = measured_peak()
-    bpc = 152
+    bpc = 152 if args.storage == "fp32" else 80
     achieved = bpc * res["cells"] / (res["kernel_ms"] / 1e3) / 1e9
     v, nt, bps = res["shape"]
+    if args.storage != "fp32" and not args.no_cpu_baseline:
+        import tdlbcpp_b200 as tb
+        config = dict(config, error_vs_fp64=batched_error(tb, draw_batched_tanks(), args.storage, local))
     config = dict(config, shape={"cells_per_thread": v, "threads": nt, "blocks_per_sm": bps},
                   sequential_plain_mlups=res["seq_mlups"], sequential_steps_per_tank=res["seq_steps"],
                   single_step_ms=res["step_ms_single"])
     line = {
         "metric": "MLUPS", "value": res["value_mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "fp32",
+        "vs_baseline": None, "dtype": "fp32" if args.storage == "fp32" else f"fp32 arithmetic, {args.storage} storage",
         "data": "synthetic", "config": config,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "kernel": "k_batch_step", "bytes_per_cell": bpc,
@@ -925,7 +965,7 @@ def main():
                   "l2": "lattices > L2 (no flush needed)"}
     elif args.workload == "batched":
         tanks = draw_batched_tanks()
-        workload = f"batched-{len(tanks)}-tanks-esotwist-fp32-les"
+        workload = f"batched-{len(tanks)}-tanks-esotwist-{args.storage}-les"
         config = {"workload": workload, "tanks": len(tanks), "edges": [t[0] for t in tanks],
                   "cells": sum(t[0] ** 3 for t in tanks), "seed": BATCH_SEED,
                   "draw": "edge U{32,48,64,96,128}, tip U[0.05,0.12], Re log-U[1e3,2e4] per tank, in that order",

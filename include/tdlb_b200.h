@@ -250,9 +250,29 @@ int tdlb_checkpoint_write(tdlb_handle h, const char* dir, const char* unit_name,
 int tdlb_checkpoint_read(tdlb_handle h, const char* dir, const char* unit_name);
 
 /* Step-kernel variant: cells per thread (1, 2 or 4 -- float2 / float4
- * traffic; default 1, the fastest on B200 for both schemes). All variants
- * compute identical results. */
+ * traffic; default 1, the fastest on B200 for both schemes). FP32 storage:
+ * all variants compute identical results; 16-bit storage: 2 and 4 cells per
+ * thread use packed FP32x2 arithmetic (results within FP32 rounding). Not
+ * while a residual box is set (TDLB_ESTATE). */
 int tdlb_set_cells_per_thread(tdlb_handle h, int v);
+
+/* Residual box of the 16-bit storage forms (no counterpart in the
+ * reference, whose storage is FP32). For every population location of the
+ * cells [i0, i1) x [j0, j1) x [k0, k1) the library keeps, beside the 16-bit
+ * deviation, the FP32 residual of its rounding, so these locations are
+ * stored exactly: the stirred tank's velocity error against FP64 comes
+ * mostly from the 16-bit rounding in the impeller's swept volume. The box
+ * costs 72 (Esotwist) or 144 (Simple) bytes of device memory per box cell
+ * and traffic only there. tdlb_attach_rushton sets it over the blades'
+ * swept volume with a 4-cell margin, unless a box was set (or removed) with
+ * this call; an empty box (i1 <= i0) removes it. Requires 16-bit storage
+ * (TDLB_EINVAL), one cell per thread and a lattice outside a batch
+ * (TDLB_ESTATE; a lattice joining a batch loses its box), and i0, j0, k0 >= 1.
+ * Read-back (moments, velocity), the forcing pass and the FP64 sums include
+ * the residuals. */
+int tdlb_set_residual_box(tdlb_handle h, int64_t i0, int64_t i1, int64_t j0, int64_t j1, int64_t k0, int64_t k1);
+/* The current box as {i0, i1, j0, j1, k0, k1} (all zero: none). */
+int tdlb_get_residual_box(tdlb_handle h, int64_t* box6);
 
 /* Split steps. mode 0 (default): off; 1: on when the inner chunks hold at
  * most 60 % of the lattice (large tanks; a small one is mostly stencil

@@ -217,6 +217,8 @@ def load_library() -> ctypes.CDLL:
         "tdlb_impeller_load_async": (i32, [H, vp]),
         "tdlb_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "tdlb_set_cells_per_thread": (i32, [H, i32]),
+        "tdlb_set_residual_box": (i32, [H] + [ctypes.c_int64] * 6),
+        "tdlb_get_residual_box": (i32, [H, vp]),
         "tdlb_set_overlap": (i32, [H, i32]),
         "tdlb_join": (i32, [H]),
         "tdlb_read_zone": (i32, [H, vp]),
@@ -459,8 +461,19 @@ class ComputeUnit:
         return q, f
 
     def set_cells_per_thread(self, v: int):
-        """Step-kernel variant (1, 2 or 4 cells per thread); results are identical."""
+        """Step-kernel variant (1, 2 or 4 cells per thread)."""
         self._check(self.lib.tdlb_set_cells_per_thread(self.h, v))
+
+    def set_residual_box(self, i0: int, i1: int, j0: int, j1: int, k0: int, k1: int):
+        """16-bit storage: keep the locations of the box [i0,i1) x [j0,j1) x [k0,k1)
+        exact (an empty box removes it; tdlb_set_residual_box)."""
+        self._check(self.lib.tdlb_set_residual_box(self.h, i0, i1, j0, j1, k0, k1))
+
+    def residual_box(self):
+        """(i0, i1, j0, j1, k0, k1) of the residual box, all zero without one."""
+        out = np.zeros(6, np.int64)
+        self._check(self.lib.tdlb_get_residual_box(self.h, _p(out)))
+        return tuple(int(v) for v in out)
 
     def set_overlap(self, mode):
         """Split steps: the outer cells of a step run while the previous

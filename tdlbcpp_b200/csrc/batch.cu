@@ -595,6 +595,9 @@ void adopt_tank(tdlb_batch_s* b, tdlb_lattice* h) {
     if (h->cfg.streaming != b->streaming || h->cfg.storage != b->storage)
         throw BFail{TDLB_EINVAL, "all tanks of a batch share one streaming scheme and one storage precision"};
     if (h->device != b->device) throw BFail{TDLB_EINVAL, "the lattice lives on another device"};
+    // the batched step keeps no 16-bit residuals: the tank continues at its
+    // storage precision everywhere
+    tdlb_rt::drop_residual_box(h);
     tdlb_rt::borrow_stream(h, b->stream);
     h->vec = b->vec;
     b->tanks.push_back(h);

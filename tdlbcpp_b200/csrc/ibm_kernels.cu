@@ -76,7 +76,7 @@ __device__ __forceinline__ float ld_state(const float* plane, long long e) {
 // rho and momentum of the state at interior cell (i, j, k).
 template <typename S>
 __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int even, const Dims& g, int i, int j, int k,
-                                              const CollideParams& p, float* m4) {
+                                              const CollideParams& p, float* m4, const ResidualBox& rb) {
     if (mode == 1) {
         const long long e = ((long long)i * g.ny + j) * g.kp + k;
 #pragma unroll
@@ -91,6 +91,10 @@ __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int eve
             const bool in = (unsigned)si < (unsigned)g.nx && (unsigned)sj < (unsigned)g.ny && (unsigned)sk < (unsigned)g.nz;
             const long long src = in ? ((long long)si * g.ny + sj) * g.kp + sk : ((long long)i * g.ny + j) * g.kp + k;
             q[d] = ld_state<S>(A.p[d], src) + (Storage<S>::deviation ? (is_face(d) ? p.wface : p.wedge) : 0.f);
+            if (Storage<S>::deviation && rb.on()) {   // residual box: the exact deviation
+                const int li = in ? si : i, lj = in ? sj : j, lk = in ? sk : k;
+                if (rb.contains(li, lj, lk)) q[d] += *rb.at(d, li, lj, lk);
+            }
         }
         moments4_of(q, m4);
         return;
@@ -105,6 +109,8 @@ __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int eve
         const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
         q[d] = ld_state<S>(A.p[s], ((long long)(oi ? i1 : i) * g.ny + (oj ? j1 : j)) * g.kp + (ok ? k1 : k)) +
                (mode == 2 && Storage<S>::deviation ? (is_face(d) ? p.wface : p.wedge) : 0.f);
+        if (Storage<S>::deviation && mode == 2 && rb.on() && rb.contains(oi ? i1 : i, oj ? j1 : j, ok ? k1 : k))
+            q[d] += *rb.at(s, oi ? i1 : i, oj ? j1 : j, ok ? k1 : k);
     }
     if (mode == 3) {
 #pragma unroll
@@ -145,7 +151,7 @@ __device__ __forceinline__ void ibm_cell(const IbmArgs& a, int c) {
     const int i = row / g.ny;
     const int j = row - i * g.ny;
     float m4[4];
-    cell_moments4<S>(a.A, a.state_mode, a.even, g, i, j, k, a.p, m4);
+    cell_moments4<S>(a.A, a.state_mode, a.even, g, i, j, k, a.p, m4, a.rbox);
     const long long C = a.ncell;
 #pragma unroll
     for (int s = 0; s < 4; s++) a.cell_m[s * C + c] = m4[s];
@@ -178,7 +184,7 @@ __device__ __forceinline__ void ibm_tail_marker(const IbmArgs& a, int t) {
             const float w = stencil_weight(mk.iCartFraction, mk.kCartFraction, i1, k1);
             const int i2 = wrap_i(i + i1, a.g.nx), k2 = wrap_i(k + k1, a.g.nz);
             float m4[4];
-            cell_moments4<S>(a.A, a.state_mode, a.even, a.g, i2, j, k2, a.p, m4);
+            cell_moments4<S>(a.A, a.state_mode, a.even, a.g, i2, j, k2, a.p, m4, a.rbox);
             s[(TF_W + c) * cap + t] = w;
             s[(TF_RHO + c) * cap + t] = m4[0];
             s[(TF_MX + c) * cap + t] = m4[1];
@@ -198,16 +204,79 @@ __global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
     if (t < a.n - a.n0) ibm_tail_marker<S>(a, t);
 }
 
+// Bulk asynchronous copies global -> shared memory with an mbarrier
+// (cp.async.bulk, no multicast): one thread issues them, the group waits on
+// the barrier's transaction count. Source and destination 16-byte aligned,
+// sizes a multiple of 16 bytes.
+__device__ unsigned g_ibm_bulk_timeouts = 0;   // waits that gave up (then the tile is loaded by plain loads)
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, unsigned bytes) {
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }" ::"r"(smem_addr(bar)),
+                 "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+// Wait for phase 0 of the barrier, at most `limit` polls; false when it gave up.
+__device__ __forceinline__ bool mbar_wait0(uint64_t* bar, int limit) {
+    for (int it = 0; it < limit; it++) {
+        unsigned done;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(smem_addr(bar)) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// The 16-byte aligned span of elements [c0, c0 + n) of a 4-byte array:
+// the first element copied, its offset from c0 and the bytes to copy.
+struct BulkSpan {
+    const void* src;
+    int off;
+    unsigned bytes;
+};
+__device__ __forceinline__ BulkSpan bulk_span(const void* base, int c0, int n) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(base) + 4ull * (unsigned)c0;
+    const uintptr_t lo = a & ~uintptr_t(15), hi = (a + 4ull * (unsigned)n + 15) & ~uintptr_t(15);
+    return BulkSpan{reinterpret_cast<const void*>(lo), (int)((a - lo) >> 2), (unsigned)(hi - lo)};
+}
+
+// A group of NT threads (whole warps) that walks one j-plane. Several groups
+// can share a CTA, each synchronising on its own named barrier (bar.sync id,
+// NT), so that the planes of one CTA advance independently; a group that is
+// the whole CTA uses barrier 0 (__syncthreads).
+template <int NT, bool NAMED = false>
+struct PlaneGroup {
+    int base;  // the group's first thread in the CTA
+    int bar;   // named barrier id (NAMED), else the CTA barrier
+    // thread index within the group (read from threadIdx each time, so that
+    // it occupies no register of the register-bound walks)
+    __device__ __forceinline__ int tid() const { return NAMED ? (int)threadIdx.x - base : (int)threadIdx.x; }
+    __device__ __forceinline__ void sync() const {
+        if constexpr (NAMED) asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(NT) : "memory");
+        else __syncthreads();
+    }
+};
+
 // Blade levels of plane j on global memory: F and the touched flags are
 // read back from L2 (__ldcg), since earlier levels of this CTA wrote them.
-// Used when the plane's blade stencils do not fit the shared-memory table.
-__device__ __forceinline__ void blade_levels_global(const IbmArgs& a, int j) {
+// Used when the plane's blade stencils do not fit the shared-memory table;
+// a called function rather than inlined, so that this rare fallback costs
+// the register-bound walks around it no registers.
+template <int NT, typename GRP>
+__device__ __noinline__ void blade_levels_global(const IbmArgs& a, int j, const GRP grp) {
     const Dims g = a.g;
     const float* s = a.tail;
     const long long cap = a.tail_cap;
     for (int lv = a.plane_lv1[j]; lv < a.plane_lv1[j + 1]; lv++) {
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
-        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+#pragma unroll 1
+        for (int p = p0 + grp.tid(); p < p1; p += NT) {
             const int t = p - a.n0;
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
 #pragma unroll
@@ -253,7 +322,7 @@ __device__ __forceinline__ void blade_levels_global(const IbmArgs& a, int j) {
                 atomicOr(&a.mask_new[wd], bit);
             }
         }
-        __syncthreads();
+        grp.sync();
     }
 }
 
@@ -267,8 +336,9 @@ __device__ __forceinline__ void blade_levels_global(const IbmArgs& a, int j) {
 // values in the same order as blade_levels_global; only the L2 round trips
 // between levels go. Needs 4 H + 9 nb words of `tile`; returns false, having
 // done nothing, when they do not fit.
-template <int THREADS>
-__device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float* tile, int tile_words) {
+template <int THREADS, typename GRP>
+__device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float* tile, int tile_words,
+                                                  const GRP grp) {
     const int lv0 = a.plane_lv1[j], lv1 = a.plane_lv1[j + 1];
     const int q0 = a.level_ptr[lv0], q1 = a.level_ptr[lv1];
     const int nref = 9 * (q1 - q0);
@@ -286,9 +356,9 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
     const long long cap = a.tail_cap;
     const bool distinct = g.nx >= 3 && g.nz >= 3;   // the 9 stencil cells of a marker differ
 
-    for (int h = threadIdx.x; h < H; h += THREADS) keys[h] = -1;
-    __syncthreads();
-    for (int r = threadIdx.x; r < nref; r += THREADS) {
+    for (int h = grp.tid(); h < H; h += THREADS) keys[h] = -1;
+    grp.sync();
+    for (int r = grp.tid(); r < nref; r += THREADS) {
         const int m = r / 9, c = r - 9 * m;
         const int key = __float_as_int(s[(TF_CELL + c) * cap + (q0 + m - a.n0)]);
         unsigned h = ((unsigned)key * 2654435761u) >> (32 - lg);
@@ -299,8 +369,8 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
         }
         ref[r] = (int)h;
     }
-    __syncthreads();
-    for (int h = threadIdx.x; h < H; h += THREADS) {
+    grp.sync();
+    for (int h = grp.tid(); h < H; h += THREADS) {
         const int key = keys[h];
         if (key < 0) continue;
         const int i2 = key >> 16, k2 = key & 0xffff;
@@ -313,10 +383,11 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
         hy[h] = live ? __ldcg(a.Fy + e) : 0.f;
         hz[h] = live ? __ldcg(a.Fz + e) : 0.f;
     }
-    __syncthreads();
+    grp.sync();
     for (int lv = lv0; lv < lv1; lv++) {
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
-        for (int p = p0 + threadIdx.x; p < p1; p += THREADS) {
+#pragma unroll 1
+        for (int p = p0 + grp.tid(); p < p1; p += THREADS) {
             const int t = p - a.n0;
             const int* rf = ref + 9 * (p - q0);
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
@@ -358,9 +429,9 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
                 }
             }
         }
-        __syncthreads();
+        grp.sync();
     }
-    for (int h = threadIdx.x; h < H; h += THREADS) {
+    for (int h = grp.tid(); h < H; h += THREADS) {
         const int key = keys[h];
         if (key < 0) continue;
         const int i2 = key >> 16, k2 = key & 0xffff;
@@ -380,15 +451,56 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
 // table when they fit the tile, else on global F. The touched flags of the
 // first segment never change, so each pass starts mask_new as a copy of them
 // (mask_static) and the blade walk adds its cells.
-template <int THREADS>
-__device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int tile_cells, float* tile) {
+// BULK: the group's tile is [4][tile_cells + 8] words (F x, y, z and the
+// cells' elements), filled by bulk copies of the plane's cell range (bar:
+// the group's mbarrier); the write-back then takes the elements from shared
+// memory. Otherwise the tile is [3][tile_cells] and filled by plain loads.
+template <int THREADS, bool BULK = false, typename GRP = PlaneGroup<THREADS>>
+__device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int tile_cells, float* tile, const GRP grp,
+                                                 uint64_t* bar = nullptr, int* bulk_fail = nullptr) {
     const int c0 = a.plane_cell[j], nc = a.plane_cell[j + 1] - c0;
     const long long C = a.ncell;
     const bool in_smem = nc <= tile_cells;
     float *fx, *fy, *fz;
-    if (in_smem) {
+    const int* ce = nullptr;   // BULK: the cells' elements in shared memory
+    if (BULK && in_smem && nc > 0) {
+        const int tc = tile_cells + 8;
+        const BulkSpan sx = bulk_span(a.cell_F + c0, 0, nc), sy = bulk_span(a.cell_F + C + c0, 0, nc),
+                       sz = bulk_span(a.cell_F + 2 * C + c0, 0, nc), se = bulk_span(a.cell_e + c0, 0, nc);
+        if (grp.tid() == 0) {
+            mbar_init(bar);
+            *bulk_fail = 0;
+        }
+        grp.sync();
+        if (grp.tid() == 0) {
+            mbar_expect(bar, sx.bytes + sy.bytes + sz.bytes + se.bytes);
+            bulk_to_smem(tile, sx.src, sx.bytes, bar);
+            bulk_to_smem(tile + tc, sy.src, sy.bytes, bar);
+            bulk_to_smem(tile + 2 * tc, sz.src, sz.bytes, bar);
+            bulk_to_smem(tile + 3 * tc, se.src, se.bytes, bar);
+        }
+        fx = tile + sx.off; fy = tile + tc + sy.off; fz = tile + 2 * tc + sz.off;
+        ce = reinterpret_cast<const int*>(tile + 3 * tc) + se.off;
+        // bounded wait; the group decides together whether it gave up, so
+        // that every thread takes the same barriers
+        if (!mbar_wait0(bar, 1 << 20)) *bulk_fail = 1;
+        grp.sync();
+        if (*bulk_fail) {
+            // should not happen: count it, give the copies more time, then
+            // load the tile with plain loads
+            if (grp.tid() == 0) atomicAdd(&g_ibm_bulk_timeouts, 1u);
+            mbar_wait0(bar, 1 << 22);
+            grp.sync();
+            for (int t = grp.tid(); t < nc; t += THREADS) {
+                fx[t] = a.cell_F[c0 + t];
+                fy[t] = a.cell_F[C + c0 + t];
+                fz[t] = a.cell_F[2 * C + c0 + t];
+                reinterpret_cast<int*>(tile + 3 * tc)[se.off + t] = a.cell_e[c0 + t];
+            }
+        }
+    } else if (in_smem) {
         fx = tile; fy = tile + tile_cells; fz = tile + 2 * tile_cells;
-        for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+        for (int t = grp.tid(); t < nc; t += THREADS) {
             fx[t] = a.cell_F[c0 + t];
             fy[t] = a.cell_F[C + c0 + t];
             fz[t] = a.cell_F[2 * C + c0 + t];
@@ -396,7 +508,7 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
     } else {
         fx = a.cell_F + c0; fy = a.cell_F + C + c0; fz = a.cell_F + 2 * C + c0;
     }
-    __syncthreads();
+    grp.sync();
 
     // ---- first segment: each marker in list order relative to every marker
     //      it shares a cell with (level walk). With x and z at least 3 the 9
@@ -410,7 +522,8 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
     const float* mz = a.cell_m + 3 * C + c0;
     for (int lv = a.plane_lv0[j]; lv < a.plane_lv0[j + 1]; lv++) {
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
-        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+#pragma unroll 1
+        for (int p = p0 + grp.tid(); p < p1; p += THREADS) {
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
             float w[9], ox[9], oy[9], oz[9];
             int li[9];
@@ -455,27 +568,53 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
                 }
             }
         }
-        __syncthreads();
+        grp.sync();
     }
     // ---- write the plane's cells back to F
-    for (int t = threadIdx.x; t < nc; t += blockDim.x) {
-        const int e = a.cell_e[c0 + t];
+    for (int t = grp.tid(); t < nc; t += THREADS) {
+        const int e = BULK && ce ? ce[t] : a.cell_e[c0 + t];
         a.Fx[e] = fx[t];
         a.Fy[e] = fy[t];
         a.Fz[e] = fz[t];
     }
-    __syncthreads();
+    grp.sync();
 
     // ---- second segment (blades)
     if (a.plane_lv1[j] == a.plane_lv1[j + 1]) return;
-    if (!blade_levels_tile<THREADS>(a, j, tile, 3 * tile_cells)) blade_levels_global(a, j);
+    const int words = BULK ? 4 * (tile_cells + 8) : 3 * tile_cells;
+    if (!blade_levels_tile<THREADS>(a, j, tile, words, grp)) blade_levels_global<THREADS>(a, j, grp);
 }
 
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes,
-                                                                       int tile_cells) {
-    extern __shared__ float tile[];                             // [3][tile_cells]
-    ibm_spread_plane<THREADS>(a, planes[blockIdx.x], tile_cells, tile);
+// G planes per CTA, NT threads each: group g walks plane planes[blockIdx.x *
+// G + g] on its own F tile (G x 3 x tile_cells floats of shared memory) with
+// its own barrier.
+template <int NT, int G>
+__global__ void __launch_bounds__(NT * G, 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes, int nplanes,
+                                                         int tile_cells) {
+    extern __shared__ float tile[];                             // [G][3][tile_cells]
+    const int g = G == 1 ? 0 : (int)threadIdx.x / NT;
+    const int q = (int)blockIdx.x * G + g;
+    if (q >= nplanes) return;                                   // the whole group: no barrier is left waiting
+    const PlaneGroup<NT, (G > 1)> grp{g * NT, g + 1};
+    ibm_spread_plane<NT>(a, planes[q], tile_cells, tile + (size_t)g * 3 * tile_cells, grp);
+}
+
+// The ordinary planes, G per CTA: group g (NT threads, its own barrier)
+// walks plane planes[blockIdx.x * G + g] on its own tile, which bulk copies
+// fill with one latency whatever the group's size. G planes then share an
+// SM, so all planes of a large lattice are resident at once.
+template <int NT, int G>
+__global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_bulk(IbmArgs a, const int* __restrict__ planes, int nplanes,
+                                                              int tile_cells) {
+    extern __shared__ __align__(128) float btile[];             // [G][4][tile_cells + 8]
+    __shared__ uint64_t bars[G];
+    __shared__ int fails[G];
+    const int g = G == 1 ? 0 : (int)threadIdx.x / NT;
+    const int q = (int)blockIdx.x * G + g;
+    if (q >= nplanes) return;
+    const PlaneGroup<NT, (G > 1)> grp{g * NT, g + 1};
+    ibm_spread_plane<NT, true>(a, planes[q], tile_cells, btile + (size_t)g * 4 * (tile_cells + 8), grp, &bars[g],
+                               &fails[g]);
 }
 
 // Impeller rotation on the device: recomputes the blade markers of the
@@ -581,7 +720,7 @@ __global__ void __launch_bounds__(256) k_reduce_fp64(IbmArgs a, const uint32_t* 
         const long long row = t / g.nz;
         const int j = (int)(row % g.ny), i = (int)(row / g.ny);
         float m4[4];
-        cell_moments4<S>(a.A, a.state_mode, a.even, g, i, j, k, a.p, m4);
+        cell_moments4<S>(a.A, a.state_mode, a.even, g, i, j, k, a.p, m4, a.rbox);
         const long long e = row * g.kp + k;
         const bool on = (mask[row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
         acc[0] += m4[0];
@@ -653,8 +792,32 @@ cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
     return e;
 }
 
-cudaError_t ibm_prepare_smem(size_t bytes) {
-    return raise_smem_limit((const void*)k_ibm_spread<512>, bytes);
+// Ordinary planes per CTA: as many 128-thread groups as their tiles (F and
+// the cell elements, 16 bytes per cell) fit in the 227 KB of shared memory a
+// CTA may use, at most 4.
+int spread_groups(int tile_cells) {
+    const size_t per = (size_t)16 * (tile_cells + 8);
+    const int G = (int)((227 * 1024 - 64) / per);
+    return G < 1 ? 1 : (G > 4 ? 4 : G);
+}
+
+template <int G>
+static const void* spread_bulk_fn() { return (const void*)k_ibm_spread_bulk<128, G>; }
+
+template <int G>
+static void spread_small(const IbmArgs& a, cudaStream_t st) {
+    const unsigned grid = (unsigned)((a.n_small + G - 1) / G);
+    const size_t bytes = (size_t)G * 16 * (a.smem_cells + 8);
+    k_ibm_spread_bulk<128, G><<<grid, 128 * G, bytes, st>>>(a, a.plane_list, a.n_small, a.smem_cells);
+}
+
+cudaError_t ibm_prepare_smem(int small_cells, size_t big_bytes) {
+    const int G = spread_groups(small_cells);
+    const void* fn = G == 4 ? spread_bulk_fn<4>() : G == 3 ? spread_bulk_fn<3>() : G == 2 ? spread_bulk_fn<2>()
+                                                                                       : spread_bulk_fn<1>();
+    cudaError_t e = raise_smem_limit(fn, (size_t)G * 16 * (small_cells + 8));
+    if (e != cudaSuccess) return e;
+    return raise_smem_limit((const void*)k_ibm_spread<512, 1>, big_bytes);
 }
 
 cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, cudaStream_t st) {
@@ -691,16 +854,22 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
         if (err != cudaSuccess) return err;
         err = cudaStreamWaitEvent(a.side, a.ev_fork, 0);
         if (err != cudaSuccess) return err;
-        k_ibm_spread<512><<<a.n_big, 512, ibm_smem_bytes(a.g, a.big_tile_cells), a.side>>>(a, a.plane_list + a.n_small,
-                                                                                           a.big_tile_cells);
+        k_ibm_spread<512, 1><<<a.n_big, 512, ibm_smem_bytes(a.g, a.big_tile_cells), a.side>>>(
+            a, a.plane_list + a.n_small, a.n_big, a.big_tile_cells);
         err = cudaGetLastError();
         if (err != cudaSuccess) return err;
         err = cudaEventRecord(a.ev_join, a.side);
         if (err != cudaSuccess) return err;
     }
     if (split) cells(a.ncell_big, a.ncell - a.ncell_big);
-    if (a.n_small > 0)
-        k_ibm_spread<512><<<a.n_small, 512, ibm_smem_bytes(a.g, a.smem_cells), st>>>(a, a.plane_list, a.smem_cells);
+    if (a.n_small > 0) {
+        switch (spread_groups(a.smem_cells)) {
+            case 4: spread_small<4>(a, st); break;
+            case 3: spread_small<3>(a, st); break;
+            case 2: spread_small<2>(a, st); break;
+            default: spread_small<1>(a, st); break;
+        }
+    }
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     if (a.n_big > 0) return cudaStreamWaitEvent(st, a.ev_join, 0);
@@ -762,13 +931,66 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1) k_ibm_spread_
     const int2 w = work[blockIdx.x];
     stage_args<THREADS>(sa, args + w.x);
     __syncthreads();
-    ibm_spread_plane<THREADS>(sa, w.y, big ? sa.big_tile_cells : sa.smem_cells, tile);
+    const PlaneGroup<THREADS> grp{0, 0};
+    ibm_spread_plane<THREADS>(sa, w.y, big ? sa.big_tile_cells : sa.smem_cells, tile, grp);
 }
 
+// The batch's ordinary planes, G work items (lattice, plane) per CTA: each
+// group stages its lattice's arguments and walks its plane on a tile that
+// bulk copies fill, as k_ibm_spread_bulk does for one lattice. region_cells:
+// the largest tile of the batch's lattices (the group's share of shared
+// memory); each lattice's walk uses its own tile size within it.
+template <int NT, int G>
+__global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_batch_bulk(const IbmArgs* __restrict__ args,
+                                                                    const int2* __restrict__ work, int nwork,
+                                                                    int region_cells) {
+    extern __shared__ __align__(128) float btile[];             // [G][4][region_cells + 8]
+    __shared__ IbmArgs sa[G];
+    __shared__ uint64_t bars[G];
+    __shared__ int fails[G];
+    const int g = G == 1 ? 0 : (int)threadIdx.x / NT;
+    const int q = (int)blockIdx.x * G + g;
+    if (q >= nwork) return;
+    const PlaneGroup<NT, (G > 1)> grp{g * NT, g + 1};
+    const int2 w = work[q];
+    constexpr int words = sizeof(IbmArgs) / 8;
+    for (int i = grp.tid(); i < words; i += NT)
+        reinterpret_cast<unsigned long long*>(&sa[g])[i] = reinterpret_cast<const unsigned long long*>(args + w.x)[i];
+    grp.sync();
+    ibm_spread_plane<NT, true>(sa[g], w.y, sa[g].smem_cells, btile + (size_t)g * 4 * (region_cells + 8), grp, &bars[g],
+                               &fails[g]);
+}
+
+// Work items per CTA of the batched ordinary-plane spread for tiles of
+// `cells` cells (as spread_groups, leaving room for the staged arguments).
+static int batch_spread_groups(int cells) {
+    const size_t per = (size_t)16 * (cells + 8) + sizeof(IbmArgs) + 16;
+    const int G = (int)((227 * 1024 - 256) / per);
+    return G < 1 ? 1 : (G > 4 ? 4 : G);
+}
+
+template <int G>
+static const void* batch_bulk_fn() { return (const void*)k_ibm_spread_batch_bulk<128, G>; }
+
 cudaError_t ibm_batch_prepare_smem(size_t small_bytes, size_t big_bytes) {
-    cudaError_t e = raise_smem_limit((const void*)k_ibm_spread_batch<128>, small_bytes);
-    if (e != cudaSuccess) return e;
+    (void)small_bytes;
+    // every variant may be launched (tank groups with smaller tiles take more
+    // work items per CTA): each gets the dynamic shared memory its widest
+    // launch can use
+    const void* fns[4] = {batch_bulk_fn<1>(), batch_bulk_fn<2>(), batch_bulk_fn<3>(), batch_bulk_fn<4>()};
+    for (int G = 1; G <= 4; G++) {
+        const size_t bytes = 227 * 1024 - (size_t)G * (sizeof(IbmArgs) + 16) - 256;
+        cudaError_t e = raise_smem_limit(fns[G - 1], bytes);
+        if (e != cudaSuccess) return e;
+    }
     return raise_smem_limit((const void*)k_ibm_spread_batch<512>, big_bytes);
+}
+
+template <int G>
+static void batch_spread_small(const IbmBatch& b, cudaStream_t st) {
+    const unsigned grid = (unsigned)((b.n_small + G - 1) / G);
+    const size_t bytes = (size_t)G * 16 * (b.small_tile + 8);
+    k_ibm_spread_batch_bulk<128, G><<<grid, 128 * G, bytes, st>>>(b.args, b.small, b.n_small, b.small_tile);
 }
 
 cudaError_t launch_ibm_batch(const IbmBatch& b, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
@@ -796,7 +1018,14 @@ cudaError_t launch_ibm_batch(const IbmBatch& b, cudaStream_t st, cudaStream_t si
         err = cudaEventRecord(join, side);
         if (err != cudaSuccess) return err;
     }
-    if (b.n_small > 0) k_ibm_spread_batch<128><<<b.n_small, 128, ibm_smem_bytes(Dims{}, b.small_tile), st>>>(b.args, b.small, 0);
+    if (b.n_small > 0) {
+        switch (batch_spread_groups(b.small_tile)) {
+            case 4: batch_spread_small<4>(b, st); break;
+            case 3: batch_spread_small<3>(b, st); break;
+            case 2: batch_spread_small<2>(b, st); break;
+            default: batch_spread_small<1>(b, st); break;
+        }
+    }
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     if (b.n_big > 0) return cudaStreamWaitEvent(st, join, 0);

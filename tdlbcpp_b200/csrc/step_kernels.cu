@@ -59,7 +59,7 @@ static cudaError_t launch_simple_v(const StepArgs& a, cudaStream_t st) {
     const dim3 grid(step_blocks(a, V)), block(128);
 #define TDLB_SIMPLE(LES, FM, COL, PART)                                                                       \
     k_step_simple<float, V, LES, FM, COL, PART><<<grid, block, 0, st>>>(a.A, a.B, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, \
-                                                                      a.g, a.p, a.zone)
+                                                                      a.g, a.p, a.zone, ResidualBox{}, ResidualBox{})
     if (!a.collide) TDLB_SIMPLE(false, false, false, 0);
     else if (a.from_moments) { if (a.les) TDLB_SIMPLE(true, true, true, 0); else TDLB_SIMPLE(false, true, true, 0); }
     else if constexpr (V == 1) {
@@ -81,8 +81,8 @@ static cudaError_t launch_simple_v(const StepArgs& a, cudaStream_t st) {
 
 template <int V, bool LES, bool FM, bool COL, int PART>
 static void eso_launch(const StepArgs& a, dim3 grid, cudaStream_t st) {
-    if (a.even) k_step_esotwist<float, V, LES, FM, COL, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone);
-    else k_step_esotwist<float, V, LES, FM, COL, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone);
+    if (a.even) k_step_esotwist<float, V, LES, FM, COL, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone, ResidualBox{});
+    else k_step_esotwist<float, V, LES, FM, COL, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone, ResidualBox{});
 }
 
 template <int V>
@@ -133,10 +133,10 @@ cudaError_t launch_fill_uniform_moments(Planes Q, const Dims& g, float rho, cuda
 }
 
 cudaError_t launch_state_moments(Planes A, Planes M, const Dims& g, int mode, int even, cudaStream_t st, int storage,
-                                 const CollideParams& p) {
+                                 const CollideParams& p, const ResidualBox& rb) {
     const unsigned blocks = blocks_for(g.rows() * g.nz, 256);
     with_storage(storage, [&](auto s) {
-        k_state_moments<decltype(s)><<<blocks, 256, 0, st>>>(A, M, g, mode, even, p);
+        k_state_moments<decltype(s)><<<blocks, 256, 0, st>>>(A, M, g, mode, even, p, rb);
     });
     return cudaGetLastError();
 }

@@ -220,6 +220,62 @@ __device__ __forceinline__ void collide_quad(float (&f)[NQ][V], const Quad& q, f
 }
 
 // ---------------------------------------------------------------------------
+// Residual box (16-bit storage, one cell per thread; tdlb::ResidualBox).
+// Called functions rather than inlined: only the warps near the box call
+// them, and the issue-bound step kernels keep their straight-line code and
+// registers. f holds the cell's 18 values in direction order.
+// ---------------------------------------------------------------------------
+// Simple: add the residuals of the source locations inside the box (x - c_d,
+// or the cell itself where x - c_d is off the lattice).
+static __device__ __noinline__ void box_pull_simple(const ResidualBox rr, int i, int j, int k, int nx, int ny, int nz,
+                                             float* f) {
+#pragma unroll
+    for (int d = 0; d < NQ; d++) {
+        const int si = i - cx_of(d), sj = j - cy_of(d), sk = k - cz_of(d);
+        const bool in = (unsigned)si < (unsigned)nx && (unsigned)sj < (unsigned)ny && (unsigned)sk < (unsigned)nz;
+        const int li = in ? si : i, lj = in ? sj : j, lk = in ? sk : k;
+        if (rr.contains(li, lj, lk)) f[d] += *rr.at(d, li, lj, lk);
+    }
+}
+// Simple: the residuals of the cell's own 18 outputs.
+template <typename S>
+__device__ __noinline__ void box_store_simple(const ResidualBox rw, int i, int j, int k, const float* f) {
+#pragma unroll
+    for (int d = 0; d < NQ; d++) *rw.at(d, i, j, k) = f[d] - Storage<S>::dec(Storage<S>::enc(f[d]));
+}
+// Esotwist: slot s of cell (i, j, k) lives at (li, lj, lk); on reading, it
+// holds direction EVEN ? s : s ^ 1, on writing EVEN ? s ^ 1 : s.
+template <bool EVEN>
+__device__ __forceinline__ void eso_location(int s, int i, int j, int k, int i1, int j1, int k1, int& li, int& lj,
+                                             int& lk) {
+    const int sg = EVEN ? -1 : 1;
+    li = sg * cx_of(s) > 0 ? i1 : i;
+    lj = sg * cy_of(s) > 0 ? j1 : j;
+    lk = sg * cz_of(s) > 0 ? k1 : k;
+}
+template <bool EVEN>
+__device__ __noinline__ void box_read_eso(const ResidualBox rb, int i, int j, int k, int i1, int j1, int k1,
+                                          float* f) {
+#pragma unroll
+    for (int s = 0; s < NQ; s++) {
+        int li, lj, lk;
+        eso_location<EVEN>(s, i, j, k, i1, j1, k1, li, lj, lk);
+        if (rb.contains(li, lj, lk)) f[EVEN ? s : (s ^ 1)] += *rb.at(s, li, lj, lk);
+    }
+}
+template <typename S, bool EVEN>
+__device__ __noinline__ void box_write_eso(const ResidualBox rb, int i, int j, int k, int i1, int j1, int k1,
+                                           const float* f) {
+#pragma unroll
+    for (int s = 0; s < NQ; s++) {
+        int li, lj, lk;
+        eso_location<EVEN>(s, i, j, k, i1, j1, k1, li, lj, lk);
+        const float v = f[EVEN ? (s ^ 1) : s];
+        if (rb.contains(li, lj, lk)) *rb.at(s, li, lj, lk) = v - Storage<S>::dec(Storage<S>::enc(v));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Simple (A/B, pull).
 //
 // All loads of a thread are issued as one straight-line batch (no branch
@@ -235,7 +291,8 @@ template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool FOR
 __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, float* __restrict__ Nu,
                                             const float* __restrict__ Fx, const float* __restrict__ Fy,
                                             const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
-                                            const Dims& g, const CollideParams& p, unsigned t) {
+                                            const Dims& g, const CollideParams& p, unsigned t,
+                                            const ResidualBox rr = ResidualBox{}, const ResidualBox rw = ResidualBox{}) {
     static_assert(!(Storage<S>::deviation && FROM_MOMENTS), "16-bit state always holds populations");
     const int nq = g.kp / V;
     const Quad q = quad_of<V, sizeof(S) == 2>(g, nq, t);
@@ -258,6 +315,10 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
                               (cz > 0 && k_first) || (cz < 0 && k_last));
             const int off = in ? -(cx * rs + cy * g.kp + cz) : 0;
             f[d][0] = pload1<S, true>(A.p[d], q.e0 + off);
+        }
+        if constexpr (Storage<S>::deviation) {
+            // residual box: the exact deviation of every source location inside it
+            if (q.active && rr.near(q.i, q.j, q.k0)) box_pull_simple(rr, q.i, q.j, q.k0, g.nx, g.ny, g.nz, &f[0][0]);
         }
     } else {
         float hal[NQ], own[NQ];
@@ -326,6 +387,9 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
 #pragma unroll
     for (int d = 0; d < NQ; d++) pstore<S, V>(B.p[d], q.e0, f[d]);
     if (COLLIDE && LES) vstore<V>(Nu + q.e0, nu);
+    if constexpr (Storage<S>::deviation && V == 1) {
+        if (rw.on() && rw.contains(q.i, q.j, q.k0)) box_store_simple<S>(rw, q.i, q.j, q.k0, &f[0][0]);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -346,7 +410,7 @@ template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVE
 __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict__ Nu, const float* __restrict__ Fx,
                                               const float* __restrict__ Fy, const float* __restrict__ Fz,
                                               const uint32_t* __restrict__ mask, const Dims& g, const CollideParams& p,
-                                              unsigned t) {
+                                              unsigned t, const ResidualBox rb = ResidualBox{}) {
     static_assert(!(Storage<S>::deviation && FROM_MOMENTS), "16-bit state always holds populations");
     const int nq = g.kp / V;
     const Quad q = quad_of<V, sizeof(S) == 2>(g, nq, t);
@@ -384,6 +448,11 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
             } else {
                 f[d][0] = v[s];
             }
+        }
+        if constexpr (Storage<S>::deviation) {
+            // residual box: the exact deviation of every location inside it
+            // (slot s of this cell lives at cell (li, lj, lk))
+            if (q.active && rb.near(q.i, q.j, q.k0)) box_read_eso<EVEN>(rb, q.i, q.j, q.k0, i1, j1, k1, &f[0][0]);
         }
     } else {
         float hal[NQ], wrap[NQ];
@@ -444,6 +513,9 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
             if (q.active && (warp_end || row_end)) pstore1<S>(Q.p[s], base + k1, f[d][0]);
         }
         if (COLLIDE && LES && q.active) Nu[q.e0] = nu[0];
+        if constexpr (Storage<S>::deviation) {
+            if (q.active && rb.near(q.i, q.j, q.k0)) box_write_eso<S, EVEN>(rb, q.i, q.j, q.k0, i1, j1, k1, &f[0][0]);
+        }
         return;
     }
     const bool k_first = q.k0 == 0;
@@ -505,11 +577,12 @@ template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, int PART
 __global__ void __launch_bounds__(128, 4) k_step_simple(Planes A, Planes B, float* __restrict__ Nu,
                                                        const float* __restrict__ Fx, const float* __restrict__ Fy,
                                                        const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
-                                                       Dims g, CollideParams p, StepPart part) {
+                                                       Dims g, CollideParams p, StepPart part, ResidualBox rr,
+                                                       ResidualBox rw) {
     static_assert(PART == 0 || V == 1, "split steps run one cell per thread");
     unsigned t;
     if (!part_thread<PART>(part, t)) return;   // whole warps
-    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE, PART != 1>(A, B, Nu, Fx, Fy, Fz, mask, g, p, t);
+    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE, PART != 1>(A, B, Nu, Fx, Fy, Fz, mask, g, p, t, rr, rw);
 }
 
 // Resident 128-thread blocks per SM the Esotwist kernel is built for: the
@@ -522,11 +595,11 @@ template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVE
 __global__ void __launch_bounds__(128, kEsotwistBlocksPerSM<V>) k_step_esotwist(Planes Q, float* __restrict__ Nu,
                                                          const float* __restrict__ Fx, const float* __restrict__ Fy,
                                                          const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
-                                                         Dims g, CollideParams p, StepPart part) {
+                                                         Dims g, CollideParams p, StepPart part, ResidualBox rb) {
     static_assert(PART == 0 || V == 1, "split steps run one cell per thread");
     unsigned t;
     if (!part_thread<PART>(part, t)) return;   // whole warps
-    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN, PART != 1>(Q, Nu, Fx, Fy, Fz, mask, g, p, t);
+    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN, PART != 1>(Q, Nu, Fx, Fy, Fz, mask, g, p, t, rb);
 }
 
 // Moments of the current state at every interior cell (what the reference's
@@ -535,7 +608,8 @@ __global__ void __launch_bounds__(128, kEsotwistBlocksPerSM<V>) k_step_esotwist(
 // 2 = Esotwist populations (read map, parity `even`), 3 = Esotwist moments.
 template <typename S>
 __device__ __forceinline__ void state_moments18(const Planes& A, const Dims& g, int mode, int even, const CollideParams& p,
-                                                int i, int j, int k, float (&m)[NQ]) {
+                                                int i, int j, int k, float (&m)[NQ],
+                                                const ResidualBox rb = ResidualBox{}) {
     const int e = (int)(((long long)i * g.ny + j) * g.kp + k);
     float q[NQ];
     if (mode <= 1) {
@@ -546,6 +620,13 @@ __device__ __forceinline__ void state_moments18(const Planes& A, const Dims& g, 
                 const int si = i - cx_of(d), sj = j - cy_of(d), sk = k - cz_of(d);
                 const bool in = (unsigned)si < (unsigned)g.nx && (unsigned)sj < (unsigned)g.ny && (unsigned)sk < (unsigned)g.nz;
                 if (in) src = (si * g.ny + sj) * g.kp + sk;
+                if (Storage<S>::deviation && rb.on()) {
+                    const int li = in ? si : i, lj = in ? sj : j, lk = in ? sk : k;
+                    if (rb.contains(li, lj, lk)) {
+                        q[d] = pload1<S, false>(A.p[d], src) + *rb.at(d, li, lj, lk) + rest_of<S>(d, p);
+                        continue;
+                    }
+                }
             }
             q[d] = pload1<S, false>(A.p[d], src) + (mode == 0 ? rest_of<S>(d, p) : 0.f);
         }
@@ -558,6 +639,8 @@ __device__ __forceinline__ void state_moments18(const Planes& A, const Dims& g, 
             const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
             q[d] = pload1<S, false>(A.p[s], ((oi ? i1 : i) * g.ny + (oj ? j1 : j)) * g.kp + (ok ? k1 : k)) +
                    (mode == 2 ? rest_of<S>(d, p) : 0.f);
+            if (Storage<S>::deviation && mode == 2 && rb.on() && rb.contains(oi ? i1 : i, oj ? j1 : j, ok ? k1 : k))
+                q[d] += *rb.at(s, oi ? i1 : i, oj ? j1 : j, ok ? k1 : k);
         }
     }
     if (mode == 0 || mode == 2) moments_of(q, m);
@@ -568,7 +651,8 @@ __device__ __forceinline__ void state_moments18(const Planes& A, const Dims& g, 
 }
 
 template <typename S>
-__global__ void __launch_bounds__(256) k_state_moments(Planes A, Planes M, Dims g, int mode, int even, CollideParams p) {
+__global__ void __launch_bounds__(256) k_state_moments(Planes A, Planes M, Dims g, int mode, int even, CollideParams p,
+                                                       ResidualBox rb) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long total = g.rows() * g.nz;
     if (t >= total) return;
@@ -577,7 +661,7 @@ __global__ void __launch_bounds__(256) k_state_moments(Planes A, Planes M, Dims 
     const int j = (int)(row % g.ny);
     const int i = (int)(row / g.ny);
     float m[NQ];
-    state_moments18<S>(A, g, mode, even, p, i, j, k, m);
+    state_moments18<S>(A, g, mode, even, p, i, j, k, m, rb);
     const long long e = row * g.kp + k;
 #pragma unroll
     for (int d = 0; d < NQ; d++) M.p[d][e] = m[d];

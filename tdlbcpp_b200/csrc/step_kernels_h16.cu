@@ -14,8 +14,10 @@ static inline unsigned grid16(const StepArgs& a, int V) {
 
 template <typename S, int V, bool LES, int PART>
 static void simple16_part(const StepArgs& a, cudaStream_t st) {
+    // the residual box serves one cell per thread
+    const ResidualBox rr = V == 1 ? a.rr : ResidualBox{}, rw = V == 1 ? a.rw : ResidualBox{};
     k_step_simple<S, V, LES, false, true, PART><<<grid16(a, V), 128, 0, st>>>(a.A, a.B, a.Nu, a.Fx, a.Fy, a.Fz, a.mask,
-                                                                            a.g, a.p, a.zone);
+                                                                            a.g, a.p, a.zone, rr, rw);
 }
 
 template <typename S, int V, bool LES>
@@ -37,8 +39,9 @@ static cudaError_t simple16(const StepArgs& a, cudaStream_t st) {
 template <typename S, int V, bool LES, int PART>
 static void eso16_part(const StepArgs& a, cudaStream_t st) {
     const unsigned grid = grid16(a, V);
-    if (a.even) k_step_esotwist<S, V, LES, false, true, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone);
-    else k_step_esotwist<S, V, LES, false, true, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone);
+    const ResidualBox rb = V == 1 ? a.rr : ResidualBox{};
+    if (a.even) k_step_esotwist<S, V, LES, false, true, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone, rb);
+    else k_step_esotwist<S, V, LES, false, true, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone, rb);
 }
 
 template <typename S, int V, bool LES>

@@ -137,6 +137,32 @@ inline auto with_storage(int kind, F&& f) {
 // rest population of slot/direction d for the deviation storage
 __host__ __device__ constexpr bool is_face(int d) { return d < 6; }
 
+// Residual box of the 16-bit storage: for every population location (cell,
+// slot) inside the box [i0, i0+bx) x [j0, j0+by) x [k0, k0+bz) the FP32
+// residual of its 16-bit rounding is kept as well, so that such a location
+// holds its deviation exactly: dec(stored) + residual. Placed over the
+// impeller's swept volume it keeps the stirred flow's most sensitive cells at
+// FP32 storage precision (there the 16-bit rounding dominates the velocity
+// error against FP64). res == nullptr: no box. Residual plane s (one per
+// slot) starts at res + s * n.
+struct ResidualBox {
+    float* res = nullptr;
+    long long n = 0;
+    int i0 = 0, j0 = 0, k0 = 0, bx = 0, by = 0, bz = 0;
+    __host__ __device__ bool on() const { return res != nullptr; }
+    __device__ __forceinline__ bool contains(int i, int j, int k) const {
+        return (unsigned)(i - i0) < (unsigned)bx && (unsigned)(j - j0) < (unsigned)by && (unsigned)(k - k0) < (unsigned)bz;
+    }
+    // the 3x3x3 neighbourhood of (i, j, k) meets the box
+    __device__ __forceinline__ bool near(int i, int j, int k) const {
+        return res && (unsigned)(i - i0 + 1) < (unsigned)(bx + 2) && (unsigned)(j - j0 + 1) < (unsigned)(by + 2) &&
+               (unsigned)(k - k0 + 1) < (unsigned)(bz + 2);
+    }
+    __device__ __forceinline__ float* at(int s, int i, int j, int k) const {
+        return res + (long long)s * n + ((long long)(i - i0) * by + (j - j0)) * bz + (k - k0);
+    }
+};
+
 // Collision constants (FlowParams fields the step reads).
 struct CollideParams {
     float nu;       // molecular viscosity

@@ -109,6 +109,11 @@ struct tdlb_lattice {
     int* d_zone_list = nullptr;          // the inner chunks, then the outer chunks, each ascending
     int n_zone = 0, n_outer = 0;
     long long zone_list_cap = 0;
+    // 16-bit storage: the residual box (tdlb::ResidualBox) and its residuals,
+    // one set per population buffer (Simple: A and B; Esotwist: one)
+    tdlb::ResidualBox rbox_geom{};        // geometry only (res unused)
+    float* d_res[2] = {nullptr, nullptr};
+    bool rbox_auto = true;                // set from the impeller by tdlb_attach_rushton
     // step-kernel timing (tdlb_set_kernel_timing): start/stop event pairs
     bool timing = false;
     std::vector<cudaEvent_t> tev;
@@ -129,6 +134,14 @@ struct tdlb_lattice {
         for (int d = 0; d < tdlb::NQ; d++) p.p[d] = base + (size_t)d * (size_t)g.plane;
         return p;
     }
+    // residual box of population buffer `buf` (0: bufA, 1: bufB); off when
+    // no box is set
+    tdlb::ResidualBox rbox(int buf) const {
+        tdlb::ResidualBox b = rbox_geom;
+        b.res = d_res[buf];
+        return b;
+    }
+    int state_index() const { return cfg.streaming == TDLB_STREAMING_SIMPLE && cur == 1 ? 1 : 0; }
     float* state_buf() const { return cfg.streaming == TDLB_STREAMING_SIMPLE && cur == 1 ? bufB : bufA; }
     float* other_buf() const { return cur == 1 ? bufA : bufB; }
     uint32_t* mask_cur() const { return mask + (size_t)(pass & 1) * mask_words; }
@@ -151,4 +164,9 @@ void return_stream(tdlb_lattice* h);
 // Make `stream` wait for the forcing pass and inner launches queued on the
 // split-step stream (every entry point other than the step loop calls it).
 cudaError_t join_side(tdlb_lattice* h);
+// Remove the residual box (a tank joining a batch, whose step kernel keeps
+// none), or set its residuals to zero (after the planes were written
+// without them).
+void drop_residual_box(tdlb_lattice* h);
+void clear_residual_box(tdlb_lattice* h);
 }  // namespace tdlb_rt

@@ -31,6 +31,8 @@ struct StepArgs {
     int storage;            // StorageKind of the population planes
     int part;               // 0: every cell; 1: outer chunks; 2: inner chunks (vec == 1, populations)
     StepPart zone;          // the chunks of part 1 or 2
+    ResidualBox rr;         // 16-bit storage, one cell per thread: residuals of the locations read ...
+    ResidualBox rw;         // ... and written (Simple: of buffer A and B; Esotwist: the same box)
 };
 
 cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st);
@@ -39,7 +41,7 @@ cudaError_t launch_step_simple_h16(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_esotwist_h16(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_fill_uniform_moments(Planes Q, const Dims& g, float rho, cudaStream_t st);
 cudaError_t launch_state_moments(Planes A, Planes M, const Dims& g, int mode, int even, cudaStream_t st, int storage,
-                                 const CollideParams& p);
+                                 const CollideParams& p, const ResidualBox& rb = ResidualBox{});
 
 // ---- immersed boundary ----
 
@@ -108,6 +110,7 @@ struct IbmArgs {
     float alpha, beta;
     int storage;                // StorageKind of the state planes
     CollideParams p;            // rest offsets of the 16-bit storage
+    ResidualBox rbox;           // residuals of the state's locations (16-bit storage; off: res == NULL)
 };
 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st);
@@ -134,8 +137,10 @@ cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, 
 // Shared memory the spread kernel needs: the plane's touched-flag tile plus
 // an F tile of `cells` cells.
 size_t ibm_smem_bytes(const Dims& g, int cells);
-// Opt the spread kernel in to `bytes` of dynamic shared memory (> 48 KiB).
-cudaError_t ibm_prepare_smem(size_t bytes);
+// Opt the spread kernels in to the dynamic shared memory of the ordinary
+// planes' launch (tiles of `small_cells` cells) and of the big planes'
+// launch (`big_bytes`).
+cudaError_t ibm_prepare_smem(int small_cells, size_t big_bytes);
 // FP64 force and torque of markers [begin, n) (by list index) of the last
 // forcing pass: out[0..2] = -beta * sum of spread sums, out[3] = torque about
 // the tank axis (ci, ck), out[4] = number of markers summed. `partial` holds

@@ -100,6 +100,7 @@ def test_16bit_cells_per_thread_variants_agree(gpu, streaming, storage):
                             streaming=tb.STREAMING_SIMPLE if streaming == "Simple" else tb.STREAMING_ESOTWIST)
         cu.set_cells_per_thread(vec)
         cu.attach_rushton(rt, d, 0.0, d)
+        cu.set_residual_box(0, 0, 0, 0, 0, 0)      # one cell per thread would get one; the others cannot
         cu.initialise(1.0)
         cu.forcing_resident(ALPHA, BETA)
         angle = 0.0
@@ -140,13 +141,15 @@ def fp64_oracle_velocity(po, tb, edge, steps, re, tip):
     return rho, (m[..., 1:4] + 0.5 * f) / rho[..., None]
 
 
-def gpu_velocity(tb, edge, steps, re, tip, storage):
+def gpu_velocity(tb, edge, steps, re, tip, storage, box=True):
     rt = tb.RushtonTurbine(edge, edge, edge, tip_speed=tip, startup_steps=0)
     nu = tb.nu_from_reynolds(re, tip, rt.blade_outer_radius())
     cu = tb.ComputeUnit(x=edge, y=edge, z=edge, nu=nu, cs0=0.1, g3=0.8, useLES=1, initialRho=1.0, storage=storage,
                         streaming=tb.STREAMING_ESOTWIST)
     d1 = rt.increment(1)
     cu.attach_rushton(rt, d1, d1, d1)
+    if not box:
+        cu.set_residual_box(0, 0, 0, 0, 0, 0)
     cu.initialise(1.0)
     cu.forcing_resident(ALPHA, BETA)
     angle = d1
@@ -162,11 +165,11 @@ def gpu_velocity(tb, edge, steps, re, tip, storage):
     return rho, u, red
 
 
-# storage -> stated bound of the velocity error against FP64 (relative L2)
-FP64_BOUNDS = {"fp32": 5e-5, "fp16": 1e-3, "bf16": 5e-3}
+# storage form -> stated bound of the velocity error against FP64 (relative L2)
+FP64_BOUNDS = {"fp32": 5e-5, "fp16": 1e-3, "bf16": 5e-3, "fp16-nobox": 1e-3, "bf16-nobox": 5e-3}
 
 
-@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16", "fp16-nobox", "bf16-nobox"])
 def test_storage_forms_vs_fp64_oracle(gpu, port_oracle, storage):
     """Each storage form against the FP64 CPU restatement (48^3 Rushton tank,
     Esotwist, Re 20000, tip speed 0.1, LES, 300 steps), not against FP32.
@@ -174,15 +177,94 @@ def test_storage_forms_vs_fp64_oracle(gpu, port_oracle, storage):
     Stated bounds on the velocity field's relative L2 error: FP32 5e-5
     (measured about 1.2e-5), FP16 1e-3 (the target; measured about 3.4e-4),
     BF16 5e-3 (measured about 2.6e-3: BF16's 8-bit significand misses the
-    1e-3 target). Density: within the same bounds. The FP64 mass sum
+    1e-3 target). The 16-bit forms run with the residual box that
+    tdlb_attach_rushton places over the impeller's swept volume, and
+    without it ("-nobox"). Density: within the same bounds. The FP64 mass sum
     of the 16-bit forms drifts by at most 1e-6 relative: the deviations
     carry rho - rho0 without the rest weights' rounding."""
     tb, po = gpu, port_oracle
     edge, steps, re, tip = 48, 300, 20000.0, 0.1
     rho_ref, u_ref = fp64_oracle_velocity(po, tb, edge, steps, re, tip)
-    rho, u, red = gpu_velocity(tb, edge, steps, re, tip, storage)
+    rho, u, red = gpu_velocity(tb, edge, steps, re, tip, storage.split("-")[0], box="nobox" not in storage)
     bound = FP64_BOUNDS[storage]
     assert rel_l2(u, u_ref) <= bound
     assert rel_l2(rho, rho_ref) <= bound
     if storage != "fp32":
         assert abs(red[0] / edge ** 3 - 1.0) <= 1e-6
+
+
+def test_residual_box_api(gpu):
+    """tdlb_attach_rushton gives a 16-bit lattice a residual box over the
+    blades' swept volume; FP32 storage has none; the box excludes other
+    cells-per-thread variants until it is removed; a lattice joining a batch
+    loses it."""
+    tb = gpu
+    e = 48
+    rt = tb.RushtonTurbine(e, e, e, tip_speed=0.1)
+    d = rt.increment(1)
+    blades = rt.rotating(0.0, d)
+    cu = tb.ComputeUnit(x=e, y=e, z=e, nu=1e-3, cs0=0.1, useLES=1, storage="fp16", streaming=tb.STREAMING_ESOTWIST)
+    assert cu.residual_box() == (0, 0, 0, 0, 0, 0)
+    cu.attach_rushton(rt, d, 0.0, d)
+    i0, i1, j0, j1, k0, k1 = cu.residual_box()
+    assert j0 <= blades["j"].min() - 4 and j1 >= blades["j"].max() + 5
+    assert i0 <= blades["i"].min() - 3 and i1 >= blades["i"].max() + 4
+    assert k0 <= blades["k"].min() - 3 and k1 >= blades["k"].max() + 4
+    with pytest.raises(tb.TdlbError):
+        cu.set_cells_per_thread(2)
+    with pytest.raises(tb.TdlbError):
+        cu.set_residual_box(0, 10, 1, 10, 1, 10)          # index 0 may not lie in the box
+    cu.set_residual_box(0, 0, 0, 0, 0, 0)
+    assert cu.residual_box() == (0, 0, 0, 0, 0, 0)
+    cu.set_cells_per_thread(2)
+    cu.close()
+    c32 = tb.ComputeUnit(x=e, y=e, z=e, nu=1e-3, storage="fp32")
+    c32.attach_rushton(rt, d, 0.0, d)
+    assert c32.residual_box() == (0, 0, 0, 0, 0, 0)
+    with pytest.raises(tb.TdlbError):
+        c32.set_residual_box(1, 10, 1, 10, 1, 10)
+    c32.close()
+    # a lattice joining a batch loses its box
+    cu = tb.ComputeUnit(x=e, y=e, z=e, nu=1e-3, cs0=0.1, useLES=1, storage="fp16", streaming=tb.STREAMING_ESOTWIST)
+    cu.attach_rushton(rt, d, 0.0, d)
+    assert cu.residual_box() != (0, 0, 0, 0, 0, 0)
+    with tb.Batch([dict(x=24, y=24, z=24, nu=1e-3, streaming="Esotwist", storage="fp16")]) as b:
+        b.adopt(cu)
+        assert cu.residual_box() == (0, 0, 0, 0, 0, 0)
+        with pytest.raises(tb.TdlbError):
+            cu.set_residual_box(1, 10, 1, 10, 1, 10)
+
+
+@pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
+def test_near_full_residual_box_tracks_fp32(gpu, streaming):
+    """With a box over every cell but the i = 0, j = 0 and k = 0 planes, FP16
+    storage keeps almost every location exact: after 30 steps of a 40^3
+    Rushton tank its velocity is within 1e-4 relative L2 of the FP32-storage
+    run (without the box: about 1e-3), which checks that every location's
+    residual is written and read back at the right place."""
+    tb = gpu
+    e = 40
+    out = {}
+    for storage, box in (("fp32", False), ("fp16", True), ("fp16", False)):
+        rt = tb.RushtonTurbine(e, e, e, tip_speed=0.1)
+        d = rt.increment(1)
+        nu = tb.nu_from_reynolds(7300.0, 0.1, rt.blade_outer_radius())
+        cu = tb.ComputeUnit(x=e, y=e, z=e, nu=nu, cs0=0.1, useLES=1, initialRho=1.0, storage=storage,
+                            streaming=tb.STREAMING_SIMPLE if streaming == "Simple" else tb.STREAMING_ESOTWIST)
+        cu.attach_rushton(rt, d, 0.0, d)
+        if storage == "fp16":
+            cu.set_residual_box(*((1, e) * 3) if box else (0,) * 6)
+        cu.initialise(1.0)
+        cu.forcing_resident(ALPHA, BETA)
+        angle = 0.0
+        for _ in range(30):
+            angle += d
+            cu.rotate_impeller(angle, d)
+            cu.collision()
+            cu.forcing_resident(ALPHA, BETA)
+        out[(storage, box)] = cu.read_velocity_density()[1]
+        cu.close()
+    err_box = rel_l2(out[("fp16", True)], out[("fp32", False)])
+    err_plain = rel_l2(out[("fp16", False)], out[("fp32", False)])
+    assert err_box <= 1e-4, (err_box, err_plain)
+    assert err_box < 0.2 * err_plain
