@@ -262,14 +262,17 @@ int tdlb_set_cells_per_thread(tdlb_handle h, int v);
  * deviation, the FP32 residual of its rounding, so these locations are
  * stored exactly: the stirred tank's velocity error against FP64 comes
  * mostly from the 16-bit rounding in the impeller's swept volume. The box
- * costs 72 (Esotwist) or 144 (Simple) bytes of device memory per box cell
- * and traffic only there. tdlb_attach_rushton sets it over the blades'
- * swept volume with a 4-cell margin, unless a box was set (or removed) with
- * this call; an empty box (i1 <= i0) removes it. Requires 16-bit storage
- * (TDLB_EINVAL), one cell per thread and a lattice outside a batch
- * (TDLB_ESTATE; a lattice joining a batch loses its box), and i0, j0, k0 >= 1.
- * Read-back (moments, velocity), the forcing pass and the FP64 sums include
- * the residuals. */
+ * costs 72 (Esotwist) or 144 (Simple) bytes of device memory per box cell,
+ * plus 76 bytes of scratch per cell of the 32-cell chunks within one cell of
+ * it, and traffic only there: a step with a box adds two launches over those
+ * chunks (they are stepped with the residuals before the plain launch and
+ * committed after it) and never splits (tdlb_set_overlap).
+ * tdlb_attach_rushton sets it over the blades' swept volume with a 4-cell
+ * margin, unless a box was set (or removed) with this call; an empty box
+ * (i1 <= i0) removes it. Requires 16-bit storage (TDLB_EINVAL), one cell per
+ * thread and a lattice outside a batch (TDLB_ESTATE; a lattice joining a
+ * batch loses its box), and i0, j0, k0 >= 1. Read-back (moments, velocity),
+ * the forcing pass and the FP64 sums include the residuals. */
 int tdlb_set_residual_box(tdlb_handle h, int64_t i0, int64_t i1, int64_t j0, int64_t j1, int64_t k0, int64_t k1);
 /* The current box as {i0, i1, j0, j1, k0, k1} (all zero: none). */
 int tdlb_get_residual_box(tdlb_handle h, int64_t* box6);
@@ -286,7 +289,8 @@ int tdlb_get_residual_box(tdlb_handle h, int64_t* box6);
  * so results are bit-identical with overlap on and off. Measured on B200
  * at 400^3 (Rushton tank): whole steps 0-4 % faster, because the two
  * launches over scattered chunks lose most of what the overlap hides, hence
- * off by default. Entry points other
+ * off by default. A step with a residual box (tdlb_set_residual_box) runs
+ * unsplit. Entry points other
  * than tdlb_collision, tdlb_forcing_resident, tdlb_rotate_impeller and
  * tdlb_step first order the handle's stream after that second stream. */
 int tdlb_set_overlap(tdlb_handle h, int mode);

@@ -73,7 +73,9 @@ __device__ __forceinline__ float ld_state(const float* plane, long long e) {
     else return Storage<S>::dec(reinterpret_cast<const S*>(plane)[e]);
 }
 
-// rho and momentum of the state at interior cell (i, j, k).
+// rho and momentum of the state at interior cell (i, j, k). With a residual
+// box, a cell near it adds the residuals of its locations inside the box
+// after its 18 loads (the other cells take no box code).
 template <typename S>
 __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int even, const Dims& g, int i, int j, int k,
                                               const CollideParams& p, float* m4, const ResidualBox& rb) {
@@ -84,6 +86,7 @@ __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int eve
         return;
     }
     float q[NQ];
+    const bool near_box = Storage<S>::deviation && rb.near(i, j, k);
     if (mode == 0) {
 #pragma unroll
         for (int d = 0; d < NQ; d++) {
@@ -91,7 +94,12 @@ __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int eve
             const bool in = (unsigned)si < (unsigned)g.nx && (unsigned)sj < (unsigned)g.ny && (unsigned)sk < (unsigned)g.nz;
             const long long src = in ? ((long long)si * g.ny + sj) * g.kp + sk : ((long long)i * g.ny + j) * g.kp + k;
             q[d] = ld_state<S>(A.p[d], src) + (Storage<S>::deviation ? (is_face(d) ? p.wface : p.wedge) : 0.f);
-            if (Storage<S>::deviation && rb.on()) {   // residual box: the exact deviation
+        }
+        if (near_box) {   // residual box: the exact deviations
+#pragma unroll
+            for (int d = 0; d < NQ; d++) {
+                const int si = i - cx_of(d), sj = j - cy_of(d), sk = k - cz_of(d);
+                const bool in = (unsigned)si < (unsigned)g.nx && (unsigned)sj < (unsigned)g.ny && (unsigned)sk < (unsigned)g.nz;
                 const int li = in ? si : i, lj = in ? sj : j, lk = in ? sk : k;
                 if (rb.contains(li, lj, lk)) q[d] += *rb.at(d, li, lj, lk);
             }
@@ -109,8 +117,15 @@ __device__ __forceinline__ void cell_moments4(const Planes& A, int mode, int eve
         const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
         q[d] = ld_state<S>(A.p[s], ((long long)(oi ? i1 : i) * g.ny + (oj ? j1 : j)) * g.kp + (ok ? k1 : k)) +
                (mode == 2 && Storage<S>::deviation ? (is_face(d) ? p.wface : p.wedge) : 0.f);
-        if (Storage<S>::deviation && mode == 2 && rb.on() && rb.contains(oi ? i1 : i, oj ? j1 : j, ok ? k1 : k))
-            q[d] += *rb.at(s, oi ? i1 : i, oj ? j1 : j, ok ? k1 : k);
+    }
+    if (mode == 2 && near_box) {   // residual box: the exact deviations
+#pragma unroll
+        for (int d = 0; d < NQ; d++) {
+            const int s = even ? d : (d ^ 1);
+            const int sg = even ? -1 : 1;
+            const bool oi = sg * cx_of(s) > 0, oj = sg * cy_of(s) > 0, ok = sg * cz_of(s) > 0;
+            if (rb.contains(oi ? i1 : i, oj ? j1 : j, ok ? k1 : k)) q[d] += *rb.at(s, oi ? i1 : i, oj ? j1 : j, ok ? k1 : k);
+        }
     }
     if (mode == 3) {
 #pragma unroll
@@ -127,15 +142,14 @@ __global__ void k_ibm_prepare(IbmArgs a, float* __restrict__ prep) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n0) return;
     const Marker mk = a.markers[a.sched[p]];
-    const long long n0 = a.n0;
+    float* row = prep + (size_t)p * PF_STRIDE;
     int c = 0;
     for (int k1 = -1; k1 <= 1; k1++)
         for (int i1 = -1; i1 <= 1; i1++, c++)
-            prep[(PF_W + c) * n0 + p] =
-                stencil_weight(mk.iCartFraction, mk.kCartFraction, i1, k1);
-    prep[PF_U * n0 + p] = mk.uDelta;
-    prep[PF_V * n0 + p] = mk.vDelta;
-    prep[PF_WV * n0 + p] = mk.wDelta;
+            row[PF_W + c] = stencil_weight(mk.iCartFraction, mk.kCartFraction, i1, k1);
+    row[PF_U] = mk.uDelta;
+    row[PF_V] = mk.vDelta;
+    row[PF_WV] = mk.wDelta;
 }
 
 // Per pass: rho and momentum of every unique stencil cell of the first
@@ -153,8 +167,7 @@ __device__ __forceinline__ void ibm_cell(const IbmArgs& a, int c) {
     float m4[4];
     cell_moments4<S>(a.A, a.state_mode, a.even, g, i, j, k, a.p, m4, a.rbox);
     const long long C = a.ncell;
-#pragma unroll
-    for (int s = 0; s < 4; s++) a.cell_m[s * C + c] = m4[s];
+    reinterpret_cast<float4*>(a.cell_m)[c] = make_float4(m4[0], m4[1], m4[2], m4[3]);
     const bool live = (a.mask_old[(long long)row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
     a.cell_F[c] = live ? a.Fx[e] : 0.f;
     a.cell_F[C + c] = live ? a.Fy[e] : 0.f;
@@ -198,10 +211,34 @@ __device__ __forceinline__ void ibm_tail_marker(const IbmArgs& a, int t) {
     s[TF_WV * cap + t] = mk.wDelta;
 }
 
+// One thread per (blade marker t, stencil cell c): thread u takes c = u /
+// ntail, t = u % ntail (c = 3 (k1 + 1) + (i1 + 1), as ibm_tail_marker), so
+// the 9 cells of a marker are gathered in parallel; c = 0 also writes the
+// marker velocity.
 template <typename S>
 __global__ void __launch_bounds__(128) k_ibm_gather_tail(IbmArgs a) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < a.n - a.n0) ibm_tail_marker<S>(a, t);
+    const int ntail = a.n - a.n0;
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= 9 * ntail) return;
+    const int c = u / ntail, t = u - c * ntail;
+    const Marker mk = a.markers[a.sched[a.n0 + t]];
+    const int k1 = c / 3 - 1, i1 = c - 3 * (c / 3) - 1;
+    const int i2 = wrap_i((int)mk.i + i1, a.g.nx), j = (int)mk.j, k2 = wrap_i((int)mk.k + k1, a.g.nz);
+    float m4[4];
+    cell_moments4<S>(a.A, a.state_mode, a.even, a.g, i2, j, k2, a.p, m4, a.rbox);
+    float* s = a.tail;
+    const long long cap = a.tail_cap;
+    s[(TF_W + c) * cap + t] = stencil_weight(mk.iCartFraction, mk.kCartFraction, i1, k1);
+    s[(TF_RHO + c) * cap + t] = m4[0];
+    s[(TF_MX + c) * cap + t] = m4[1];
+    s[(TF_MY + c) * cap + t] = m4[2];
+    s[(TF_MZ + c) * cap + t] = m4[3];
+    s[(TF_CELL + c) * cap + t] = __int_as_float((i2 << 16) | k2);
+    if (c == 0) {
+        s[TF_U * cap + t] = mk.uDelta;
+        s[TF_V * cap + t] = mk.vDelta;
+        s[TF_WV * cap + t] = mk.wDelta;
+    }
 }
 
 // Bulk asynchronous copies global -> shared memory with an mbarrier
@@ -244,6 +281,43 @@ __device__ __forceinline__ BulkSpan bulk_span(const void* base, int c0, int n) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(base) + 4ull * (unsigned)c0;
     const uintptr_t lo = a & ~uintptr_t(15), hi = (a + 4ull * (unsigned)n + 15) & ~uintptr_t(15);
     return BulkSpan{reinterpret_cast<const void*>(lo), (int)((a - lo) >> 2), (unsigned)(hi - lo)};
+}
+// Floats between the three F arrays of a bulk tile of `cells` cells: room
+// for the 16-byte rounding of each copy, and a multiple of 4, so that every
+// array (a bulk copy's destination) starts on a 16-byte boundary.
+__host__ __device__ constexpr int bulk_tile_stride(int cells) { return (cells + 8 + 3) & ~3; }
+
+// Element i of a row held as float4 registers (i a compile-time constant
+// after unrolling).
+template <int N>
+__device__ __forceinline__ float f4_lane(const float4 (&r)[N], int i) {
+    const float4 v = r[i >> 2];
+    return (i & 3) == 0 ? v.x : (i & 3) == 1 ? v.y : (i & 3) == 2 ? v.z : v.w;
+}
+
+// Bring elements [c0, c0 + n) of a 4-byte array into L2 (cp.async.bulk
+// prefetch: no completion to wait for). The span is rounded out to 16 bytes;
+// every array prefetched this way is allocated with 16 elements of padding.
+__device__ __forceinline__ void prefetch_l2(const void* base, int c0, int n) {
+    if (n <= 0) return;
+    const BulkSpan sp = bulk_span(base, c0, n);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(sp.src), "r"(sp.bytes) : "memory");
+}
+// The per-marker and per-cell data a group's walk of plane j reads, into L2
+// while the group fills its tile: the first segment's weights, cells and
+// velocities (markers [pm0, pm1) of the prep arrays), the plane's cell
+// moments, and the blade markers' gathered stencils. One array per lane.
+template <typename GRP>
+__device__ __forceinline__ void prefetch_plane(const IbmArgs& a, int j, int c0, int nc, const GRP grp) {
+    const int lane = grp.tid();
+    if (lane >= 32) return;
+    const int pm0 = a.level_ptr[a.plane_lv0[j]], pm1 = a.level_ptr[a.plane_lv0[j + 1]];
+    const int q0 = a.level_ptr[a.plane_lv1[j]] - a.n0, q1 = a.level_ptr[a.plane_lv1[j + 1]] - a.n0;
+    for (int f = lane; f < 2 + TF_COUNT; f += 32) {
+        if (f == 0) prefetch_l2(a.prep, pm0 * PF_STRIDE, (pm1 - pm0) * PF_STRIDE);
+        else if (f == 1) prefetch_l2(a.cell_m, 4 * c0, 4 * nc);
+        else prefetch_l2(a.tail + (size_t)(f - 2) * a.tail_cap, q0, q1 - q0);
+    }
 }
 
 // A group of NT threads (whole warps) that walks one j-plane. Several groups
@@ -378,10 +452,13 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
         const long long e = row * g.kp + k2;
         const long long wd = row * g.kw + (k2 >> 5);
         const uint32_t bit = 1u << (k2 & 31);
+        // F is read whatever the flags say (e is a lattice cell), so that the
+        // flag and F loads make one round trip
+        const float vx = __ldcg(a.Fx + e), vy = __ldcg(a.Fy + e), vz = __ldcg(a.Fz + e);
         const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
-        hx[h] = live ? __ldcg(a.Fx + e) : 0.f;
-        hy[h] = live ? __ldcg(a.Fy + e) : 0.f;
-        hz[h] = live ? __ldcg(a.Fz + e) : 0.f;
+        hx[h] = live ? vx : 0.f;
+        hy[h] = live ? vy : 0.f;
+        hz[h] = live ? vz : 0.f;
     }
     grp.sync();
     for (int lv = lv0; lv < lv1; lv++) {
@@ -451,10 +528,10 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
 // table when they fit the tile, else on global F. The touched flags of the
 // first segment never change, so each pass starts mask_new as a copy of them
 // (mask_static) and the blade walk adds its cells.
-// BULK: the group's tile is [4][tile_cells + 8] words (F x, y, z and the
-// cells' elements), filled by bulk copies of the plane's cell range (bar:
-// the group's mbarrier); the write-back then takes the elements from shared
-// memory. Otherwise the tile is [3][tile_cells] and filled by plain loads.
+// BULK: the group's tile is [3][bulk_tile_stride(tile_cells)] words (F x, y,
+// z), filled by bulk copies of the plane's cell range (bar: the group's
+// mbarrier).
+// Otherwise the tile is [3][tile_cells] and filled by plain loads.
 template <int THREADS, bool BULK = false, typename GRP = PlaneGroup<THREADS>>
 __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int tile_cells, float* tile, const GRP grp,
                                                  uint64_t* bar = nullptr, int* bulk_fail = nullptr) {
@@ -462,25 +539,23 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
     const long long C = a.ncell;
     const bool in_smem = nc <= tile_cells;
     float *fx, *fy, *fz;
-    const int* ce = nullptr;   // BULK: the cells' elements in shared memory
+    prefetch_plane(a, j, c0, nc, grp);
     if (BULK && in_smem && nc > 0) {
-        const int tc = tile_cells + 8;
+        const int tc = bulk_tile_stride(tile_cells);
         const BulkSpan sx = bulk_span(a.cell_F + c0, 0, nc), sy = bulk_span(a.cell_F + C + c0, 0, nc),
-                       sz = bulk_span(a.cell_F + 2 * C + c0, 0, nc), se = bulk_span(a.cell_e + c0, 0, nc);
+                       sz = bulk_span(a.cell_F + 2 * C + c0, 0, nc);
         if (grp.tid() == 0) {
             mbar_init(bar);
             *bulk_fail = 0;
         }
         grp.sync();
         if (grp.tid() == 0) {
-            mbar_expect(bar, sx.bytes + sy.bytes + sz.bytes + se.bytes);
+            mbar_expect(bar, sx.bytes + sy.bytes + sz.bytes);
             bulk_to_smem(tile, sx.src, sx.bytes, bar);
             bulk_to_smem(tile + tc, sy.src, sy.bytes, bar);
             bulk_to_smem(tile + 2 * tc, sz.src, sz.bytes, bar);
-            bulk_to_smem(tile + 3 * tc, se.src, se.bytes, bar);
         }
         fx = tile + sx.off; fy = tile + tc + sy.off; fz = tile + 2 * tc + sz.off;
-        ce = reinterpret_cast<const int*>(tile + 3 * tc) + se.off;
         // bounded wait; the group decides together whether it gave up, so
         // that every thread takes the same barriers
         if (!mbar_wait0(bar, 1 << 20)) *bulk_fail = 1;
@@ -495,11 +570,11 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
                 fx[t] = a.cell_F[c0 + t];
                 fy[t] = a.cell_F[C + c0 + t];
                 fz[t] = a.cell_F[2 * C + c0 + t];
-                reinterpret_cast<int*>(tile + 3 * tc)[se.off + t] = a.cell_e[c0 + t];
             }
         }
     } else if (in_smem) {
         fx = tile; fy = tile + tile_cells; fz = tile + 2 * tile_cells;
+#pragma unroll 4
         for (int t = grp.tid(); t < nc; t += THREADS) {
             fx[t] = a.cell_F[c0 + t];
             fy[t] = a.cell_F[C + c0 + t];
@@ -515,11 +590,7 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
     //      stencil cells of a marker differ (the stencil wraps onto itself
     //      only on a narrower lattice).
     const bool distinct = a.g.nx >= 3 && a.g.nz >= 3;
-    const long long n0 = a.n0;
-    const float* rho = a.cell_m + c0;
-    const float* mx = a.cell_m + C + c0;
-    const float* my = a.cell_m + 2 * C + c0;
-    const float* mz = a.cell_m + 3 * C + c0;
+    const float4* cm = reinterpret_cast<const float4*>(a.cell_m) + c0;   // rho, jx, jy, jz
     for (int lv = a.plane_lv0[j]; lv < a.plane_lv0[j + 1]; lv++) {
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
 #pragma unroll 1
@@ -527,24 +598,32 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
             float w[9], ox[9], oy[9], oz[9];
             int li[9];
+            // the slot's prep row: six float4 loads
+            float4 r[PF_STRIDE / 4];
+            const float4* row = reinterpret_cast<const float4*>(a.prep + (size_t)p * PF_STRIDE);
+#pragma unroll
+            for (int u = 0; u < PF_STRIDE / 4; u++) r[u] = row[u];
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                w[c] = a.prep[(PF_W + c) * n0 + p];
-                li[c] = __float_as_int(a.prep[(PF_CELL + c) * n0 + p]);
+                w[c] = f4_lane(r, PF_W + c);
+                li[c] = __float_as_int(f4_lane(r, PF_CELL + c));
             }
+            float4 m[9];
+#pragma unroll
+            for (int c = 0; c < 9; c++) m[c] = cm[li[c]];
 #pragma unroll
             for (int c = 0; c < 9; c++) {
                 ox[c] = fx[li[c]];
                 oy[c] = fy[li[c]];
                 oz[c] = fz[li[c]];
-                rhoSum = fmaf(w[c], rho[li[c]], rhoSum);
-                xSum = fmaf(w[c], fmaf(0.5f, ox[c], mx[li[c]]), xSum);
-                ySum = fmaf(w[c], fmaf(0.5f, oy[c], my[li[c]]), ySum);
-                zSum = fmaf(w[c], fmaf(0.5f, oz[c], mz[li[c]]), zSum);
+                rhoSum = fmaf(w[c], m[c].x, rhoSum);
+                xSum = fmaf(w[c], fmaf(0.5f, ox[c], m[c].y), xSum);
+                ySum = fmaf(w[c], fmaf(0.5f, oy[c], m[c].z), ySum);
+                zSum = fmaf(w[c], fmaf(0.5f, oz[c], m[c].w), zSum);
             }
-            xSum = fmaf(-rhoSum, a.prep[PF_U * n0 + p], xSum);
-            ySum = fmaf(-rhoSum, a.prep[PF_V * n0 + p], ySum);
-            zSum = fmaf(-rhoSum, a.prep[PF_WV * n0 + p], zSum);
+            xSum = fmaf(-rhoSum, f4_lane(r, PF_U), xSum);
+            ySum = fmaf(-rhoSum, f4_lane(r, PF_V), ySum);
+            zSum = fmaf(-rhoSum, f4_lane(r, PF_WV), zSum);
             a.sums[p] = xSum;
             a.sums[a.n + p] = ySum;
             a.sums[2 * a.n + p] = zSum;
@@ -570,50 +649,52 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
         }
         grp.sync();
     }
-    // ---- write the plane's cells back to F
-    for (int t = grp.tid(); t < nc; t += THREADS) {
-        const int e = BULK && ce ? ce[t] : a.cell_e[c0 + t];
-        a.Fx[e] = fx[t];
-        a.Fy[e] = fy[t];
-        a.Fz[e] = fz[t];
+    // ---- write the plane's cells back to F (four element loads in flight
+    //      per thread)
+    {
+        int t = grp.tid();
+        for (; t + 3 * THREADS < nc; t += 4 * THREADS) {
+            int e[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) e[u] = a.cell_e[c0 + t + u * THREADS];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                a.Fx[e[u]] = fx[t + u * THREADS];
+                a.Fy[e[u]] = fy[t + u * THREADS];
+                a.Fz[e[u]] = fz[t + u * THREADS];
+            }
+        }
+        for (; t < nc; t += THREADS) {
+            const int e = a.cell_e[c0 + t];
+            a.Fx[e] = fx[t];
+            a.Fy[e] = fy[t];
+            a.Fz[e] = fz[t];
+        }
     }
     grp.sync();
 
     // ---- second segment (blades)
     if (a.plane_lv1[j] == a.plane_lv1[j + 1]) return;
-    const int words = BULK ? 4 * (tile_cells + 8) : 3 * tile_cells;
+    const int words = BULK ? 3 * bulk_tile_stride(tile_cells) : 3 * tile_cells;
     if (!blade_levels_tile<THREADS>(a, j, tile, words, grp)) blade_levels_global<THREADS>(a, j, grp);
 }
 
-// G planes per CTA, NT threads each: group g walks plane planes[blockIdx.x *
-// G + g] on its own F tile (G x 3 x tile_cells floats of shared memory) with
-// its own barrier.
-template <int NT, int G>
-__global__ void __launch_bounds__(NT * G, 1) k_ibm_spread(IbmArgs a, const int* __restrict__ planes, int nplanes,
-                                                         int tile_cells) {
-    extern __shared__ float tile[];                             // [G][3][tile_cells]
-    const int g = G == 1 ? 0 : (int)threadIdx.x / NT;
-    const int q = (int)blockIdx.x * G + g;
-    if (q >= nplanes) return;                                   // the whole group: no barrier is left waiting
-    const PlaneGroup<NT, (G > 1)> grp{g * NT, g + 1};
-    ibm_spread_plane<NT>(a, planes[q], tile_cells, tile + (size_t)g * 3 * tile_cells, grp);
-}
-
-// The ordinary planes, G per CTA: group g (NT threads, its own barrier)
-// walks plane planes[blockIdx.x * G + g] on its own tile, which bulk copies
-// fill with one latency whatever the group's size. G planes then share an
-// SM, so all planes of a large lattice are resident at once.
+// G planes per CTA: group g (NT threads, its own barrier) walks plane
+// planes[blockIdx.x * G + g] on its own tile, which bulk copies fill with one
+// latency whatever the group's size. The ordinary planes run G = 1..4 groups
+// of 128 threads, so all planes of a large lattice are resident at once; the
+// big planes (an impeller disk) one group of 512.
 template <int NT, int G>
 __global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_bulk(IbmArgs a, const int* __restrict__ planes, int nplanes,
                                                               int tile_cells) {
-    extern __shared__ __align__(128) float btile[];             // [G][4][tile_cells + 8]
+    extern __shared__ __align__(128) float btile[];             // [G][3][bulk_tile_stride(tile_cells)]
     __shared__ uint64_t bars[G];
     __shared__ int fails[G];
     const int g = G == 1 ? 0 : (int)threadIdx.x / NT;
     const int q = (int)blockIdx.x * G + g;
     if (q >= nplanes) return;
     const PlaneGroup<NT, (G > 1)> grp{g * NT, g + 1};
-    ibm_spread_plane<NT, true>(a, planes[q], tile_cells, btile + (size_t)g * 4 * (tile_cells + 8), grp, &bars[g],
+    ibm_spread_plane<NT, true>(a, planes[q], tile_cells, btile + (size_t)g * 3 * bulk_tile_stride(tile_cells), grp, &bars[g],
                                &fails[g]);
 }
 
@@ -792,13 +873,28 @@ cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
     return e;
 }
 
-// Ordinary planes per CTA: as many 128-thread groups as their tiles (F and
-// the cell elements, 16 bytes per cell) fit in the 227 KB of shared memory a
-// CTA may use, at most 4.
-int spread_groups(int tile_cells) {
-    const size_t per = (size_t)16 * (tile_cells + 8);
-    const int G = (int)((227 * 1024 - 64) / per);
-    return G < 1 ? 1 : (G > 4 ? 4 : G);
+// Ordinary planes per CTA: as few 128-thread groups as put every plane on
+// the GPU at once (nplanes / SMs, rounded up), at most as many as their F
+// tiles (12 bytes per cell) fit in the 227 KB of shared memory a CTA may use,
+// and at most 4: groups of one CTA share its SM's load/store pipe. (At 400^3
+// the 399 ordinary planes hold 5214 cells each: 3 groups, 133 CTAs.)
+static int sm_count() {
+    static int n[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (n[dev] == 0) {
+        int v = 0;
+        n[dev] = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0 ? v : 148;
+    }
+    return n[dev];
+}
+int spread_groups(int tile_cells, int nplanes) {
+    const size_t per = (size_t)12 * bulk_tile_stride(tile_cells);
+    int G = (int)((227 * 1024 - 64) / per);
+    G = G < 1 ? 1 : (G > 4 ? 4 : G);
+    const int sms = sm_count();
+    const int want = nplanes > 0 ? (nplanes + sms - 1) / sms : 1;
+    return want < G ? (want < 1 ? 1 : want) : G;
 }
 
 template <int G>
@@ -807,17 +903,21 @@ static const void* spread_bulk_fn() { return (const void*)k_ibm_spread_bulk<128,
 template <int G>
 static void spread_small(const IbmArgs& a, cudaStream_t st) {
     const unsigned grid = (unsigned)((a.n_small + G - 1) / G);
-    const size_t bytes = (size_t)G * 16 * (a.smem_cells + 8);
+    const size_t bytes = (size_t)G * 12 * bulk_tile_stride(a.smem_cells);
     k_ibm_spread_bulk<128, G><<<grid, 128 * G, bytes, st>>>(a, a.plane_list, a.n_small, a.smem_cells);
 }
 
-cudaError_t ibm_prepare_smem(int small_cells, size_t big_bytes) {
-    const int G = spread_groups(small_cells);
+// Shared memory of the big planes' launch (one 512-thread group, a bulk
+// tile of big_cells cells; none when the tile does not fit).
+size_t big_bulk_bytes(int big_cells) { return big_cells > 0 ? (size_t)12 * bulk_tile_stride(big_cells) : 0; }
+
+cudaError_t ibm_prepare_smem(int small_cells, int n_small, size_t big_bytes) {
+    const int G = spread_groups(small_cells, n_small);
     const void* fn = G == 4 ? spread_bulk_fn<4>() : G == 3 ? spread_bulk_fn<3>() : G == 2 ? spread_bulk_fn<2>()
                                                                                        : spread_bulk_fn<1>();
-    cudaError_t e = raise_smem_limit(fn, (size_t)G * 16 * (small_cells + 8));
+    cudaError_t e = raise_smem_limit(fn, (size_t)G * 12 * bulk_tile_stride(small_cells));
     if (e != cudaSuccess) return e;
-    return raise_smem_limit((const void*)k_ibm_spread<512, 1>, big_bytes);
+    return raise_smem_limit((const void*)k_ibm_spread_bulk<512, 1>, big_bytes);
 }
 
 cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, cudaStream_t st) {
@@ -833,37 +933,47 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
         with_storage(a.storage,
                      [&](auto s) { k_ibm_cells<decltype(s)><<<(count + 255) / 256, 256, 0, st>>>(a, first, count); });
     };
+    auto tail = [&](cudaStream_t ts) {
+        if (a.n <= a.n0) return;
+        const unsigned b = (unsigned)((9LL * (a.n - a.n0) + 127) / 128);
+        with_storage(a.storage, [&](auto s) { k_ibm_gather_tail<decltype(s)><<<b, 128, 0, ts>>>(a); });
+    };
     // mask_new starts as the first segment's (static) touched cells
     cudaError_t err = cudaMemcpyAsync(a.mask_new, a.mask_static, a.mask_bytes, cudaMemcpyDeviceToDevice, st);
     if (err != cudaSuccess) return err;
-    const bool split = a.n_big > 0 && a.cell_order;
-    // Planes with many cells (an impeller disk) run on a side stream with a
-    // full-size tile and 512 threads. Their cells are prepared first, so that
-    // their spread starts while the other planes' cells are prepared: a
-    // big-plane block needs a whole SM's shared memory, which it would not
-    // find once the small-plane spread has spread its blocks over the SMs.
-    cells(0, split ? a.ncell_big : a.ncell);
-    if (a.n > a.n0) {
-        const unsigned b = (a.n - a.n0 + 127) / 128;
-        with_storage(a.storage, [&](auto s) { k_ibm_gather_tail<decltype(s)><<<b, 128, 0, st>>>(a); });
-    }
-    err = cudaGetLastError();
-    if (err != cudaSuccess) return err;
-    if (a.n_big > 0) {
+    if (a.n_big == 0) {
+        cells(0, a.ncell);
+        tail(st);
+    } else {
+        // Planes with many cells (an impeller disk) run on a side stream with
+        // a full-size tile and 512 threads. Their cells are prepared first,
+        // so that their spread starts while the other planes' cells are
+        // prepared: a big-plane block needs a whole SM's shared memory, which
+        // it would not find once the ordinary planes' spread has placed its
+        // blocks over the SMs. The blade markers' gather (which reads only
+        // the state) runs on the side stream too, beside the other planes'
+        // cells; both spreads wait for it.
+        const bool split = a.cell_order != nullptr;
+        cells(0, split ? a.ncell_big : a.ncell);
         err = cudaEventRecord(a.ev_fork, st);
         if (err != cudaSuccess) return err;
         err = cudaStreamWaitEvent(a.side, a.ev_fork, 0);
         if (err != cudaSuccess) return err;
-        k_ibm_spread<512, 1><<<a.n_big, 512, ibm_smem_bytes(a.g, a.big_tile_cells), a.side>>>(
+        tail(a.side);
+        err = cudaEventRecord(a.ev_tail, a.side);
+        if (err != cudaSuccess) return err;
+        k_ibm_spread_bulk<512, 1><<<a.n_big, 512, big_bulk_bytes(a.big_tile_cells), a.side>>>(
             a, a.plane_list + a.n_small, a.n_big, a.big_tile_cells);
         err = cudaGetLastError();
         if (err != cudaSuccess) return err;
         err = cudaEventRecord(a.ev_join, a.side);
         if (err != cudaSuccess) return err;
+        if (split) cells(a.ncell_big, a.ncell - a.ncell_big);
+        err = cudaStreamWaitEvent(st, a.ev_tail, 0);
+        if (err != cudaSuccess) return err;
     }
-    if (split) cells(a.ncell_big, a.ncell - a.ncell_big);
     if (a.n_small > 0) {
-        switch (spread_groups(a.smem_cells)) {
+        switch (spread_groups(a.smem_cells, a.n_small)) {
             case 4: spread_small<4>(a, st); break;
             case 3: spread_small<3>(a, st); break;
             case 2: spread_small<2>(a, st); break;
@@ -944,7 +1054,7 @@ template <int NT, int G>
 __global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_batch_bulk(const IbmArgs* __restrict__ args,
                                                                     const int2* __restrict__ work, int nwork,
                                                                     int region_cells) {
-    extern __shared__ __align__(128) float btile[];             // [G][4][region_cells + 8]
+    extern __shared__ __align__(128) float btile[];             // [G][3][bulk_tile_stride(region_cells)]
     __shared__ IbmArgs sa[G];
     __shared__ uint64_t bars[G];
     __shared__ int fails[G];
@@ -957,14 +1067,14 @@ __global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_batch_bulk(const IbmAr
     for (int i = grp.tid(); i < words; i += NT)
         reinterpret_cast<unsigned long long*>(&sa[g])[i] = reinterpret_cast<const unsigned long long*>(args + w.x)[i];
     grp.sync();
-    ibm_spread_plane<NT, true>(sa[g], w.y, sa[g].smem_cells, btile + (size_t)g * 4 * (region_cells + 8), grp, &bars[g],
+    ibm_spread_plane<NT, true>(sa[g], w.y, sa[g].smem_cells, btile + (size_t)g * 3 * bulk_tile_stride(region_cells), grp, &bars[g],
                                &fails[g]);
 }
 
 // Work items per CTA of the batched ordinary-plane spread for tiles of
 // `cells` cells (as spread_groups, leaving room for the staged arguments).
 static int batch_spread_groups(int cells) {
-    const size_t per = (size_t)16 * (cells + 8) + sizeof(IbmArgs) + 16;
+    const size_t per = (size_t)12 * bulk_tile_stride(cells) + sizeof(IbmArgs) + 16;
     const int G = (int)((227 * 1024 - 256) / per);
     return G < 1 ? 1 : (G > 4 ? 4 : G);
 }
@@ -989,7 +1099,7 @@ cudaError_t ibm_batch_prepare_smem(size_t small_bytes, size_t big_bytes) {
 template <int G>
 static void batch_spread_small(const IbmBatch& b, cudaStream_t st) {
     const unsigned grid = (unsigned)((b.n_small + G - 1) / G);
-    const size_t bytes = (size_t)G * 16 * (b.small_tile + 8);
+    const size_t bytes = (size_t)G * 12 * bulk_tile_stride(b.small_tile);
     k_ibm_spread_batch_bulk<128, G><<<grid, 128 * G, bytes, st>>>(b.args, b.small, b.n_small, b.small_tile);
 }
 

@@ -59,7 +59,7 @@ static cudaError_t launch_simple_v(const StepArgs& a, cudaStream_t st) {
     const dim3 grid(step_blocks(a, V)), block(128);
 #define TDLB_SIMPLE(LES, FM, COL, PART)                                                                       \
     k_step_simple<float, V, LES, FM, COL, PART><<<grid, block, 0, st>>>(a.A, a.B, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, \
-                                                                      a.g, a.p, a.zone, ResidualBox{}, ResidualBox{})
+                                                                      a.g, a.p, a.zone, ResidualBox{}, BoxOut{})
     if (!a.collide) TDLB_SIMPLE(false, false, false, 0);
     else if (a.from_moments) { if (a.les) TDLB_SIMPLE(true, true, true, 0); else TDLB_SIMPLE(false, true, true, 0); }
     else if constexpr (V == 1) {
@@ -81,8 +81,8 @@ static cudaError_t launch_simple_v(const StepArgs& a, cudaStream_t st) {
 
 template <int V, bool LES, bool FM, bool COL, int PART>
 static void eso_launch(const StepArgs& a, dim3 grid, cudaStream_t st) {
-    if (a.even) k_step_esotwist<float, V, LES, FM, COL, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone, ResidualBox{});
-    else k_step_esotwist<float, V, LES, FM, COL, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone, ResidualBox{});
+    if (a.even) k_step_esotwist<float, V, LES, FM, COL, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone, ResidualBox{}, BoxOut{});
+    else k_step_esotwist<float, V, LES, FM, COL, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.Fx, a.Fy, a.Fz, a.mask, a.g, a.p, a.zone, ResidualBox{}, BoxOut{});
 }
 
 template <int V>
@@ -110,6 +110,7 @@ static cudaError_t launch_esotwist_v(const StepArgs& a, cudaStream_t st) {
 cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st) {
     if (a.part != 0 && (a.vec != 1 || a.from_moments || !a.collide)) return cudaErrorInvalidValue;
     if (a.storage != STORE_F32) return launch_step_simple_h16(a, st);
+    if (a.box != 0) return cudaErrorInvalidValue;   // no residual box for FP32 storage
     switch (a.vec) {
         case 1: return launch_simple_v<1>(a, st);
         case 2: return launch_simple_v<2>(a, st);
@@ -120,6 +121,7 @@ cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st) {
 cudaError_t launch_step_esotwist(const StepArgs& a, cudaStream_t st) {
     if (a.part != 0 && (a.vec != 1 || a.from_moments || !a.collide)) return cudaErrorInvalidValue;
     if (a.storage != STORE_F32) return launch_step_esotwist_h16(a, st);
+    if (a.box != 0) return cudaErrorInvalidValue;   // no residual box for FP32 storage
     switch (a.vec) {
         case 1: return launch_esotwist_v<1>(a, st);
         case 2: return launch_esotwist_v<2>(a, st);

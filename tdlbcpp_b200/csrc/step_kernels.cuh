@@ -221,27 +221,29 @@ __device__ __forceinline__ void collide_quad(float (&f)[NQ][V], const Quad& q, f
 
 // ---------------------------------------------------------------------------
 // Residual box (16-bit storage, one cell per thread; tdlb::ResidualBox).
-// Called functions rather than inlined: only the warps near the box call
-// them, and the issue-bound step kernels keep their straight-line code and
-// registers. f holds the cell's 18 values in direction order.
+// A step with a box runs three launches:
+//   the box launch (BOX = 2): the 32-cell chunks with a cell near the box,
+//     from a list, with the residuals of their locations (the code below,
+//     inlined), into a scratch array (BoxOut) -- before the plain launch
+//     overwrites their populations (Esotwist) and their Nu, which the LES
+//     collision reads;
+//   the plain launch: every cell, without residuals;
+//   k_box_commit: the box chunks' exact outputs over the plain ones, with the
+//     residuals of the locations inside the box.
+// The plain kernel so stays as it is. f holds the cell's 18 values in
+// direction order.
 // ---------------------------------------------------------------------------
 // Simple: add the residuals of the source locations inside the box (x - c_d,
 // or the cell itself where x - c_d is off the lattice).
-static __device__ __noinline__ void box_pull_simple(const ResidualBox rr, int i, int j, int k, int nx, int ny, int nz,
-                                             float* f) {
+__device__ __forceinline__ void box_pull_simple(const ResidualBox& rr, int i, int j, int k, const Dims& g,
+                                                float (&f)[NQ][1]) {
 #pragma unroll
     for (int d = 0; d < NQ; d++) {
         const int si = i - cx_of(d), sj = j - cy_of(d), sk = k - cz_of(d);
-        const bool in = (unsigned)si < (unsigned)nx && (unsigned)sj < (unsigned)ny && (unsigned)sk < (unsigned)nz;
+        const bool in = (unsigned)si < (unsigned)g.nx && (unsigned)sj < (unsigned)g.ny && (unsigned)sk < (unsigned)g.nz;
         const int li = in ? si : i, lj = in ? sj : j, lk = in ? sk : k;
-        if (rr.contains(li, lj, lk)) f[d] += *rr.at(d, li, lj, lk);
+        if (rr.contains(li, lj, lk)) f[d][0] += *rr.at(d, li, lj, lk);
     }
-}
-// Simple: the residuals of the cell's own 18 outputs.
-template <typename S>
-__device__ __noinline__ void box_store_simple(const ResidualBox rw, int i, int j, int k, const float* f) {
-#pragma unroll
-    for (int d = 0; d < NQ; d++) *rw.at(d, i, j, k) = f[d] - Storage<S>::dec(Storage<S>::enc(f[d]));
 }
 // Esotwist: slot s of cell (i, j, k) lives at (li, lj, lk); on reading, it
 // holds direction EVEN ? s : s ^ 1, on writing EVEN ? s ^ 1 : s.
@@ -254,27 +256,15 @@ __device__ __forceinline__ void eso_location(int s, int i, int j, int k, int i1,
     lk = sg * cz_of(s) > 0 ? k1 : k;
 }
 template <bool EVEN>
-__device__ __noinline__ void box_read_eso(const ResidualBox rb, int i, int j, int k, int i1, int j1, int k1,
-                                          float* f) {
+__device__ __forceinline__ void box_read_eso(const ResidualBox& rb, int i, int j, int k, int i1, int j1, int k1,
+                                             float (&f)[NQ][1]) {
 #pragma unroll
     for (int s = 0; s < NQ; s++) {
         int li, lj, lk;
         eso_location<EVEN>(s, i, j, k, i1, j1, k1, li, lj, lk);
-        if (rb.contains(li, lj, lk)) f[EVEN ? s : (s ^ 1)] += *rb.at(s, li, lj, lk);
+        if (rb.contains(li, lj, lk)) f[EVEN ? s : (s ^ 1)][0] += *rb.at(s, li, lj, lk);
     }
 }
-template <typename S, bool EVEN>
-__device__ __noinline__ void box_write_eso(const ResidualBox rb, int i, int j, int k, int i1, int j1, int k1,
-                                           const float* f) {
-#pragma unroll
-    for (int s = 0; s < NQ; s++) {
-        int li, lj, lk;
-        eso_location<EVEN>(s, i, j, k, i1, j1, k1, li, lj, lk);
-        const float v = f[EVEN ? (s ^ 1) : s];
-        if (rb.contains(li, lj, lk)) *rb.at(s, li, lj, lk) = v - Storage<S>::dec(Storage<S>::enc(v));
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Simple (A/B, pull).
 //
@@ -287,13 +277,14 @@ __device__ __noinline__ void box_write_eso(const ResidualBox rb, int i, int j, i
 // scalar loads issued in the same batch (in bounds for every lane; the ones
 // a lane does not need hit L1).
 // ---------------------------------------------------------------------------
-template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool FORCE = true>
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool FORCE = true, int BOX = 0>
 __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, float* __restrict__ Nu,
                                             const float* __restrict__ Fx, const float* __restrict__ Fy,
                                             const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
                                             const Dims& g, const CollideParams& p, unsigned t,
-                                            const ResidualBox rr = ResidualBox{}, const ResidualBox rw = ResidualBox{}) {
+                                            const ResidualBox rr = ResidualBox{}, const BoxOut out = BoxOut{}) {
     static_assert(!(Storage<S>::deviation && FROM_MOMENTS), "16-bit state always holds populations");
+    static_assert(BOX == 0 || (Storage<S>::deviation && V == 1), "the residual box serves 16-bit storage, one cell per thread");
     const int nq = g.kp / V;
     const Quad q = quad_of<V, sizeof(S) == 2>(g, nq, t);
     const int lane = threadIdx.x & 31;
@@ -316,9 +307,9 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
             const int off = in ? -(cx * rs + cy * g.kp + cz) : 0;
             f[d][0] = pload1<S, true>(A.p[d], q.e0 + off);
         }
-        if constexpr (Storage<S>::deviation) {
+        if constexpr (BOX == 2) {
             // residual box: the exact deviation of every source location inside it
-            if (q.active && rr.near(q.i, q.j, q.k0)) box_pull_simple(rr, q.i, q.j, q.k0, g.nx, g.ny, g.nz, &f[0][0]);
+            if (q.active && rr.near(q.i, q.j, q.k0)) box_pull_simple(rr, q.i, q.j, q.k0, g, f);
         }
     } else {
         float hal[NQ], own[NQ];
@@ -383,13 +374,19 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
     // keeps IEEE rounding, measured slower with them, 1.38 -> 1.47 ms)
     collide_quad<V, LES, COLLIDE, Storage<S>::deviation, FORCE, Storage<S>::deviation>(f, q, Nu, Fx, Fy, Fz, mask, g,
                                                                                        p, FROM_MOMENTS, nu);
+    if constexpr (BOX == 2) {
+        // box launch: the exact outputs and Nu to the scratch array (entry
+        // blockIdx.x * 128 + threadIdx.x of the chunk list)
+        const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+        for (int d = 0; d < NQ; d++) out.v[(long long)d * out.n + o] = f[d][0];
+        out.v[(long long)NQ * out.n + o] = nu[0];
+        return;
+    }
     if (!q.active) return;
 #pragma unroll
     for (int d = 0; d < NQ; d++) pstore<S, V>(B.p[d], q.e0, f[d]);
     if (COLLIDE && LES) vstore<V>(Nu + q.e0, nu);
-    if constexpr (Storage<S>::deviation && V == 1) {
-        if (rw.on() && rw.contains(q.i, q.j, q.k0)) box_store_simple<S>(rw, q.i, q.j, q.k0, &f[0][0]);
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -406,12 +403,14 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
 // loads from any lane's stores, so a location is always read by its owner
 // before a neighbour overwrites it.
 // ---------------------------------------------------------------------------
-template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN, bool FORCE = true>
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN, bool FORCE = true, int BOX = 0>
 __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict__ Nu, const float* __restrict__ Fx,
                                               const float* __restrict__ Fy, const float* __restrict__ Fz,
                                               const uint32_t* __restrict__ mask, const Dims& g, const CollideParams& p,
-                                              unsigned t, const ResidualBox rb = ResidualBox{}) {
+                                              unsigned t, const ResidualBox rb = ResidualBox{},
+                                              const BoxOut out = BoxOut{}) {
     static_assert(!(Storage<S>::deviation && FROM_MOMENTS), "16-bit state always holds populations");
+    static_assert(BOX == 0 || (Storage<S>::deviation && V == 1), "the residual box serves 16-bit storage, one cell per thread");
     const int nq = g.kp / V;
     const Quad q = quad_of<V, sizeof(S) == 2>(g, nq, t);
     const int lane = threadIdx.x & 31;
@@ -449,10 +448,10 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
                 f[d][0] = v[s];
             }
         }
-        if constexpr (Storage<S>::deviation) {
+        if constexpr (BOX == 2) {
             // residual box: the exact deviation of every location inside it
             // (slot s of this cell lives at cell (li, lj, lk))
-            if (q.active && rb.near(q.i, q.j, q.k0)) box_read_eso<EVEN>(rb, q.i, q.j, q.k0, i1, j1, k1, &f[0][0]);
+            if (q.active && rb.near(q.i, q.j, q.k0)) box_read_eso<EVEN>(rb, q.i, q.j, q.k0, i1, j1, k1, f);
         }
     } else {
         float hal[NQ], wrap[NQ];
@@ -489,6 +488,15 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
     __syncwarp();
     float nu[V];
     collide_quad<V, LES, COLLIDE, Storage<S>::deviation, FORCE>(f, q, Nu, Fx, Fy, Fz, mask, g, p, FROM_MOMENTS, nu);
+    if constexpr (BOX == 2) {
+        // box launch: the exact outputs, slot by slot, and Nu to the scratch
+        // array (entry blockIdx.x * 128 + threadIdx.x of the chunk list)
+        const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+        for (int s = 0; s < NQ; s++) out.v[(long long)s * out.n + o] = f[EVEN ? (s ^ 1) : s][0];
+        out.v[(long long)NQ * out.n + o] = nu[0];
+        return;
+    }
     if (V == 1) {
         // Slots with a k offset write element k + 1: lane l writes element k
         // with the value of the previous lane (cell k - 1, same row), so the
@@ -513,9 +521,6 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
             if (q.active && (warp_end || row_end)) pstore1<S>(Q.p[s], base + k1, f[d][0]);
         }
         if (COLLIDE && LES && q.active) Nu[q.e0] = nu[0];
-        if constexpr (Storage<S>::deviation) {
-            if (q.active && rb.near(q.i, q.j, q.k0)) box_write_eso<S, EVEN>(rb, q.i, q.j, q.k0, i1, j1, k1, &f[0][0]);
-        }
         return;
     }
     const bool k_first = q.k0 == 0;
@@ -573,16 +578,17 @@ __device__ __forceinline__ bool part_thread(const StepPart& part, unsigned& t) {
     return true;
 }
 
-template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, int PART = 0>
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, int PART = 0, int BOX = 0>
 __global__ void __launch_bounds__(128, 4) k_step_simple(Planes A, Planes B, float* __restrict__ Nu,
                                                        const float* __restrict__ Fx, const float* __restrict__ Fy,
                                                        const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
                                                        Dims g, CollideParams p, StepPart part, ResidualBox rr,
-                                                       ResidualBox rw) {
+                                                       BoxOut out) {
     static_assert(PART == 0 || V == 1, "split steps run one cell per thread");
+    static_assert(BOX != 2 || PART != 0, "the box path runs a chunk list");
     unsigned t;
     if (!part_thread<PART>(part, t)) return;   // whole warps
-    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE, PART != 1>(A, B, Nu, Fx, Fy, Fz, mask, g, p, t, rr, rw);
+    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE, PART != 1, BOX>(A, B, Nu, Fx, Fy, Fz, mask, g, p, t, rr, out);
 }
 
 // Resident 128-thread blocks per SM the Esotwist kernel is built for: the
@@ -591,15 +597,46 @@ __global__ void __launch_bounds__(128, 4) k_step_simple(Planes A, Planes B, floa
 template <int V>
 constexpr int kEsotwistBlocksPerSM = V == 1 ? 8 : (V == 2 ? 6 : 4);
 
-template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN, int PART = 0>
-__global__ void __launch_bounds__(128, kEsotwistBlocksPerSM<V>) k_step_esotwist(Planes Q, float* __restrict__ Nu,
+template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN, int PART = 0, int BOX = 0>
+__global__ void __launch_bounds__(128, BOX == 2 ? 4 : kEsotwistBlocksPerSM<V>) k_step_esotwist(Planes Q, float* __restrict__ Nu,
                                                          const float* __restrict__ Fx, const float* __restrict__ Fy,
                                                          const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
-                                                         Dims g, CollideParams p, StepPart part, ResidualBox rb) {
+                                                         Dims g, CollideParams p, StepPart part, ResidualBox rb,
+                                                         BoxOut out) {
     static_assert(PART == 0 || V == 1, "split steps run one cell per thread");
+    static_assert(BOX != 2 || PART != 0, "the box path runs a chunk list");
     unsigned t;
     if (!part_thread<PART>(part, t)) return;   // whole warps
-    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN, PART != 1>(Q, Nu, Fx, Fy, Fz, mask, g, p, t, rb);
+    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN, PART != 1, BOX>(Q, Nu, Fx, Fy, Fz, mask, g, p, t, rb, out);
+}
+
+// After the plain launch of a step with a residual box: every cell of the box
+// chunks takes the outputs its box launch computed (entry blockIdx.x * 128 +
+// threadIdx.x of `out`): Simple stores direction d to its own cell of plane d
+// of Q (the destination buffer), Esotwist slot s to the slot's location;
+// the residuals of the locations inside the box (rb: the destination's set)
+// and Nu go with them.
+template <typename S, bool SIMPLE, bool EVEN>
+__global__ void __launch_bounds__(128) k_box_commit(Planes Q, float* __restrict__ Nu, Dims g, StepPart part,
+                                                    ResidualBox rb, BoxOut out, int les) {
+    unsigned t;
+    if (!part_thread<2>(part, t)) return;
+    const Quad q = quad_of<1, true>(g, g.kp, t);
+    if (!q.active) return;
+    const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i1 = q.i + 1 == g.nx ? 0 : q.i + 1;
+    const int j1 = q.j + 1 == g.ny ? 0 : q.j + 1;
+    const int k1 = q.k0 + 1 == g.nz ? 0 : q.k0 + 1;
+#pragma unroll
+    for (int s = 0; s < NQ; s++) {
+        int li = q.i, lj = q.j, lk = q.k0;
+        if (!SIMPLE) eso_location<EVEN>(s, q.i, q.j, q.k0, i1, j1, k1, li, lj, lk);
+        const float v = out.v[(long long)s * out.n + o];
+        const S enc = Storage<S>::enc(v);
+        reinterpret_cast<S*>(Q.p[s])[((long long)li * g.ny + lj) * g.kp + lk] = enc;
+        if (rb.contains(li, lj, lk)) *rb.at(s, li, lj, lk) = v - Storage<S>::dec(enc);
+    }
+    if (les) Nu[q.e0] = out.v[(long long)NQ * out.n + o];
 }
 
 // Moments of the current state at every interior cell (what the reference's

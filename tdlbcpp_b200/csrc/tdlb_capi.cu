@@ -69,11 +69,14 @@ void release(tdlb_lattice* h) {
     cudaFree(h->d_plane_list);
     cudaFree(h->d_exclude);
     cudaFree(h->d_zone_list);
+    cudaFree(h->d_box_list);
+    cudaFree(h->d_box_out);
     for (cudaEvent_t e : h->tev) cudaEventDestroy(e);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->ibm) cudaStreamDestroy(h->ibm);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->ev_tail) cudaEventDestroy(h->ev_tail);
     if (h->ev_outer) cudaEventDestroy(h->ev_outer);
     if (h->ev_inner) cudaEventDestroy(h->ev_inner);
     if (h->ev_sync) cudaEventDestroy(h->ev_sync);
@@ -134,6 +137,7 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
         TDLB_CK(cudaStreamCreateWithPriority(&h->ibm, cudaStreamNonBlocking, prio_hi));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+        TDLB_CK(cudaEventCreateWithFlags(&h->ev_tail, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_outer, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_inner, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_sync, cudaEventDisableTiming));
@@ -416,7 +420,54 @@ bool split_capable(tdlb_lattice* h) {
     return h->zone_ok && (h->zone_small || h->overlap == 2);
 }
 
-bool can_split(tdlb_lattice* h) { return !h->holds_moments && split_capable(h); }
+// (A step with a residual box runs unsplit: its box launch reads the box
+// chunks' populations and Nu before the plain launch writes them.)
+bool can_split(tdlb_lattice* h) {
+    if (h->rbox_geom.n) return false;
+    return !h->holds_moments && split_capable(h);
+}
+
+// The chunks with a cell near the residual box (ResidualBox::near), which the
+// box launch of a step runs, and that launch's scratch outputs.
+void build_box_list(tdlb_lattice* h) {
+    if (h->box_list_gen == h->box_gen) return;
+    TDLB_CK(tdlb_rt::join_side(h));
+    TDLB_CK(cudaStreamSynchronize(h->stream));   // no launch still reads the old list
+    const Dims& g = h->g;
+    const tdlb::ResidualBox& b = h->rbox_geom;
+    const long long nchunks = (g.rows() * g.kp + 31) / 32;
+    std::vector<uint8_t> hit((size_t)nchunks, 0);
+    for (int i = std::max(0, b.i0 - 1); i <= std::min(g.nx - 1, b.i0 + b.bx); i++)
+        for (int j = std::max(0, b.j0 - 1); j <= std::min(g.ny - 1, b.j0 + b.by); j++)
+            for (int k = std::max(0, b.k0 - 1); k <= std::min(g.nz - 1, b.k0 + b.bz); k++)
+                if (b.around(i, j, k)) hit[(size_t)((((long long)i * g.ny + j) * g.kp + k) >> 5)] = 1;
+    std::vector<int> list;
+    for (long long c = 0; c < nchunks; c++)
+        if (hit[(size_t)c]) list.push_back((int)c);
+    if ((long long)list.size() > h->box_list_cap || !h->d_box_list) {
+        cudaFree(h->d_box_list);
+        h->d_box_list = nullptr;
+        h->box_list_cap = 0;
+        TDLB_CK(cudaMalloc(&h->d_box_list, std::max<size_t>(list.size(), 1) * sizeof(int)));
+        h->box_list_cap = (long long)std::max<size_t>(list.size(), 1);
+    }
+    {
+        // one entry per thread of the box launch (128-thread blocks)
+        const long long need = (long long)(tdlb::NQ + 1) * (((long long)list.size() * 32 + 127) / 128 * 128);
+        if (need > h->box_out_cap || !h->d_box_out) {
+            cudaFree(h->d_box_out);
+            h->d_box_out = nullptr;
+            h->box_out_cap = 0;
+            TDLB_CK(cudaMalloc(&h->d_box_out, (size_t)std::max<long long>(need, 1) * sizeof(float)));
+            h->box_out_cap = std::max<long long>(need, 1);
+        }
+    }
+    if (!list.empty())
+        TDLB_CK(cudaMemcpyAsync(h->d_box_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    TDLB_CK(cudaStreamSynchronize(h->stream));
+    h->n_box = (int)list.size();
+    h->box_list_gen = h->box_gen;
+}
 
 // Queue one step-kernel launch, bracketed by timing events when enabled.
 template <typename L>
@@ -445,6 +496,17 @@ void run_step(tdlb_lattice* h, bool collide) {
     auto launch = [&](const tdlb::StepArgs& x, cudaStream_t st) {
         return simple ? tdlb::launch_step_simple(x, st) : tdlb::launch_step_esotwist(x, st);
     };
+    // With a residual box: the box launch (the chunks near the box, with
+    // residuals, into scratch), the plain launch, then the commit of the box
+    // chunks' outputs (step_kernels.cuh). Such a step is never split.
+    const bool boxed = a.rr.on();
+    if (boxed) build_box_list(h);
+    tdlb::StepArgs bx = a;
+    bx.box = 2;
+    bx.part = 2;
+    bx.zone = tdlb::StepPart{h->d_box_list, h->n_box};
+    bx.bout = tdlb::BoxOut{h->d_box_out, ((long long)h->n_box * 32 + 127) / 128 * 128};
+    const bool run_box = boxed && h->n_box > 0;
     if (collide && can_split(h)) {
         cudaStream_t side = loop_stream(h);
         if (h->inner_queued) TDLB_CK(cudaStreamWaitEvent(h->stream, h->ev_inner, 0));
@@ -464,7 +526,9 @@ void run_step(tdlb_lattice* h, bool collide) {
         h->inner_queued = true;
     } else {
         TDLB_CK(tdlb_rt::join_side(h));
+        if (run_box) timed_launch(h, h->stream, [&] { return launch(bx, h->stream); });
         timed_launch(h, h->stream, [&] { return launch(a, h->stream); });
+        if (run_box) timed_launch(h, h->stream, [&] { return tdlb::launch_box_commit(bx, simple, h->stream); });
     }
     if (simple) h->cur ^= 1;
     else h->even = !h->even;   // StreamingEsoteric.hpp:15-18
@@ -557,13 +621,13 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
     h->d_cell_e = nullptr; h->d_plane_cell = nullptr; h->d_prep = nullptr; h->d_cell_m = nullptr; h->d_cell_F = nullptr;
     TDLB_CK(cudaMalloc(&h->d_plane_cell, (size_t)(g.ny + 1) * sizeof(int)));
     if (C0) {
-        // 16 elements of padding: the spread's bulk copies round a plane's
-        // cell range out to 16-byte boundaries
+        // 16 elements of padding: the spread's bulk copies and L2 prefetches
+        // round a plane's cell range out to 16-byte boundaries
         TDLB_CK(cudaMalloc(&h->d_cell_e, (C0 + 16) * sizeof(int)));
-        TDLB_CK(cudaMalloc(&h->d_cell_m, 4 * C0 * sizeof(float)));
+        TDLB_CK(cudaMalloc(&h->d_cell_m, (4 * C0 + 16) * sizeof(float)));
         TDLB_CK(cudaMalloc(&h->d_cell_F, (3 * C0 + 16) * sizeof(float)));
     }
-    if (n0) TDLB_CK(cudaMalloc(&h->d_prep, (size_t)tdlb::PF_COUNT * n0 * sizeof(float)));
+    if (n0) TDLB_CK(cudaMalloc(&h->d_prep, ((size_t)tdlb::PF_STRIDE * n0 + 16) * sizeof(float)));
     {
         // F tiles of the ordinary planes' launch: up to 6144 cells (72 KB)
         // of shared memory;
@@ -587,8 +651,8 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
         h->smem_cells = small_cap;
         h->n_small = (int)small.size();
         h->n_big = (int)big.size();
-        h->big_tile_cells = tdlb::ibm_smem_bytes(g, big_max) <= 220 * 1024 ? big_max : 0;
-        TDLB_CK(tdlb::ibm_prepare_smem(h->smem_cells, tdlb::ibm_smem_bytes(g, h->big_tile_cells)));
+        h->big_tile_cells = tdlb::big_bulk_bytes(big_max) <= 220 * 1024 ? big_max : 0;
+        TDLB_CK(tdlb::ibm_prepare_smem(h->smem_cells, h->n_small, tdlb::big_bulk_bytes(h->big_tile_cells)));
         // cell order of the pass: the big planes' cells, then the others
         cudaFree(h->d_cell_order);
         h->d_cell_order = nullptr;
@@ -638,8 +702,9 @@ void upload_markers(tdlb_lattice* h, const tdlb_marker* m, size_t n, size_t n0, 
                             cudaMemcpyHostToDevice, h->stream));
     if (C0) TDLB_CK(cudaMemcpyAsync(h->d_cell_e, h->cells.cell_e.data(), C0 * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     if (n0) {
-        TDLB_CK(cudaMemcpyAsync(h->d_prep + (size_t)tdlb::PF_CELL * n0, h->cells.mcell.data(), (size_t)9 * n0 * sizeof(int),
-                                cudaMemcpyHostToDevice, h->stream));
+        // the 9 cell indices of each slot into its prep row
+        TDLB_CK(cudaMemcpy2DAsync(h->d_prep + tdlb::PF_CELL, tdlb::PF_STRIDE * sizeof(float), h->cells.mcell.data(),
+                                  9 * sizeof(int), 9 * sizeof(int), (size_t)n0, cudaMemcpyHostToDevice, h->stream));
         tdlb::IbmArgs a = ibm_args(h, 0.f, 0.f);
         TDLB_CK(tdlb::launch_ibm_prepare(a, h->d_prep, nullptr, h->stream));
     }
@@ -678,6 +743,7 @@ tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     a.side = h->side;
     a.ev_fork = h->ev_fork;
     a.ev_join = h->ev_join;
+    a.ev_tail = h->ev_tail;
     a.A = h->planes(h->state_buf());
     a.state_mode = h->state_mode();
     a.even = h->even ? 1 : 0;
@@ -772,6 +838,7 @@ void drop_rbox(tdlb_lattice* h) {
     cudaFree(h->d_res[1]);
     h->d_res[0] = h->d_res[1] = nullptr;
     h->rbox_geom = tdlb::ResidualBox{};
+    h->box_gen++;
 }
 
 // The box [i0, i1) x [j0, j1) x [k0, k1); an empty one removes the box. The
@@ -779,8 +846,11 @@ void drop_rbox(tdlb_lattice* h) {
 // and steps refine the locations inside the box from then on.
 void set_rbox(tdlb_lattice* h, long long i0, long long i1, long long j0, long long j1, long long k0, long long k1) {
     const Dims& g = h->g;
-    drop_rbox(h);
-    if (i1 <= i0 || j1 <= j0 || k1 <= k0) return;
+    if (i1 <= i0 || j1 <= j0 || k1 <= k0) {
+        drop_rbox(h);
+        return;
+    }
+    // a rejected box leaves the current one in place
     if (h->cfg.storage == TDLB_STORAGE_FP32) throw Fail{TDLB_EINVAL, "a residual box needs 16-bit storage (FP32 storage is exact)"};
     if (h->own_stream) throw Fail{TDLB_ESTATE, "a tank of a batch has no residual box"};
     if (h->vec != 1) throw Fail{TDLB_ESTATE, "a residual box needs one cell per thread (tdlb_set_cells_per_thread(h, 1))"};
@@ -788,6 +858,7 @@ void set_rbox(tdlb_lattice* h, long long i0, long long i1, long long j0, long lo
     // lattice (index 0) then never lies in the box
     if (i0 < 1 || j0 < 1 || k0 < 1 || i1 > g.nx || j1 > g.ny || k1 > g.nz)
         throw Fail{TDLB_EINVAL, "the residual box must lie within [1, x) x [1, y) x [1, z)"};
+    drop_rbox(h);
     tdlb::ResidualBox b;
     b.i0 = (int)i0; b.j0 = (int)j0; b.k0 = (int)k0;
     b.bx = (int)(i1 - i0); b.by = (int)(j1 - j0); b.bz = (int)(k1 - k0);
@@ -803,6 +874,7 @@ void set_rbox(tdlb_lattice* h, long long i0, long long i1, long long j0, long lo
         TDLB_CK(cudaMemsetAsync(h->d_res[q], 0, bytes, h->stream));
     }
     h->rbox_geom = b;
+    h->box_gen++;
 }
 
 // Residuals back to zero, after anything wrote the 16-bit planes without

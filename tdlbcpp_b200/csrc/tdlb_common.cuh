@@ -153,14 +153,23 @@ struct ResidualBox {
     __device__ __forceinline__ bool contains(int i, int j, int k) const {
         return (unsigned)(i - i0) < (unsigned)bx && (unsigned)(j - j0) < (unsigned)by && (unsigned)(k - k0) < (unsigned)bz;
     }
-    // the 3x3x3 neighbourhood of (i, j, k) meets the box
-    __device__ __forceinline__ bool near(int i, int j, int k) const {
-        return res && (unsigned)(i - i0 + 1) < (unsigned)(bx + 2) && (unsigned)(j - j0 + 1) < (unsigned)(by + 2) &&
+    // the 3x3x3 neighbourhood of (i, j, k) meets the box (geometry only) ...
+    __host__ __device__ __forceinline__ bool around(int i, int j, int k) const {
+        return (unsigned)(i - i0 + 1) < (unsigned)(bx + 2) && (unsigned)(j - j0 + 1) < (unsigned)(by + 2) &&
                (unsigned)(k - k0 + 1) < (unsigned)(bz + 2);
     }
+    // ... of a set box
+    __host__ __device__ __forceinline__ bool near(int i, int j, int k) const { return res && around(i, j, k); }
     __device__ __forceinline__ float* at(int s, int i, int j, int k) const {
         return res + (long long)s * n + ((long long)(i - i0) * by + (j - j0)) * bz + (k - k0);
     }
+};
+
+// Scratch outputs of an Esotwist box launch: 19 arrays (the 18 slots' values
+// and Nu) of n entries, one entry per thread of the launch.
+struct BoxOut {
+    float* v = nullptr;
+    long long n = 0;
 };
 
 // Collision constants (FlowParams fields the step reads).

@@ -48,8 +48,8 @@ struct tdlb_lattice {
     int* d_cell_order = nullptr;  // the big planes' cells first (NULL without big planes)
     int ncell_big = 0;
     int* d_plane_cell = nullptr;
-    float* d_prep = nullptr;      // PF_COUNT * n0
-    float* d_cell_m = nullptr;    // 4 * C0
+    float* d_prep = nullptr;      // PF_STRIDE * n0
+    float* d_cell_m = nullptr;    // 4 * C0 (float4 per cell)
     float* d_cell_F = nullptr;    // 3 * C0
     float* d_tail = nullptr;      // TF_COUNT * tail_cap
     long long tail_cap = 0;
@@ -60,7 +60,7 @@ struct tdlb_lattice {
     unsigned marker_gen = 0;      // bumped by every marker upload
     int n_small = 0, n_big = 0, big_tile_cells = 0;
     cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_tail = nullptr;
     uint32_t* d_mask_static = nullptr;   // first segment's touched cells
     uint32_t* d_exclude = nullptr;       // excluded output points (1 bit per cell), when set
     std::vector<uint32_t> h_exclude;
@@ -114,6 +114,16 @@ struct tdlb_lattice {
     tdlb::ResidualBox rbox_geom{};        // geometry only (res unused)
     float* d_res[2] = {nullptr, nullptr};
     bool rbox_auto = true;                // set from the impeller by tdlb_attach_rushton
+    unsigned box_gen = 0;                 // bumped by every change of the box
+    // chunks with a cell near the box (the box launch of a step), ascending,
+    // and the Esotwist box launch's scratch outputs (NQ + 1 floats per
+    // thread of that launch)
+    int* d_box_list = nullptr;
+    int n_box = 0;
+    long long box_list_cap = 0;
+    float* d_box_out = nullptr;
+    long long box_out_cap = 0;            // floats
+    unsigned box_list_gen = ~0u;          // box_gen the list was built for
     // step-kernel timing (tdlb_set_kernel_timing): start/stop event pairs
     bool timing = false;
     std::vector<cudaEvent_t> tev;

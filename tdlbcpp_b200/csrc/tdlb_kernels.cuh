@@ -30,15 +30,20 @@ struct StepArgs {
     int vec;                // cells per thread: 1, 2 or 4 (float, float2, float4 traffic)
     int storage;            // StorageKind of the population planes
     int part;               // 0: every cell; 1: outer chunks; 2: inner chunks (vec == 1, populations)
-    StepPart zone;          // the chunks of part 1 or 2
+    StepPart zone;          // the chunks of part 1 or 2 (box == 2: the chunks near the residual box)
     ResidualBox rr;         // 16-bit storage, one cell per thread: residuals of the locations read ...
     ResidualBox rw;         // ... and written (Simple: of buffer A and B; Esotwist: the same box)
+    int box;                // 0: no residual box; 2: the box launch over `zone` (the chunks near the box, part 2)
+    BoxOut bout;            // box launch: its scratch outputs
 };
 
 cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_esotwist(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_simple_h16(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_esotwist_h16(const StepArgs& a, cudaStream_t st);
+// After the plain launch of a step with a residual box: the box launch's
+// outputs (a.bout) to the cells of a.zone (k_box_commit).
+cudaError_t launch_box_commit(const StepArgs& a, bool simple, cudaStream_t st);
 cudaError_t launch_fill_uniform_moments(Planes Q, const Dims& g, float rho, cudaStream_t st);
 cudaError_t launch_state_moments(Planes A, Planes M, const Dims& g, int mode, int even, cudaStream_t st, int storage,
                                  const CollideParams& p, const ResidualBox& rb = ResidualBox{});
@@ -69,7 +74,7 @@ enum PrepField {
     PF_W = 0,
     PF_CELL = 9,            // int32 bit patterns
     PF_U = 18, PF_V = 19, PF_WV = 20,
-    PF_COUNT = 21
+    PF_STRIDE = 24          // floats per marker: marker-major rows of 96 bytes (six float4 loads)
 };
 
 struct IbmArgs {
@@ -86,8 +91,8 @@ struct IbmArgs {
     int ncell;                  // C0
     const int* cell_order;      // [C0] the big planes' cells, then the others (NULL: no big plane)
     int ncell_big;              // cells of the big planes
-    const float* prep;          // PF_COUNT * n0 (slot-major fields)
-    float* cell_m;              // 4 * C0: rho, jx, jy, jz of each cell this pass
+    const float* prep;          // PF_STRIDE * n0: one row per first-segment slot
+    float* cell_m;              // C0 float4: rho, jx, jy, jz of each cell this pass
     float* cell_F;              // 3 * C0: F of each cell at the start of this pass
     float* tail;                // TF_COUNT * ntail_cap
     long long tail_cap;
@@ -97,7 +102,7 @@ struct IbmArgs {
     int n_small, n_big;         // planes in each launch
     int big_tile_cells;         // F tile capacity of the big-plane launch
     cudaStream_t side;          // stream of the big-plane launch
-    cudaEvent_t ev_fork, ev_join;
+    cudaEvent_t ev_fork, ev_join, ev_tail;
     Planes A;                   // current state
     int state_mode;             // 0 Simple pops, 1 moments, 2 Esotwist pops, 3 Esotwist moments
     int even;                   // Esotwist parity of the state's read map
@@ -140,7 +145,9 @@ size_t ibm_smem_bytes(const Dims& g, int cells);
 // Opt the spread kernels in to the dynamic shared memory of the ordinary
 // planes' launch (tiles of `small_cells` cells) and of the big planes'
 // launch (`big_bytes`).
-cudaError_t ibm_prepare_smem(int small_cells, size_t big_bytes);
+cudaError_t ibm_prepare_smem(int small_cells, int n_small, size_t big_bytes);
+// Shared memory of the big planes' launch for a tile of `big_cells` cells.
+size_t big_bulk_bytes(int big_cells);
 // FP64 force and torque of markers [begin, n) (by list index) of the last
 // forcing pass: out[0..2] = -beta * sum of spread sums, out[3] = torque about
 // the tank axis (ci, ck), out[4] = number of markers summed. `partial` holds

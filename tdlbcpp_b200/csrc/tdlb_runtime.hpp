@@ -148,7 +148,7 @@ struct MarkerSchedule {
 struct CellList {
     std::vector<int> cell_e;       // element index (row*kp + k) of each cell
     std::vector<int> plane_cell;   // [ny+1] cell range of each plane
-    std::vector<int> mcell;        // [9][n0]: plane-local cell index of stencil cell c of slot p
+    std::vector<int> mcell;        // [n0][9]: plane-local cell index of stencil cell c of slot p
     int max_plane_cells = 0;
 
     void build(const Marker* m, const MarkerSchedule& seg0, int nx, int ny, int nz, int kp) {
@@ -182,7 +182,7 @@ struct CellList {
             for (int p = p0; p < p1; p++) {
                 int st[9];
                 MarkerSchedule::stencil(m[seg0.order[(size_t)p]], nx, nz, st);
-                for (int c = 0; c < 9; c++) mcell[(size_t)c * n0 + p] = slot[(size_t)st[c]];
+                for (int c = 0; c < 9; c++) mcell[(size_t)p * 9 + c] = slot[(size_t)st[c]];
             }
             for (int cc : cells) slot[(size_t)cc] = -1;
             plane_cell[(size_t)j + 1] = (int)cell_e.size();

@@ -212,8 +212,10 @@ def test_residual_box_api(gpu):
     assert k0 <= blades["k"].min() - 3 and k1 >= blades["k"].max() + 4
     with pytest.raises(tb.TdlbError):
         cu.set_cells_per_thread(2)
+    box = cu.residual_box()
     with pytest.raises(tb.TdlbError):
         cu.set_residual_box(0, 10, 1, 10, 1, 10)          # index 0 may not lie in the box
+    assert cu.residual_box() == box                       # a rejected box leaves the current one
     cu.set_residual_box(0, 0, 0, 0, 0, 0)
     assert cu.residual_box() == (0, 0, 0, 0, 0, 0)
     cu.set_cells_per_thread(2)

@@ -24,6 +24,8 @@ def run(tb, edge, streaming, storage, overlap, steps, host_blades=False, check_z
                         streaming=tb.STREAMING_SIMPLE if streaming == "Simple" else tb.STREAMING_ESOTWIST)
     cu.set_overlap("always" if overlap else False)
     cu.attach_rushton(rt, d, d, d)
+    if storage != "fp32":
+        cu.set_residual_box(0, 0, 0, 0, 0, 0)   # a step with a residual box never splits
     cu.initialise(1.0)
     cu.forcing_resident(ALPHA, BETA)
     angle = d
