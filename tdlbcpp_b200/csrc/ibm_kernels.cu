@@ -306,17 +306,19 @@ __device__ __forceinline__ void prefetch_l2(const void* base, int c0, int n) {
 // The per-marker and per-cell data a group's walk of plane j reads, into L2
 // while the group fills its tile: the first segment's weights, cells and
 // velocities (markers [pm0, pm1) of the prep arrays), the plane's cell
-// moments, and the blade markers' gathered stencils. One array per lane.
+// moments and elements, and the blade markers' gathered stencils. One array
+// per lane.
 template <typename GRP>
 __device__ __forceinline__ void prefetch_plane(const IbmArgs& a, int j, int c0, int nc, const GRP grp) {
     const int lane = grp.tid();
     if (lane >= 32) return;
     const int pm0 = a.level_ptr[a.plane_lv0[j]], pm1 = a.level_ptr[a.plane_lv0[j + 1]];
     const int q0 = a.level_ptr[a.plane_lv1[j]] - a.n0, q1 = a.level_ptr[a.plane_lv1[j + 1]] - a.n0;
-    for (int f = lane; f < 2 + TF_COUNT; f += 32) {
+    for (int f = lane; f < 3 + TF_COUNT; f += 32) {
         if (f == 0) prefetch_l2(a.prep, pm0 * PF_STRIDE, (pm1 - pm0) * PF_STRIDE);
         else if (f == 1) prefetch_l2(a.cell_m, 4 * c0, 4 * nc);
-        else prefetch_l2(a.tail + (size_t)(f - 2) * a.tail_cap, q0, q1 - q0);
+        else if (f == 2) prefetch_l2(a.cell_e, c0, nc);
+        else prefetch_l2(a.tail + (size_t)(f - 3) * a.tail_cap, q0, q1 - q0);
     }
 }
 
@@ -432,33 +434,64 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
 
     for (int h = grp.tid(); h < H; h += THREADS) keys[h] = -1;
     grp.sync();
-    for (int r = grp.tid(); r < nref; r += THREADS) {
-        const int m = r / 9, c = r - 9 * m;
-        const int key = __float_as_int(s[(TF_CELL + c) * cap + (q0 + m - a.n0)]);
-        unsigned h = ((unsigned)key * 2654435761u) >> (32 - lg);
-        for (int probe = 0; probe < H; probe++) {
-            const int prev = atomicCAS(&keys[h], -1, key);
-            if (prev == -1 || prev == key) break;
-            h = (h + 1) & (unsigned)(H - 1);
+    // inserts, four references per thread at a time (their keys loaded
+    // together)
+    for (int r0 = grp.tid(); r0 < nref; r0 += 4 * THREADS) {
+        int kk[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int r = r0 + u * THREADS;
+            const int m = r / 9, c = r - 9 * m;
+            kk[u] = r < nref ? __float_as_int(s[(TF_CELL + c) * cap + (q0 + m - a.n0)]) : -1;
         }
-        ref[r] = (int)h;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int r = r0 + u * THREADS;
+            if (r >= nref) break;
+            const int key = kk[u];
+            unsigned h = ((unsigned)key * 2654435761u) >> (32 - lg);
+            for (int probe = 0; probe < H; probe++) {
+                const int prev = atomicCAS(&keys[h], -1, key);
+                if (prev == -1 || prev == key) break;
+                h = (h + 1) & (unsigned)(H - 1);
+            }
+            ref[r] = (int)h;
+        }
     }
     grp.sync();
-    for (int h = grp.tid(); h < H; h += THREADS) {
-        const int key = keys[h];
-        if (key < 0) continue;
-        const int i2 = key >> 16, k2 = key & 0xffff;
-        const long long row = (long long)i2 * g.ny + j;
-        const long long e = row * g.kp + k2;
-        const long long wd = row * g.kw + (k2 >> 5);
-        const uint32_t bit = 1u << (k2 & 31);
-        // F is read whatever the flags say (e is a lattice cell), so that the
-        // flag and F loads make one round trip
-        const float vx = __ldcg(a.Fx + e), vy = __ldcg(a.Fy + e), vz = __ldcg(a.Fz + e);
-        const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
-        hx[h] = live ? vx : 0.f;
-        hy[h] = live ? vy : 0.f;
-        hz[h] = live ? vz : 0.f;
+    // each table cell's F, four entries per thread at a time: F is read
+    // whatever the flags say (e is a lattice cell), so that the flag and F
+    // loads of the four make one round trip
+    for (int h0 = grp.tid(); h0 < H; h0 += 4 * THREADS) {
+        float vx[4], vy[4], vz[4];
+        bool live[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int h = h0 + u * THREADS;
+            const int key = h < H ? keys[h] : -1;
+            const int i2 = key >> 16, k2 = key & 0xffff;
+            const long long row = (long long)i2 * g.ny + j;
+            const long long e = row * g.kp + k2;
+            const long long wd = row * g.kw + (k2 >> 5);
+            const uint32_t bit = 1u << (k2 & 31);
+            live[u] = false;
+            vx[u] = vy[u] = vz[u] = 0.f;
+            if (key >= 0) {
+                vx[u] = __ldcg(a.Fx + e);
+                vy[u] = __ldcg(a.Fy + e);
+                vz[u] = __ldcg(a.Fz + e);
+                live[u] = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int h = h0 + u * THREADS;
+            if (h < H && keys[h] >= 0) {
+                hx[h] = live[u] ? vx[u] : 0.f;
+                hy[h] = live[u] ? vy[u] : 0.f;
+                hz[h] = live[u] ? vz[u] : 0.f;
+            }
+        }
     }
     grp.sync();
     for (int lv = lv0; lv < lv1; lv++) {
@@ -532,7 +565,7 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
 // z), filled by bulk copies of the plane's cell range (bar: the group's
 // mbarrier).
 // Otherwise the tile is [3][tile_cells] and filled by plain loads.
-template <int THREADS, bool BULK = false, typename GRP = PlaneGroup<THREADS>>
+template <int THREADS, bool BULK = false, typename GRP = PlaneGroup<THREADS>, bool PIPE = false>
 __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int tile_cells, float* tile, const GRP grp,
                                                  uint64_t* bar = nullptr, int* bulk_fail = nullptr) {
     const int c0 = a.plane_cell[j], nc = a.plane_cell[j + 1] - c0;
@@ -591,35 +624,50 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
     //      only on a narrower lattice).
     const bool distinct = a.g.nx >= 3 && a.g.nz >= 3;
     const float4* cm = reinterpret_cast<const float4*>(a.cell_m) + c0;   // rho, jx, jy, jz
-    for (int lv = a.plane_lv0[j]; lv < a.plane_lv0[j + 1]; lv++) {
+    // PIPE: each thread's next slot row (the next slot of this level, else
+    // its first slot of the next level) is loaded while the current slot is
+    // processed, so a level's rounds wait for the cell moments only (it takes
+    // 24 more registers: launches of at most 384 threads).
+    const int lvb = a.plane_lv0[j], lve = a.plane_lv0[j + 1];
+    float4 r[PF_STRIDE / 4];
+    int rp = -1;   // the slot r holds
+    for (int lv = lvb; lv < lve; lv++) {
         const int p0 = a.level_ptr[lv], p1 = a.level_ptr[lv + 1];
+        const int p2 = lv + 1 < lve ? a.level_ptr[lv + 2] : p1;
 #pragma unroll 1
         for (int p = p0 + grp.tid(); p < p1; p += THREADS) {
             float rhoSum = 0.f, xSum = 0.f, ySum = 0.f, zSum = 0.f;
             float w[9], ox[9], oy[9], oz[9];
             int li[9];
-            // the slot's prep row: six float4 loads
-            float4 r[PF_STRIDE / 4];
-            const float4* row = reinterpret_cast<const float4*>(a.prep + (size_t)p * PF_STRIDE);
+            if (rp != p) {
 #pragma unroll
-            for (int u = 0; u < PF_STRIDE / 4; u++) r[u] = row[u];
+                for (int u = 0; u < PF_STRIDE / 4; u++) r[u] = reinterpret_cast<const float4*>(a.prep + (size_t)p * PF_STRIDE)[u];
+            }
+            int pn = p + THREADS, pe = p1;
+            if (pn >= p1) {
+                pn = p1 + grp.tid();
+                pe = p2;
+            }
+            float4 rn[PF_STRIDE / 4];
+            if (PIPE && pn < pe) {
+#pragma unroll
+                for (int u = 0; u < PF_STRIDE / 4; u++) rn[u] = reinterpret_cast<const float4*>(a.prep + (size_t)pn * PF_STRIDE)[u];
+            }
 #pragma unroll
             for (int c = 0; c < 9; c++) {
                 w[c] = f4_lane(r, PF_W + c);
                 li[c] = __float_as_int(f4_lane(r, PF_CELL + c));
             }
-            float4 m[9];
-#pragma unroll
-            for (int c = 0; c < 9; c++) m[c] = cm[li[c]];
 #pragma unroll
             for (int c = 0; c < 9; c++) {
+                const float4 m = cm[li[c]];
                 ox[c] = fx[li[c]];
                 oy[c] = fy[li[c]];
                 oz[c] = fz[li[c]];
-                rhoSum = fmaf(w[c], m[c].x, rhoSum);
-                xSum = fmaf(w[c], fmaf(0.5f, ox[c], m[c].y), xSum);
-                ySum = fmaf(w[c], fmaf(0.5f, oy[c], m[c].z), ySum);
-                zSum = fmaf(w[c], fmaf(0.5f, oz[c], m[c].w), zSum);
+                rhoSum = fmaf(w[c], m.x, rhoSum);
+                xSum = fmaf(w[c], fmaf(0.5f, ox[c], m.y), xSum);
+                ySum = fmaf(w[c], fmaf(0.5f, oy[c], m.z), ySum);
+                zSum = fmaf(w[c], fmaf(0.5f, oz[c], m.w), zSum);
             }
             xSum = fmaf(-rhoSum, f4_lane(r, PF_U), xSum);
             ySum = fmaf(-rhoSum, f4_lane(r, PF_V), ySum);
@@ -646,19 +694,24 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
                     fz[li[c]] = fmaf(a.alpha, fz[li[c]], -bw * zSum);
                 }
             }
+            if constexpr (PIPE) {
+#pragma unroll
+                for (int u = 0; u < PF_STRIDE / 4; u++) r[u] = rn[u];
+                rp = pn < pe ? pn : -1;
+            }
         }
         grp.sync();
     }
-    // ---- write the plane's cells back to F (four element loads in flight
+    // ---- write the plane's cells back to F (eight element loads in flight
     //      per thread)
     {
         int t = grp.tid();
-        for (; t + 3 * THREADS < nc; t += 4 * THREADS) {
-            int e[4];
+        for (; t + 7 * THREADS < nc; t += 8 * THREADS) {
+            int e[8];
 #pragma unroll
-            for (int u = 0; u < 4; u++) e[u] = a.cell_e[c0 + t + u * THREADS];
+            for (int u = 0; u < 8; u++) e[u] = a.cell_e[c0 + t + u * THREADS];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < 8; u++) {
                 a.Fx[e[u]] = fx[t + u * THREADS];
                 a.Fy[e[u]] = fy[t + u * THREADS];
                 a.Fz[e[u]] = fz[t + u * THREADS];
@@ -694,7 +747,8 @@ __global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_bulk(IbmArgs a, const 
     const int q = (int)blockIdx.x * G + g;
     if (q >= nplanes) return;
     const PlaneGroup<NT, (G > 1)> grp{g * NT, g + 1};
-    ibm_spread_plane<NT, true>(a, planes[q], tile_cells, btile + (size_t)g * 3 * bulk_tile_stride(tile_cells), grp, &bars[g],
+    ibm_spread_plane<NT, true, PlaneGroup<NT, (G > 1)>, (NT * G <= 384)>(
+        a, planes[q], tile_cells, btile + (size_t)g * 3 * bulk_tile_stride(tile_cells), grp, &bars[g],
                                &fails[g]);
 }
 
@@ -1067,7 +1121,8 @@ __global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_batch_bulk(const IbmAr
     for (int i = grp.tid(); i < words; i += NT)
         reinterpret_cast<unsigned long long*>(&sa[g])[i] = reinterpret_cast<const unsigned long long*>(args + w.x)[i];
     grp.sync();
-    ibm_spread_plane<NT, true>(sa[g], w.y, sa[g].smem_cells, btile + (size_t)g * 3 * bulk_tile_stride(region_cells), grp, &bars[g],
+    ibm_spread_plane<NT, true, PlaneGroup<NT, (G > 1)>, (NT * G <= 384)>(
+        sa[g], w.y, sa[g].smem_cells, btile + (size_t)g * 3 * bulk_tile_stride(region_cells), grp, &bars[g],
                                &fails[g]);
 }
 
