@@ -250,10 +250,11 @@ int tdlb_checkpoint_write(tdlb_handle h, const char* dir, const char* unit_name,
 int tdlb_checkpoint_read(tdlb_handle h, const char* dir, const char* unit_name);
 
 /* Step-kernel variant: cells per thread (1, 2 or 4 -- float2 / float4
- * traffic; default 1, the fastest on B200 for both schemes). FP32 storage:
- * all variants compute identical results; 16-bit storage: 2 and 4 cells per
- * thread use packed FP32x2 arithmetic (results within FP32 rounding). Not
- * while a residual box is set (TDLB_ESTATE). */
+ * traffic; default 1, the fastest on B200 for both schemes in FP32). FP32
+ * storage: all variants compute identical results; 16-bit storage: 2 and 4
+ * cells per thread use packed FP32x2 arithmetic (results within FP32
+ * rounding). A residual box works with every variant (its own launches run
+ * one cell per thread). */
 int tdlb_set_cells_per_thread(tdlb_handle h, int v);
 
 /* Residual box of the 16-bit storage forms (no counterpart in the
@@ -269,10 +270,10 @@ int tdlb_set_cells_per_thread(tdlb_handle h, int v);
  * committed after it) and never splits (tdlb_set_overlap).
  * tdlb_attach_rushton sets it over the blades' swept volume with a 4-cell
  * margin, unless a box was set (or removed) with this call; an empty box
- * (i1 <= i0) removes it. Requires 16-bit storage (TDLB_EINVAL), one cell per
- * thread and a lattice outside a batch (TDLB_ESTATE; a lattice joining a
- * batch loses its box), and i0, j0, k0 >= 1. Read-back (moments, velocity),
- * the forcing pass and the FP64 sums include the residuals. */
+ * (i1 <= i0) removes it. Requires 16-bit storage (TDLB_EINVAL), a lattice
+ * outside a batch (TDLB_ESTATE; a lattice joining a batch loses its box),
+ * and i0, j0, k0 >= 1. Read-back (moments, velocity), the forcing pass and
+ * the FP64 sums include the residuals. */
 int tdlb_set_residual_box(tdlb_handle h, int64_t i0, int64_t i1, int64_t j0, int64_t j1, int64_t k0, int64_t k1);
 /* The current box as {i0, i1, j0, j1, k0, k1} (all zero: none). */
 int tdlb_get_residual_box(tdlb_handle h, int64_t* box6);

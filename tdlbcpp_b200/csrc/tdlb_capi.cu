@@ -853,7 +853,6 @@ void set_rbox(tdlb_lattice* h, long long i0, long long i1, long long j0, long lo
     // a rejected box leaves the current one in place
     if (h->cfg.storage == TDLB_STORAGE_FP32) throw Fail{TDLB_EINVAL, "a residual box needs 16-bit storage (FP32 storage is exact)"};
     if (h->own_stream) throw Fail{TDLB_ESTATE, "a tank of a batch has no residual box"};
-    if (h->vec != 1) throw Fail{TDLB_ESTATE, "a residual box needs one cell per thread (tdlb_set_cells_per_thread(h, 1))"};
     // no box cell at index 0: an Esotwist location that wraps around the
     // lattice (index 0) then never lies in the box
     if (i0 < 1 || j0 < 1 || k0 < 1 || i1 > g.nx || j1 > g.ny || k1 > g.nz)
@@ -891,7 +890,7 @@ void clear_rbox(tdlb_lattice* h) {
 // this volume alone brings FP16 from 2.2e-3 to about 6e-4 after 2000 steps
 // of a 120^3 tank at Re 20000).
 void auto_rbox(tdlb_lattice* h, const tdlb::RushtonGeom& G, const std::vector<tdlb::RotatingPolar>& pol, double rmax) {
-    if (h->cfg.storage == TDLB_STORAGE_FP32 || !h->rbox_auto || h->own_stream || h->vec != 1 || pol.empty()) return;
+    if (h->cfg.storage == TDLB_STORAGE_FP32 || !h->rbox_auto || h->own_stream || pol.empty()) return;
     long long jmin = pol[0].j, jmax = pol[0].j;
     for (const tdlb::RotatingPolar& p : pol) {
         jmin = std::min(jmin, p.j);
@@ -1144,8 +1143,6 @@ int tdlb_get_even_step(tdlb_handle h, int* even) {
 int tdlb_set_cells_per_thread(tdlb_handle h, int v) {
     return guarded(h, [&] {
         if (v != 1 && v != 2 && v != 4) throw Fail{TDLB_EINVAL, "cells per thread must be 1, 2 or 4"};
-        if (v != 1 && h->rbox_geom.n)
-            throw Fail{TDLB_ESTATE, "the residual box needs one cell per thread (remove it with tdlb_set_residual_box)"};
         h->vec = v;
     });
 }

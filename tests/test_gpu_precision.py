@@ -85,11 +85,12 @@ def test_fp64_reduction_matches_field_sums(gpu, storage):
 @pytest.mark.parametrize("streaming", ["Simple", "Esotwist"])
 @pytest.mark.parametrize("storage", ["fp16", "bf16"])
 def test_16bit_cells_per_thread_variants_agree(gpu, streaming, storage):
-    """One, two and four cells per thread with 16-bit storage: two and four
-    cells per thread compute in packed FP32x2 arithmetic, which rounds some
-    intermediate results differently from the scalar form by FP32 ulps; the
-    fields after 8 steps agree within 1e-4 relative L2 (a 16-bit storage
-    rounding of 2^-11 or 2^-8 flipped in a few populations)."""
+    """One, two and four cells per thread with 16-bit storage, each with the
+    impeller's residual box (whose own launches run one cell per thread): two
+    and four cells per thread compute in packed FP32x2 arithmetic, which
+    rounds some intermediate results differently from the scalar form by
+    FP32 ulps; the fields after 8 steps agree within 1e-4 relative L2 (a
+    16-bit storage rounding of 2^-11 or 2^-8 flipped in a few populations)."""
     tb = gpu
     out = []
     for vec in (1, 2, 4):
@@ -100,7 +101,7 @@ def test_16bit_cells_per_thread_variants_agree(gpu, streaming, storage):
                             streaming=tb.STREAMING_SIMPLE if streaming == "Simple" else tb.STREAMING_ESOTWIST)
         cu.set_cells_per_thread(vec)
         cu.attach_rushton(rt, d, 0.0, d)
-        cu.set_residual_box(0, 0, 0, 0, 0, 0)      # one cell per thread would get one; the others cannot
+        assert cu.residual_box() != (0, 0, 0, 0, 0, 0)
         cu.initialise(1.0)
         cu.forcing_resident(ALPHA, BETA)
         angle = 0.0
@@ -195,9 +196,8 @@ def test_storage_forms_vs_fp64_oracle(gpu, port_oracle, storage):
 
 def test_residual_box_api(gpu):
     """tdlb_attach_rushton gives a 16-bit lattice a residual box over the
-    blades' swept volume; FP32 storage has none; the box excludes other
-    cells-per-thread variants until it is removed; a lattice joining a batch
-    loses it."""
+    blades' swept volume; FP32 storage has none; the box stays with every
+    cells-per-thread variant; a lattice joining a batch loses it."""
     tb = gpu
     e = 48
     rt = tb.RushtonTurbine(e, e, e, tip_speed=0.1)
@@ -210,9 +210,9 @@ def test_residual_box_api(gpu):
     assert j0 <= blades["j"].min() - 4 and j1 >= blades["j"].max() + 5
     assert i0 <= blades["i"].min() - 3 and i1 >= blades["i"].max() + 4
     assert k0 <= blades["k"].min() - 3 and k1 >= blades["k"].max() + 4
-    with pytest.raises(tb.TdlbError):
-        cu.set_cells_per_thread(2)
     box = cu.residual_box()
+    cu.set_cells_per_thread(2)
+    assert cu.residual_box() == box
     with pytest.raises(tb.TdlbError):
         cu.set_residual_box(0, 10, 1, 10, 1, 10)          # index 0 may not lie in the box
     assert cu.residual_box() == box                       # a rejected box leaves the current one
