@@ -250,7 +250,9 @@ int tdlb_checkpoint_write(tdlb_handle h, const char* dir, const char* unit_name,
 int tdlb_checkpoint_read(tdlb_handle h, const char* dir, const char* unit_name);
 
 /* Step-kernel variant: cells per thread (1, 2 or 4 -- float2 / float4
- * traffic; default 1, the fastest on B200 for both schemes in FP32). FP32
+ * traffic). Default: 4 for 16-bit storage with Simple streaming, else 1 (the
+ * fastest on B200 at 400^3 for each). Split steps (tdlb_set_overlap) need
+ * one cell per thread. FP32
  * storage: all variants compute identical results; 16-bit storage: 2 and 4
  * cells per thread use packed FP32x2 arithmetic (results within FP32
  * rounding). A residual box works with every variant (its own launches run

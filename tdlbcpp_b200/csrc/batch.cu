@@ -42,9 +42,7 @@ namespace tdlb {
 struct TankStep {
     Planes A, B;                 // Simple: source / destination; Esotwist: A
     float* Nu;
-    const float* Fx;
-    const float* Fy;
-    const float* Fz;
+    const float4* F;
     const uint32_t* mask;
     Dims g;
     CollideParams p;
@@ -70,10 +68,10 @@ __device__ __forceinline__ void stage(TankStep& dst, const TankStep* src) {
 template <typename S, int V, bool ESO, bool LES, bool FM>
 __device__ __forceinline__ void tank_quad(const TankStep& ts, unsigned t) {
     if constexpr (!ESO) {
-        simple_quad<S, V, LES, FM, true>(ts.A, ts.B, ts.Nu, ts.Fx, ts.Fy, ts.Fz, ts.mask, ts.g, ts.p, t);
+        simple_quad<S, V, LES, FM, true>(ts.A, ts.B, ts.Nu, ts.F, ts.mask, ts.g, ts.p, t);
     } else {
-        if (ts.even) esotwist_quad<S, V, LES, FM, true, true>(ts.A, ts.Nu, ts.Fx, ts.Fy, ts.Fz, ts.mask, ts.g, ts.p, t);
-        else esotwist_quad<S, V, LES, FM, true, false>(ts.A, ts.Nu, ts.Fx, ts.Fy, ts.Fz, ts.mask, ts.g, ts.p, t);
+        if (ts.even) esotwist_quad<S, V, LES, FM, true, true>(ts.A, ts.Nu, ts.F, ts.mask, ts.g, ts.p, t);
+        else esotwist_quad<S, V, LES, FM, true, false>(ts.A, ts.Nu, ts.F, ts.mask, ts.g, ts.p, t);
     }
 }
 
@@ -356,9 +354,7 @@ TankStep view_of(tdlb_lattice* h) {
     s.A = a.A;
     s.B = a.B;
     s.Nu = a.Nu;
-    s.Fx = a.Fx;
-    s.Fy = a.Fy;
-    s.Fz = a.Fz;
+    s.F = a.F;
     s.mask = a.mask;
     s.g = a.g;
     s.p = a.p;
@@ -613,7 +609,7 @@ tdlb_lattice* detach_tank(tdlb_batch_s* b, int t) {
     TDLB_BCK(quiesce(b));
     tdlb_lattice* h = b->tanks[(size_t)t];
     tdlb_rt::return_stream(h);
-    h->vec = 1;
+    h->vec = tdlb_rt::default_cells_per_thread(h->cfg);
     b->tanks.erase(b->tanks.begin() + t);
     b->ibm_gen.erase(b->ibm_gen.begin() + t);
     b->members_changed = true;

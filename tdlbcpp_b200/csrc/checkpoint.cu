@@ -72,8 +72,7 @@ __global__ void __launch_bounds__(256) k_ckpt_q_out(Planes A, Dims g, int mode, 
     }
 }
 
-__global__ void __launch_bounds__(256) k_ckpt_f_out(const float* __restrict__ Fx, const float* __restrict__ Fy,
-                                                    const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+__global__ void __launch_bounds__(256) k_ckpt_f_out(const float4* __restrict__ F, const uint32_t* __restrict__ mask,
                                                     const float* __restrict__ Nu, Dims g, float* __restrict__ f3,
                                                     float* __restrict__ nu) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -85,9 +84,10 @@ __global__ void __launch_bounds__(256) k_ckpt_f_out(const float* __restrict__ Fx
     const long long e = row * g.kp + k;
     const long long o = ghost_index(g, i, j, k);
     const bool on = (mask[row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
-    f3[3 * o] = on ? Fx[e] : 0.f;
-    f3[3 * o + 1] = on ? Fy[e] : 0.f;
-    f3[3 * o + 2] = on ? Fz[e] : 0.f;
+    const float4 v = F[e];
+    f3[3 * o] = on ? v.x : 0.f;
+    f3[3 * o + 1] = on ? v.y : 0.f;
+    f3[3 * o + 2] = on ? v.z : 0.f;
     nu[o] = Nu[e];
 }
 
@@ -111,8 +111,8 @@ __global__ void __launch_bounds__(256) k_ckpt_q_in(const float* __restrict__ in,
 // where its F is non-zero (an untouched cell's F is zero, and a touched one
 // whose F is exactly zero acts the same either way).
 __global__ void __launch_bounds__(256) k_ckpt_f_in(const float* __restrict__ f3, const float* __restrict__ nu, Dims g,
-                                                   float* __restrict__ Fx, float* __restrict__ Fy, float* __restrict__ Fz,
-                                                   float* __restrict__ Nu, uint32_t* __restrict__ mask) {
+                                                   float4* __restrict__ F, float* __restrict__ Nu,
+                                                   uint32_t* __restrict__ mask) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.rows() * g.kw) return;
     const long long row = t / g.kw;
@@ -125,12 +125,13 @@ __global__ void __launch_bounds__(256) k_ckpt_f_in(const float* __restrict__ f3,
         if (k >= g.kp) break;
         const long long e = row * g.kp + k;
         if (k >= g.nz) {
-            Fx[e] = 0.f; Fy[e] = 0.f; Fz[e] = 0.f; Nu[e] = 0.f;
+            F[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+            Nu[e] = 0.f;
             continue;
         }
         const long long o = ghost_index(g, i, j, k);
         const float x = f3[3 * o], y = f3[3 * o + 1], z = f3[3 * o + 2];
-        Fx[e] = x; Fy[e] = y; Fz[e] = z;
+        F[e] = make_float4(x, y, z, 0.f);
         Nu[e] = nu[o];
         if (x != 0.f || y != 0.f || z != 0.f) bits |= 1u << b;
     }
@@ -379,7 +380,7 @@ int tdlb_checkpoint_write(tdlb_handle h, const char* dir, const char* unit_name,
         write_device(grid_file(sdir, id, unit, "Q"), sc.dev, (size_t)ng * tdlb::NQ * sizeof(float), h->stream, sc.pin);
         // F and Nu share the scratch: F at [0, 3 ng), Nu at [3 ng, 4 ng)
         TDLB_CCK(cudaMemsetAsync(sc.dev, 0, (size_t)ng * 4 * sizeof(float), h->stream));
-        tdlb::k_ckpt_f_out<<<blocks(cells), 256, 0, h->stream>>>(h->F, h->F + g.plane, h->F + 2 * g.plane, h->mask_cur(),
+        tdlb::k_ckpt_f_out<<<blocks(cells), 256, 0, h->stream>>>(reinterpret_cast<const float4*>(h->F), h->mask_cur(),
                                                                  h->Nu, g, sc.dev, sc.dev + 3 * ng);
         TDLB_CCK(cudaGetLastError());
         write_device(grid_file(sdir, id, unit, "F"), sc.dev, (size_t)ng * 3 * sizeof(float), h->stream, sc.pin);
@@ -447,8 +448,8 @@ int tdlb_checkpoint_read(tdlb_handle h, const char* dir, const char* unit_name) 
         read_device(grid_file(sdir, id, unit, "F"), sc.dev, (size_t)ng * 3 * sizeof(float), h->stream, sc.pin);
         read_device(grid_file(sdir, id, unit, "Nu"), sc.dev + 3 * ng, (size_t)ng * sizeof(float), h->stream, sc.pin);
         TDLB_CCK(cudaMemsetAsync(h->mask, 0, (size_t)2 * h->mask_words * sizeof(uint32_t), h->stream));
-        tdlb::k_ckpt_f_in<<<blocks(g.rows() * g.kw), 256, 0, h->stream>>>(sc.dev, sc.dev + 3 * ng, g, h->F, h->F + g.plane,
-                                                                          h->F + 2 * g.plane, h->Nu, h->mask);
+        tdlb::k_ckpt_f_in<<<blocks(g.rows() * g.kw), 256, 0, h->stream>>>(sc.dev, sc.dev + 3 * ng, g,
+                                                                          reinterpret_cast<float4*>(h->F), h->Nu, h->mask);
         TDLB_CCK(cudaGetLastError());
         TDLB_CCK(cudaStreamSynchronize(h->stream));
         h->cfg = c;

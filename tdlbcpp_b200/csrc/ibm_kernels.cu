@@ -169,16 +169,25 @@ __device__ __forceinline__ void ibm_cell(const IbmArgs& a, int c) {
     const long long C = a.ncell;
     reinterpret_cast<float4*>(a.cell_m)[c] = make_float4(m4[0], m4[1], m4[2], m4[3]);
     const bool live = (a.mask_old[(long long)row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
-    a.cell_F[c] = live ? a.Fx[e] : 0.f;
-    a.cell_F[C + c] = live ? a.Fy[e] : 0.f;
-    a.cell_F[2 * C + c] = live ? a.Fz[e] : 0.f;
+    const float4 f = live ? a.F4[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+    a.cell_F[c] = f.x;
+    a.cell_F[C + c] = f.y;
+    a.cell_F[2 * C + c] = f.z;
 }
 
 // Cells [first, first + count) of a.cell_order (of the cell list itself
 // when there is no order).
+// copy_mask: the launch also starts mask_new as the first segment's touched
+// flags (mask_static, a multiple of 16 bytes), so that the pass needs no
+// separate copy.
 template <typename S>
-__global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a, int first, int count) {
+__global__ void __launch_bounds__(256) k_ibm_cells(IbmArgs a, int first, int count, int copy_mask) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (copy_mask) {
+        const long long n4 = (long long)(a.mask_bytes / 16);
+        for (long long w = t; w < n4; w += (long long)gridDim.x * blockDim.x)
+            reinterpret_cast<uint4*>(a.mask_new)[w] = reinterpret_cast<const uint4*>(a.mask_static)[w];
+    }
     if (t >= count) return;
     ibm_cell<S>(a, a.cell_order ? a.cell_order[first + t] : first + t);
 }
@@ -365,9 +374,8 @@ __device__ __noinline__ void blade_levels_global(const IbmArgs& a, int j, const 
                 const long long wd = row * g.kw + (k2 >> 5);
                 const uint32_t bit = 1u << (k2 & 31);
                 const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
-                const float vx = live ? __ldcg(a.Fx + e) : 0.f;
-                const float vy = live ? __ldcg(a.Fy + e) : 0.f;
-                const float vz = live ? __ldcg(a.Fz + e) : 0.f;
+                const float4 v = live ? __ldcg(a.F4 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float vx = v.x, vy = v.y, vz = v.z;
                 rhoSum = fmaf(w, s[(TF_RHO + c) * cap + t], rhoSum);
                 xSum = fmaf(w, fmaf(0.5f, vx, s[(TF_MX + c) * cap + t]), xSum);
                 ySum = fmaf(w, fmaf(0.5f, vy, s[(TF_MY + c) * cap + t]), ySum);
@@ -388,13 +396,10 @@ __device__ __noinline__ void blade_levels_global(const IbmArgs& a, int j, const 
                 const long long wd = row * g.kw + (k2 >> 5);
                 const uint32_t bit = 1u << (k2 & 31);
                 const bool live = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
-                const float vx = live ? __ldcg(a.Fx + e) : 0.f;
-                const float vy = live ? __ldcg(a.Fy + e) : 0.f;
-                const float vz = live ? __ldcg(a.Fz + e) : 0.f;
+                const float4 v = live ? __ldcg(a.F4 + e) : make_float4(0.f, 0.f, 0.f, 0.f);
                 const float bw = a.beta * s[(TF_W + c) * cap + t];
-                a.Fx[e] = fmaf(a.alpha, vx, -bw * xSum);
-                a.Fy[e] = fmaf(a.alpha, vy, -bw * ySum);
-                a.Fz[e] = fmaf(a.alpha, vz, -bw * zSum);
+                a.F4[e] = make_float4(fmaf(a.alpha, v.x, -bw * xSum), fmaf(a.alpha, v.y, -bw * ySum),
+                                      fmaf(a.alpha, v.z, -bw * zSum), 0.f);
                 atomicOr(&a.mask_new[wd], bit);
             }
         }
@@ -477,9 +482,10 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
             live[u] = false;
             vx[u] = vy[u] = vz[u] = 0.f;
             if (key >= 0) {
-                vx[u] = __ldcg(a.Fx + e);
-                vy[u] = __ldcg(a.Fy + e);
-                vz[u] = __ldcg(a.Fz + e);
+                const float4 v = __ldcg(a.F4 + e);
+                vx[u] = v.x;
+                vy[u] = v.y;
+                vz[u] = v.z;
                 live[u] = (__ldcg(a.mask_new + wd) & bit) || (a.mask_old[wd] & bit);
             }
         }
@@ -547,9 +553,7 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
         const int i2 = key >> 16, k2 = key & 0xffff;
         const long long row = (long long)i2 * g.ny + j;
         const long long e = row * g.kp + k2;
-        a.Fx[e] = hx[h];
-        a.Fy[e] = hy[h];
-        a.Fz[e] = hz[h];
+        a.F4[e] = make_float4(hx[h], hy[h], hz[h], 0.f);
         atomicOr(&a.mask_new[row * g.kw + (k2 >> 5)], 1u << (k2 & 31));
     }
     return true;
@@ -565,7 +569,7 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
 // z), filled by bulk copies of the plane's cell range (bar: the group's
 // mbarrier).
 // Otherwise the tile is [3][tile_cells] and filled by plain loads.
-template <int THREADS, bool BULK = false, typename GRP = PlaneGroup<THREADS>, bool PIPE = false>
+template <int THREADS, bool BULK = false, typename GRP = PlaneGroup<THREADS>, bool PIPE = false, bool BLADES = true>
 __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int tile_cells, float* tile, const GRP grp,
                                                  uint64_t* bar = nullptr, int* bulk_fail = nullptr) {
     const int c0 = a.plane_cell[j], nc = a.plane_cell[j + 1] - c0;
@@ -711,23 +715,18 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
 #pragma unroll
             for (int u = 0; u < 8; u++) e[u] = a.cell_e[c0 + t + u * THREADS];
 #pragma unroll
-            for (int u = 0; u < 8; u++) {
-                a.Fx[e[u]] = fx[t + u * THREADS];
-                a.Fy[e[u]] = fy[t + u * THREADS];
-                a.Fz[e[u]] = fz[t + u * THREADS];
-            }
+            for (int u = 0; u < 8; u++)
+                a.F4[e[u]] = make_float4(fx[t + u * THREADS], fy[t + u * THREADS], fz[t + u * THREADS], 0.f);
         }
         for (; t < nc; t += THREADS) {
             const int e = a.cell_e[c0 + t];
-            a.Fx[e] = fx[t];
-            a.Fy[e] = fy[t];
-            a.Fz[e] = fz[t];
+            a.F4[e] = make_float4(fx[t], fy[t], fz[t], 0.f);
         }
     }
     grp.sync();
 
-    // ---- second segment (blades)
-    if (a.plane_lv1[j] == a.plane_lv1[j + 1]) return;
+    // ---- second segment (blades), unless a separate launch walks them
+    if (!BLADES || a.plane_lv1[j] == a.plane_lv1[j + 1]) return;
     const int words = BULK ? 3 * bulk_tile_stride(tile_cells) : 3 * tile_cells;
     if (!blade_levels_tile<THREADS>(a, j, tile, words, grp)) blade_levels_global<THREADS>(a, j, grp);
 }
@@ -737,7 +736,7 @@ __device__ __forceinline__ void ibm_spread_plane(const IbmArgs& a, int j, int ti
 // latency whatever the group's size. The ordinary planes run G = 1..4 groups
 // of 128 threads, so all planes of a large lattice are resident at once; the
 // big planes (an impeller disk) one group of 512.
-template <int NT, int G>
+template <int NT, int G, bool BLADES = true>
 __global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_bulk(IbmArgs a, const int* __restrict__ planes, int nplanes,
                                                               int tile_cells) {
     extern __shared__ __align__(128) float btile[];             // [G][3][bulk_tile_stride(tile_cells)]
@@ -747,9 +746,24 @@ __global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_bulk(IbmArgs a, const 
     const int q = (int)blockIdx.x * G + g;
     if (q >= nplanes) return;
     const PlaneGroup<NT, (G > 1)> grp{g * NT, g + 1};
-    ibm_spread_plane<NT, true, PlaneGroup<NT, (G > 1)>, (NT * G <= 384)>(
+    ibm_spread_plane<NT, true, PlaneGroup<NT, (G > 1)>, (NT * G <= 384), BLADES>(
         a, planes[q], tile_cells, btile + (size_t)g * 3 * bulk_tile_stride(tile_cells), grp, &bars[g],
                                &fails[g]);
+}
+
+// The blade levels of the planes that have blades, one plane per CTA of NT
+// threads, after both first-segment spreads have written their planes' F:
+// the blade planes' walks then run wide instead of holding up the
+// 128-thread groups of the ordinary planes' launch. `words` floats of
+// shared memory hold the plane's hash table.
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) k_ibm_blades(IbmArgs a, const int* __restrict__ planes, int nplanes,
+                                                      int words) {
+    extern __shared__ __align__(16) float btab[];
+    if ((int)blockIdx.x >= nplanes) return;
+    const int j = planes[blockIdx.x];
+    const PlaneGroup<NT> grp{0, 0};
+    if (!blade_levels_tile<NT>(a, j, btab, words, grp)) blade_levels_global<NT>(a, j, grp);
 }
 
 // Impeller rotation on the device: recomputes the blade markers of the
@@ -859,9 +873,10 @@ __global__ void __launch_bounds__(256) k_reduce_fp64(IbmArgs a, const uint32_t* 
         const long long e = row * g.kp + k;
         const bool on = (mask[row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
         acc[0] += m4[0];
-        acc[1] += (double)m4[1] + (on ? 0.5 * (double)a.Fx[e] : 0.0);
-        acc[2] += (double)m4[2] + (on ? 0.5 * (double)a.Fy[e] : 0.0);
-        acc[3] += (double)m4[3] + (on ? 0.5 * (double)a.Fz[e] : 0.0);
+        const float4 f = on ? a.F4[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+        acc[1] += (double)m4[1] + (on ? 0.5 * (double)f.x : 0.0);
+        acc[2] += (double)m4[2] + (on ? 0.5 * (double)f.y : 0.0);
+        acc[3] += (double)m4[3] + (on ? 0.5 * (double)f.z : 0.0);
     }
     for (int c = 0; c < 4; c++) red[c][threadIdx.x] = acc[c];
     __syncthreads();
@@ -952,13 +967,27 @@ int spread_groups(int tile_cells, int nplanes) {
 }
 
 template <int G>
-static const void* spread_bulk_fn() { return (const void*)k_ibm_spread_bulk<128, G>; }
+static const void* spread_bulk_fn() { return (const void*)k_ibm_spread_bulk<128, G, false>; }
 
 template <int G>
 static void spread_small(const IbmArgs& a, cudaStream_t st) {
     const unsigned grid = (unsigned)((a.n_small + G - 1) / G);
     const size_t bytes = (size_t)G * 12 * bulk_tile_stride(a.smem_cells);
-    k_ibm_spread_bulk<128, G><<<grid, 128 * G, bytes, st>>>(a, a.plane_list, a.n_small, a.smem_cells);
+    k_ibm_spread_bulk<128, G, false><<<grid, 128 * G, bytes, st>>>(a, a.plane_list, a.n_small, a.smem_cells);
+}
+
+// Shared memory (floats) of the blade launch for a plane of nb blade
+// markers: blade_levels_tile's table of H >= 9 nb entries (a power of two,
+// at least 32) of four words, and 9 nb references.
+int blade_table_words(int nb) {
+    const int nref = 9 * nb;
+    int H = 32;
+    while (H < nref) H *= 2;
+    return 4 * H + nref;
+}
+
+cudaError_t ibm_prepare_blades(int words) {
+    return raise_smem_limit((const void*)k_ibm_blades<512>, (size_t)words * sizeof(float));
 }
 
 // Shared memory of the big planes' launch (one 512-thread group, a bulk
@@ -971,7 +1000,7 @@ cudaError_t ibm_prepare_smem(int small_cells, int n_small, size_t big_bytes) {
                                                                                        : spread_bulk_fn<1>();
     cudaError_t e = raise_smem_limit(fn, (size_t)G * 12 * bulk_tile_stride(small_cells));
     if (e != cudaSuccess) return e;
-    return raise_smem_limit((const void*)k_ibm_spread_bulk<512, 1>, big_bytes);
+    return raise_smem_limit((const void*)k_ibm_spread_bulk<512, 1, false>, big_bytes);
 }
 
 cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, cudaStream_t st) {
@@ -982,21 +1011,25 @@ cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, 
 }
 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
-    auto cells = [&](int first, int count) {
+    bool mask_copied = false;
+    auto cells = [&](int first, int count, bool copy_mask) {
         if (count <= 0) return;
-        with_storage(a.storage,
-                     [&](auto s) { k_ibm_cells<decltype(s)><<<(count + 255) / 256, 256, 0, st>>>(a, first, count); });
+        with_storage(a.storage, [&](auto s) {
+            k_ibm_cells<decltype(s)><<<(count + 255) / 256, 256, 0, st>>>(a, first, count, copy_mask ? 1 : 0);
+        });
+        mask_copied |= copy_mask;
     };
     auto tail = [&](cudaStream_t ts) {
         if (a.n <= a.n0) return;
         const unsigned b = (unsigned)((9LL * (a.n - a.n0) + 127) / 128);
         with_storage(a.storage, [&](auto s) { k_ibm_gather_tail<decltype(s)><<<b, 128, 0, ts>>>(a); });
     };
-    // mask_new starts as the first segment's (static) touched cells
-    cudaError_t err = cudaMemcpyAsync(a.mask_new, a.mask_static, a.mask_bytes, cudaMemcpyDeviceToDevice, st);
-    if (err != cudaSuccess) return err;
+    // mask_new starts as the first segment's (static) touched cells: copied
+    // by the (largest) cells launch, else by a copy; only the blade walk
+    // reads or sets mask_new, after both
+    cudaError_t err = cudaSuccess;
     if (a.n_big == 0) {
-        cells(0, a.ncell);
+        cells(0, a.ncell, true);
         tail(st);
     } else {
         // Planes with many cells (an impeller disk) run on a side stream with
@@ -1008,7 +1041,7 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
         // the state) runs on the side stream too, beside the other planes'
         // cells; both spreads wait for it.
         const bool split = a.cell_order != nullptr;
-        cells(0, split ? a.ncell_big : a.ncell);
+        cells(0, split ? a.ncell_big : a.ncell, !split);
         err = cudaEventRecord(a.ev_fork, st);
         if (err != cudaSuccess) return err;
         err = cudaStreamWaitEvent(a.side, a.ev_fork, 0);
@@ -1016,14 +1049,18 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
         tail(a.side);
         err = cudaEventRecord(a.ev_tail, a.side);
         if (err != cudaSuccess) return err;
-        k_ibm_spread_bulk<512, 1><<<a.n_big, 512, big_bulk_bytes(a.big_tile_cells), a.side>>>(
+        k_ibm_spread_bulk<512, 1, false><<<a.n_big, 512, big_bulk_bytes(a.big_tile_cells), a.side>>>(
             a, a.plane_list + a.n_small, a.n_big, a.big_tile_cells);
         err = cudaGetLastError();
         if (err != cudaSuccess) return err;
         err = cudaEventRecord(a.ev_join, a.side);
         if (err != cudaSuccess) return err;
-        if (split) cells(a.ncell_big, a.ncell - a.ncell_big);
+        if (split) cells(a.ncell_big, a.ncell - a.ncell_big, true);
         err = cudaStreamWaitEvent(st, a.ev_tail, 0);
+        if (err != cudaSuccess) return err;
+    }
+    if (!mask_copied) {
+        err = cudaMemcpyAsync(a.mask_new, a.mask_static, a.mask_bytes, cudaMemcpyDeviceToDevice, st);
         if (err != cudaSuccess) return err;
     }
     if (a.n_small > 0) {
@@ -1036,8 +1073,17 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
     }
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
-    if (a.n_big > 0) return cudaStreamWaitEvent(st, a.ev_join, 0);
-    return cudaSuccess;
+    if (a.n_big > 0) {
+        err = cudaStreamWaitEvent(st, a.ev_join, 0);
+        if (err != cudaSuccess) return err;
+    }
+    // the blade levels, once every plane's first segment is in F
+    if (a.n_blade > 0) {
+        k_ibm_blades<512><<<a.n_blade, 512, (size_t)a.blade_words * sizeof(float), st>>>(a, a.blade_planes, a.n_blade,
+                                                                                      a.blade_words);
+        err = cudaGetLastError();
+    }
+    return err;
 }
 
 // ---------------------------------------------------------------------------

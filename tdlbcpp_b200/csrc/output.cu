@@ -95,8 +95,7 @@ __global__ void __launch_bounds__(256) k_vorticity(Planes A, Dims g, int mode, i
 // slot is that moment of that cell.
 template <typename S>
 __global__ void __launch_bounds__(256) k_plane_xz(Planes A, Dims g, int mode, int even, CollideParams p, int j,
-                                                  int esotwist, const float* __restrict__ Fx,
-                                                  const float* __restrict__ Fy, const float* __restrict__ Fz,
+                                                  int esotwist, const float4* __restrict__ F,
                                                   const uint32_t* __restrict__ mask, const uint32_t* __restrict__ excl,
                                                   float* __restrict__ out) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -123,9 +122,10 @@ __global__ void __launch_bounds__(256) k_plane_xz(Planes A, Dims g, int mode, in
         }
     }
     const bool on = (mask[row * g.kw + (k >> 5)] >> (k & 31)) & 1u;
-    o[4] = on ? Fx[e] : 0.f;
-    o[5] = on ? Fy[e] : 0.f;
-    o[6] = on ? Fz[e] : 0.f;
+    const float4 v = F[e];
+    o[4] = on ? v.x : 0.f;
+    o[5] = on ? v.y : 0.f;
+    o[6] = on ? v.z : 0.f;
     o[7] = excl && ((excl[row * g.kw + (k >> 5)] >> (k & 31)) & 1u) ? 1.f : 0.f;
 }
 
@@ -243,8 +243,7 @@ int tdlb_plane_xz(tdlb_handle h, int64_t j, tdlb_disk_grid4* q_out, size_t q_cap
         tdlb::with_storage(h->cfg.storage, [&](auto s) {
             tdlb::k_plane_xz<decltype(s)><<<blocks(n), 256, 0, h->stream>>>(A, g, mode, even, h->cp, (int)j,
                                                                            h->cfg.streaming == TDLB_STREAMING_ESOTWIST,
-                                                                           h->F,
-                                                                           h->F + g.plane, h->F + 2 * g.plane,
+                                                                           reinterpret_cast<const float4*>(h->F),
                                                                            h->mask_cur(), h->d_exclude, d.p);
         });
         TDLB_OCK(cudaGetLastError());

@@ -102,19 +102,19 @@ int tdlb_double_resolution(tdlb_handle h) {
         const size_t pop = (size_t)tdlb::NQ * n.plane * sizeof(float);
         size_t free_b = 0, total_b = 0;
         TDLB_RCK(cudaMemGetInfo(&free_b, &total_b));
-        const size_t need = pop * (simple ? 2 : 1) + (size_t)4 * n.plane * sizeof(float) + 2 * words * sizeof(uint32_t);
+        const size_t need = pop * (simple ? 2 : 1) + (size_t)5 * n.plane * sizeof(float) + 2 * words * sizeof(uint32_t);
         if (need > free_b)
             throw RFail{TDLB_ENOMEM, "doubled lattice needs " + std::to_string(need) + " B, " + std::to_string(free_b) +
                                          " B free"};
         TDLB_RCK(cudaMalloc(&A, pop));
         if (simple) TDLB_RCK(cudaMalloc(&B, pop));
         TDLB_RCK(cudaMalloc(&Nu, (size_t)n.plane * sizeof(float)));
-        TDLB_RCK(cudaMalloc(&F, (size_t)3 * n.plane * sizeof(float)));
+        TDLB_RCK(cudaMalloc(&F, (size_t)4 * n.plane * sizeof(float)));   // one float4 per element
         TDLB_RCK(cudaMalloc(&mask, (size_t)2 * words * sizeof(uint32_t)));
         TDLB_RCK(cudaMemsetAsync(A, 0, pop, h->stream));
         if (B) TDLB_RCK(cudaMemsetAsync(B, 0, pop, h->stream));
         TDLB_RCK(cudaMemsetAsync(Nu, 0, (size_t)n.plane * sizeof(float), h->stream));
-        TDLB_RCK(cudaMemsetAsync(F, 0, (size_t)3 * n.plane * sizeof(float), h->stream));
+        TDLB_RCK(cudaMemsetAsync(F, 0, (size_t)4 * n.plane * sizeof(float), h->stream));
         TDLB_RCK(cudaMemsetAsync(mask, 0, (size_t)2 * words * sizeof(uint32_t), h->stream));
         Planes dst;
         for (int d = 0; d < tdlb::NQ; d++) dst.p[d] = A + (size_t)d * n.plane;

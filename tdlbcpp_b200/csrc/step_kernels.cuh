@@ -158,17 +158,20 @@ __device__ __forceinline__ Quad quad_of(const Dims& g, int nq, unsigned t) {
 // touched flags.
 template <int V, bool LES, bool COLLIDE, bool DEV, bool FORCE = true, bool FAST = false>
 __device__ __forceinline__ void collide_quad(float (&f)[NQ][V], const Quad& q, float* __restrict__ Nu,
-                                             const float* __restrict__ Fx, const float* __restrict__ Fy,
-                                             const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+                                             const float4* __restrict__ F, const uint32_t* __restrict__ mask,
                                              const Dims& g, const CollideParams& p, bool from_moments, float (&nu)[V]) {
     if (!COLLIDE) return;
     float fx[V], fy[V], fz[V];
     const uint32_t bits =
         FORCE ? (__ldg(mask + (size_t)q.row * g.kw + (q.k0 >> 5)) >> (q.k0 & 31)) & ((1u << V) - 1u) : 0u;
     if (bits) {
-        vload<V>(Fx + q.e0, fx);
-        vload<V>(Fy + q.e0, fy);
-        vload<V>(Fz + q.e0, fz);
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const float4 v = F[q.e0 + e];
+            fx[e] = v.x;
+            fy[e] = v.y;
+            fz[e] = v.z;
+        }
 #pragma unroll
         for (int e = 0; e < V; e++)
             if (!((bits >> e) & 1u)) fx[e] = fy[e] = fz[e] = 0.f;
@@ -279,8 +282,7 @@ __device__ __forceinline__ void box_read_eso(const ResidualBox& rb, int i, int j
 // ---------------------------------------------------------------------------
 template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool FORCE = true, int BOX = 0>
 __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, float* __restrict__ Nu,
-                                            const float* __restrict__ Fx, const float* __restrict__ Fy,
-                                            const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+                                            const float4* __restrict__ F, const uint32_t* __restrict__ mask,
                                             const Dims& g, const CollideParams& p, unsigned t,
                                             const ResidualBox rr = ResidualBox{}, const BoxOut out = BoxOut{}) {
     static_assert(!(Storage<S>::deviation && FROM_MOMENTS), "16-bit state always holds populations");
@@ -372,7 +374,7 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
     // 16-bit storage: approximate reciprocals and square root (measured on
     // B200 at 400^3: FP16 step 1.28 -> 1.19 ms; the Esotwist kernel, which
     // keeps IEEE rounding, measured slower with them, 1.38 -> 1.47 ms)
-    collide_quad<V, LES, COLLIDE, Storage<S>::deviation, FORCE, Storage<S>::deviation>(f, q, Nu, Fx, Fy, Fz, mask, g,
+    collide_quad<V, LES, COLLIDE, Storage<S>::deviation, FORCE, Storage<S>::deviation>(f, q, Nu, F, mask, g,
                                                                                        p, FROM_MOMENTS, nu);
     if constexpr (BOX == 2) {
         // box launch: the exact outputs and Nu to the scratch array (entry
@@ -404,8 +406,7 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
 // before a neighbour overwrites it.
 // ---------------------------------------------------------------------------
 template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN, bool FORCE = true, int BOX = 0>
-__device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict__ Nu, const float* __restrict__ Fx,
-                                              const float* __restrict__ Fy, const float* __restrict__ Fz,
+__device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict__ Nu, const float4* __restrict__ F,
                                               const uint32_t* __restrict__ mask, const Dims& g, const CollideParams& p,
                                               unsigned t, const ResidualBox rb = ResidualBox{},
                                               const BoxOut out = BoxOut{}) {
@@ -487,7 +488,7 @@ __device__ __forceinline__ void esotwist_quad(const Planes& Q, float* __restrict
     }
     __syncwarp();
     float nu[V];
-    collide_quad<V, LES, COLLIDE, Storage<S>::deviation, FORCE>(f, q, Nu, Fx, Fy, Fz, mask, g, p, FROM_MOMENTS, nu);
+    collide_quad<V, LES, COLLIDE, Storage<S>::deviation, FORCE>(f, q, Nu, F, mask, g, p, FROM_MOMENTS, nu);
     if constexpr (BOX == 2) {
         // box launch: the exact outputs, slot by slot, and Nu to the scratch
         // array (entry blockIdx.x * 128 + threadIdx.x of the chunk list)
@@ -580,15 +581,14 @@ __device__ __forceinline__ bool part_thread(const StepPart& part, unsigned& t) {
 
 template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, int PART = 0, int BOX = 0>
 __global__ void __launch_bounds__(128, 4) k_step_simple(Planes A, Planes B, float* __restrict__ Nu,
-                                                       const float* __restrict__ Fx, const float* __restrict__ Fy,
-                                                       const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+                                                       const float4* __restrict__ F, const uint32_t* __restrict__ mask,
                                                        Dims g, CollideParams p, StepPart part, ResidualBox rr,
                                                        BoxOut out) {
     static_assert(PART == 0 || V == 1, "split steps run one cell per thread");
     static_assert(BOX != 2 || PART != 0, "the box path runs a chunk list");
     unsigned t;
     if (!part_thread<PART>(part, t)) return;   // whole warps
-    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE, PART != 1, BOX>(A, B, Nu, Fx, Fy, Fz, mask, g, p, t, rr, out);
+    simple_quad<S, V, LES, FROM_MOMENTS, COLLIDE, PART != 1, BOX>(A, B, Nu, F, mask, g, p, t, rr, out);
 }
 
 // Resident 128-thread blocks per SM the Esotwist kernel is built for: the
@@ -599,15 +599,14 @@ constexpr int kEsotwistBlocksPerSM = V == 1 ? 8 : (V == 2 ? 6 : 4);
 
 template <typename S, int V, bool LES, bool FROM_MOMENTS, bool COLLIDE, bool EVEN, int PART = 0, int BOX = 0>
 __global__ void __launch_bounds__(128, BOX == 2 ? 4 : kEsotwistBlocksPerSM<V>) k_step_esotwist(Planes Q, float* __restrict__ Nu,
-                                                         const float* __restrict__ Fx, const float* __restrict__ Fy,
-                                                         const float* __restrict__ Fz, const uint32_t* __restrict__ mask,
+                                                         const float4* __restrict__ F, const uint32_t* __restrict__ mask,
                                                          Dims g, CollideParams p, StepPart part, ResidualBox rb,
                                                          BoxOut out) {
     static_assert(PART == 0 || V == 1, "split steps run one cell per thread");
     static_assert(BOX != 2 || PART != 0, "the box path runs a chunk list");
     unsigned t;
     if (!part_thread<PART>(part, t)) return;   // whole warps
-    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN, PART != 1, BOX>(Q, Nu, Fx, Fy, Fz, mask, g, p, t, rb, out);
+    esotwist_quad<S, V, LES, FROM_MOMENTS, COLLIDE, EVEN, PART != 1, BOX>(Q, Nu, F, mask, g, p, t, rb, out);
 }
 
 // After the plain launch of a step with a residual box: every cell of the box

@@ -57,6 +57,7 @@ void release(tdlb_lattice* h) {
     cudaFree(h->d_level_ptr);
     cudaFree(h->d_plane_lv0);
     cudaFree(h->d_plane_lv1);
+    cudaFree(h->d_blade_planes);
     cudaFree(h->d_cell_e);
     cudaFree(h->d_cell_order);
     cudaFree(h->d_plane_cell);
@@ -119,9 +120,7 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
     try {
         h->cfg = c;
         h->device = device;
-        // measured on B200 at 400^3: both schemes are fastest with one cell
-        // per thread (direct loads; Esotwist with 64 registers, 8 blocks/SM)
-        h->vec = 1;
+        h->vec = tdlb_rt::default_cells_per_thread(c);
         h->err.reserve(512);
         TDLB_CK(cudaSetDevice(device));
         TDLB_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -155,18 +154,18 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
         size_t free_b = 0, total_b = 0;
         TDLB_CK(cudaMemGetInfo(&free_b, &total_b));
         const size_t need = pop_bytes * (c.streaming == TDLB_STREAMING_SIMPLE ? 2 : 1) +
-                            (size_t)4 * g.plane * sizeof(float) + 2 * h->mask_words * sizeof(uint32_t);
+                            (size_t)5 * g.plane * sizeof(float) + 2 * h->mask_words * sizeof(uint32_t);   // F (float4), Nu
         if (need > free_b) throw Fail{TDLB_ENOMEM, "lattice needs " + std::to_string(need) + " B, " +
                                                        std::to_string(free_b) + " B free on device"};
         TDLB_CK(cudaMalloc(&h->bufA, pop_bytes));
         if (c.streaming == TDLB_STREAMING_SIMPLE) TDLB_CK(cudaMalloc(&h->bufB, pop_bytes));
         TDLB_CK(cudaMalloc(&h->Nu, (size_t)g.plane * sizeof(float)));
-        TDLB_CK(cudaMalloc(&h->F, (size_t)3 * g.plane * sizeof(float)));
+        TDLB_CK(cudaMalloc(&h->F, (size_t)4 * g.plane * sizeof(float)));
         TDLB_CK(cudaMalloc(&h->mask, (size_t)2 * h->mask_words * sizeof(uint32_t)));
         TDLB_CK(cudaMemsetAsync(h->bufA, 0, pop_bytes, h->stream));
         if (h->bufB) TDLB_CK(cudaMemsetAsync(h->bufB, 0, pop_bytes, h->stream));
         TDLB_CK(cudaMemsetAsync(h->Nu, 0, (size_t)g.plane * sizeof(float), h->stream));
-        TDLB_CK(cudaMemsetAsync(h->F, 0, (size_t)3 * g.plane * sizeof(float), h->stream));
+        TDLB_CK(cudaMemsetAsync(h->F, 0, (size_t)4 * g.plane * sizeof(float), h->stream));
         TDLB_CK(cudaMemsetAsync(h->mask, 0, (size_t)2 * h->mask_words * sizeof(uint32_t), h->stream));
         TDLB_CK(cudaStreamSynchronize(h->stream));
     } catch (...) {
@@ -254,9 +253,7 @@ tdlb::StepArgs step_args(tdlb_lattice* h, bool collide) {
     a.A = h->planes(h->state_buf());
     if (h->cfg.streaming == TDLB_STREAMING_SIMPLE) a.B = h->planes(h->other_buf());
     a.Nu = h->Nu;
-    a.Fx = h->F;
-    a.Fy = h->F + h->g.plane;
-    a.Fz = h->F + 2 * h->g.plane;
+    a.F = reinterpret_cast<const float4*>(h->F);
     a.mask = h->mask_cur();
     a.g = h->g;
     a.p = h->cp;
@@ -504,6 +501,7 @@ void run_step(tdlb_lattice* h, bool collide) {
     tdlb::StepArgs bx = a;
     bx.box = 2;
     bx.part = 2;
+    bx.vec = 1;   // the box launches run one cell per thread, whatever the plain launch's variant
     bx.zone = tdlb::StepPart{h->d_box_list, h->n_box};
     bx.bout = tdlb::BoxOut{h->d_box_out, ((long long)h->n_box * 32 + 127) / 128 * 128};
     const bool run_box = boxed && h->n_box > 0;
@@ -569,8 +567,38 @@ void ensure_level_cap(tdlb_lattice* h, long long need) {
 }
 
 // Device copy of the second segment's schedule (slots n0.., levels L0..).
+// The planes whose second segment (blades) has levels, for the blade launch
+// of the forcing pass, and its shared memory; uploaded when they change.
+void update_blade_planes(tdlb_lattice* h) {
+    const Dims& g = h->g;
+    const auto& lv = h->seg1.plane_lv;
+    const auto& lp = h->seg1.level_ptr;
+    const int L0 = h->seg0.nlevels;
+    std::vector<int> planes;
+    int words = 0;
+    for (int j = 0; j < g.ny; j++) {
+        if (lv[(size_t)j] == lv[(size_t)j + 1]) continue;
+        planes.push_back(j);
+        // the level ranges are global level indices; seg1's level_ptr starts at level L0
+        const int nb = lp[(size_t)(lv[(size_t)j + 1] - L0)] - lp[(size_t)(lv[(size_t)j] - L0)];
+        words = std::max(words, tdlb::blade_table_words(nb));
+    }
+    words = std::min(words, 220 * 1024 / 4);   // a plane beyond this walks its blades on global memory
+    if (planes != h->h_blade_planes) {
+        if (!h->d_blade_planes) TDLB_CK(cudaMalloc(&h->d_blade_planes, (size_t)std::max(g.ny, 1) * sizeof(int)));
+        h->h_blade_planes = planes;
+        if (!planes.empty())
+            TDLB_CK(cudaMemcpyAsync(h->d_blade_planes, h->h_blade_planes.data(), planes.size() * sizeof(int),
+                                    cudaMemcpyHostToDevice, h->stream));
+        h->n_blade = (int)planes.size();
+    }
+    if (words > h->blade_words) TDLB_CK(tdlb::ibm_prepare_blades(words));
+    h->blade_words = std::max(h->blade_words, words);
+}
+
 void upload_seg1(tdlb_lattice* h) {
     const Dims& g = h->g;
+    update_blade_planes(h);
     const int L0 = h->seg0.nlevels;
     ensure_level_cap(h, (long long)L0 + h->seg1.nlevels + 1);
     const int n1 = h->n_markers - h->n0;
@@ -739,6 +767,9 @@ tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     a.plane_list = h->d_plane_list;
     a.n_small = h->n_small;
     a.n_big = h->n_big;
+    a.blade_planes = h->d_blade_planes;
+    a.n_blade = h->n_blade;
+    a.blade_words = h->blade_words;
     a.big_tile_cells = h->big_tile_cells;
     a.side = h->side;
     a.ev_fork = h->ev_fork;
@@ -747,9 +778,7 @@ tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     a.A = h->planes(h->state_buf());
     a.state_mode = h->state_mode();
     a.even = h->even ? 1 : 0;
-    a.Fx = h->F;
-    a.Fy = h->F + h->g.plane;
-    a.Fz = h->F + 2 * h->g.plane;
+    a.F4 = reinterpret_cast<float4*>(h->F);
     a.mask_old = h->mask_cur();
     a.mask_new = h->mask_next();
     a.mask_static = h->d_mask_static;
@@ -775,7 +804,7 @@ void run_forcing(tdlb_lattice* h, float alpha, float beta) {
     if (!h->markers_set) throw Fail{TDLB_ESTATE, "no markers set (tdlb_set_markers / tdlb_forcing)"};
     TDLB_CK(tdlb::launch_ibm(ibm_args(h, alpha, beta), ibm_stream(h)));
     h->launches += (h->cells.cell_e.empty() ? 0 : 1) + (h->n_markers > h->n0 ? 1 : 0) + (h->n_small > 0 ? 1 : 0) +
-                   (h->n_big > 0 ? 1 : 0);
+                   (h->n_big > 0 ? 1 : 0) + (h->n_blade > 0 ? 1 : 0);
     h->pass++;
     h->last_beta = beta;
 }
@@ -793,6 +822,21 @@ void planes_to_host_aos(tdlb_lattice* h, const float* dev, int npl, float* out) 
             for (int k = 0; k < g.nz; k++, c++) {
                 const size_t e = ((size_t)i * g.ny + j) * g.kp + k;
                 for (int l = 0; l < npl; l++) out[c * npl + l] = tmp[(size_t)l * g.plane + e];
+            }
+}
+
+// The force field (one float4 per element) as (Fx, Fy, Fz) per interior cell.
+void force_to_host(tdlb_lattice* h, float* out3) {
+    const Dims& g = h->g;
+    std::vector<float> tmp((size_t)4 * g.plane);
+    TDLB_CK(cudaMemcpyAsync(tmp.data(), h->F, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    TDLB_CK(cudaStreamSynchronize(h->stream));
+    size_t c = 0;
+    for (int i = 0; i < g.nx; i++)
+        for (int j = 0; j < g.ny; j++)
+            for (int k = 0; k < g.nz; k++, c++) {
+                const size_t e = ((size_t)i * g.ny + j) * g.kp + k;
+                for (int l = 0; l < 3; l++) out3[c * 3 + l] = tmp[4 * e + (size_t)l];
             }
 }
 
@@ -968,7 +1012,7 @@ int tdlb_lattice_bytes(const tdlb_config* c, int64_t* bytes) {
     // fields, flags, and the marker buffers of a tank-wall geometry
     // (about 8 markers per (i, j) column at most, 256 bytes each with
     // their schedule, stencil-cell and per-pass data)
-    *bytes = pops + 4 * plane * 4 + 2 * mask_words * 4 + 8 * c->x * c->y * 256;
+    *bytes = pops + 5 * plane * 4 + 2 * mask_words * 4 + 8 * c->x * c->y * 256;   // F (float4) and Nu: 5 planes
     return TDLB_OK;
 }
 
@@ -998,7 +1042,7 @@ int tdlb_initialise(tdlb_handle h, float rho) {
             h->holds_moments = false;
         }
         TDLB_CK(cudaMemsetAsync(h->Nu, 0, (size_t)g.plane * sizeof(float), h->stream));
-        TDLB_CK(cudaMemsetAsync(h->F, 0, (size_t)3 * g.plane * sizeof(float), h->stream));
+        TDLB_CK(cudaMemsetAsync(h->F, 0, (size_t)4 * g.plane * sizeof(float), h->stream));
         TDLB_CK(cudaMemsetAsync(h->mask, 0, (size_t)2 * h->mask_words * sizeof(uint32_t), h->stream));
         clear_rbox(h);
         h->initialised = true;
@@ -1064,7 +1108,7 @@ int tdlb_read_velocity_density(tdlb_handle h, float* rho, float* ux, float* uy, 
         const size_t ncell = (size_t)g.nx * g.ny * g.nz;
         std::vector<float> m(ncell * tdlb::NQ), f(ncell * 3);
         planes_to_host_aos(h, M.p, tdlb::NQ, m.data());
-        planes_to_host_aos(h, h->F, 3, f.data());
+        force_to_host(h, f.data());
         std::vector<uint8_t> t(ncell);
         std::vector<uint32_t> words((size_t)h->mask_words);
         TDLB_CK(cudaMemcpy(words.data(), h->mask_cur(), words.size() * 4, cudaMemcpyDeviceToHost));
@@ -1088,7 +1132,7 @@ int tdlb_read_force(tdlb_handle h, float* f3) {
         require_init(h);
         if (!f3) throw Fail{TDLB_EINVAL, "out is NULL"};
         const Dims& g = h->g;
-        planes_to_host_aos(h, h->F, 3, f3);
+        force_to_host(h, f3);
         std::vector<uint32_t> words((size_t)h->mask_words);
         TDLB_CK(cudaMemcpy(words.data(), h->mask_cur(), words.size() * 4, cudaMemcpyDeviceToHost));
         const size_t ncell = (size_t)g.nx * g.ny * g.nz;
@@ -1314,6 +1358,7 @@ int tdlb_set_rotating_markers(tdlb_handle h, const tdlb_marker* markers, size_t 
         std::copy(markers, markers + n, h->h_markers.begin() + h->n0);
         const auto* mk = reinterpret_cast<const tdlb::Marker*>(h->h_markers.data());
         h->seg1.build(mk, h->n0, h->n_markers, h->g.nx, h->g.ny, h->g.nz, h->n0, h->seg0.nlevels, nullptr);
+        update_blade_planes(h);
         const int L0 = h->seg0.nlevels;
         ensure_level_cap(h, (long long)L0 + h->seg1.nlevels + 1);
         const size_t b_mk = n * sizeof(tdlb::Marker);

@@ -12,8 +12,11 @@
 //     elements (16: every FP32 row starts on a 64-byte boundary);
 //   * 18 population planes (SoA), each `plane` elements long and 256-byte
 //     aligned, addressed through an 18-pointer table;
-//   * F as three SoA planes (Fx, Fy, Fz), Nu as one plane, and the IBM "touched"
-//     flags as one bit per cell: word r*kw + k/32, bit k%32.
+//   * F as one float4 (Fx, Fy, Fz, unused) per element -- the forcing pass
+//     reads and writes it at scattered stencil cells, where one 16-byte
+//     access replaces three 4-byte ones in three planes --, Nu as one plane,
+//     and the IBM "touched" flags as one bit per cell: word r*kw + k/32,
+//     bit k%32.
 #pragma once
 #include <cstdint>
 #include <cuda_bf16.h>

@@ -59,6 +59,10 @@ struct tdlb_lattice {
     std::vector<int> h_plane_list;   // host copy of d_plane_list
     unsigned marker_gen = 0;      // bumped by every marker upload
     int n_small = 0, n_big = 0, big_tile_cells = 0;
+    // the planes with blade levels, walked by their own launch
+    std::vector<int> h_blade_planes;
+    int* d_blade_planes = nullptr;
+    int n_blade = 0, blade_words = 0;
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_tail = nullptr;
     uint32_t* d_mask_static = nullptr;   // first segment's touched cells
@@ -165,6 +169,12 @@ struct tdlb_lattice {
 
 // Runtime helpers shared by the C-ABI translation units (tdlb_capi.cu).
 namespace tdlb_rt {
+// Default cells per thread of a lattice's step kernel. Measured on B200 at
+// 400^3: FP32 storage and Esotwist are fastest with one cell per thread;
+// 16-bit Simple with four (packed FP32x2 arithmetic: 1.15 vs 1.19 ms).
+inline int default_cells_per_thread(const tdlb_config& c) {
+    return c.storage != TDLB_STORAGE_FP32 && c.streaming == TDLB_STREAMING_SIMPLE ? 4 : 1;
+}
 tdlb::StepArgs step_args(tdlb_lattice* h, bool collide);
 tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta);
 // Queue h's work on `s` instead of its own stream (batches share one).

@@ -17,9 +17,7 @@ struct StepArgs {
     Planes A;               // Simple: source buffer; Esotwist: the single buffer
     Planes B;               // Simple: destination buffer (unused for Esotwist)
     float* Nu;
-    const float* Fx;
-    const float* Fy;
-    const float* Fz;
+    const float4* F;        // force, one float4 (Fx, Fy, Fz, unused) per element
     const uint32_t* mask;   // IBM-touched flags of the forcing pass this step uses
     Dims g;
     CollideParams p;
@@ -100,13 +98,15 @@ struct IbmArgs {
     int smem_cells;             // F tile capacity of the small-plane launch
     const int* plane_list;      // [ny] small planes first, then the big ones
     int n_small, n_big;         // planes in each launch
+    const int* blade_planes;    // the planes with blade levels (the blade launch)
+    int n_blade, blade_words;   // their count; shared-memory floats of the blade launch
     int big_tile_cells;         // F tile capacity of the big-plane launch
     cudaStream_t side;          // stream of the big-plane launch
     cudaEvent_t ev_fork, ev_join, ev_tail;
     Planes A;                   // current state
     int state_mode;             // 0 Simple pops, 1 moments, 2 Esotwist pops, 3 Esotwist moments
     int even;                   // Esotwist parity of the state's read map
-    float* Fx; float* Fy; float* Fz;
+    float4* F4;                 // force, one float4 (Fx, Fy, Fz, unused) per element
     const uint32_t* mask_old;   // touched flags of the previous forcing pass
     uint32_t* mask_new;         // touched flags of this pass (fully written)
     const uint32_t* mask_static;   // touched flags of the first segment (every pass)
@@ -148,6 +148,10 @@ size_t ibm_smem_bytes(const Dims& g, int cells);
 cudaError_t ibm_prepare_smem(int small_cells, int n_small, size_t big_bytes);
 // Shared memory of the big planes' launch for a tile of `big_cells` cells.
 size_t big_bulk_bytes(int big_cells);
+// Shared-memory floats of the blade launch for a plane of nb blade markers,
+// and the opt-in to that many.
+int blade_table_words(int nb);
+cudaError_t ibm_prepare_blades(int words);
 // FP64 force and torque of markers [begin, n) (by list index) of the last
 // forcing pass: out[0..2] = -beta * sum of spread sums, out[3] = torque about
 // the tank axis (ci, ck), out[4] = number of markers summed. `partial` holds

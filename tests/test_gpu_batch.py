@@ -51,8 +51,10 @@ def run_alone(tb, spec, streaming, storage, steps):
     cu = tb.ComputeUnit(**cfg)
     prepare(cu, rt)
     if storage != "fp32":
-        # a tank of a batch keeps no 16-bit residual box: compare like with like
+        # a tank of a batch keeps no 16-bit residual box and steps one cell
+        # per thread: compare like with like
         cu.set_residual_box(0, 0, 0, 0, 0, 0)
+        cu.set_cells_per_thread(1)
         prepare(cu, rt)
     angle = rt.increment(1)
     for s in range(2, steps + 2):

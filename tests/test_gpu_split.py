@@ -26,6 +26,7 @@ def run(tb, edge, streaming, storage, overlap, steps, host_blades=False, check_z
     cu.attach_rushton(rt, d, d, d)
     if storage != "fp32":
         cu.set_residual_box(0, 0, 0, 0, 0, 0)   # a step with a residual box never splits
+        cu.set_cells_per_thread(1)              # nor one with several cells per thread
     cu.initialise(1.0)
     cu.forcing_resident(ALPHA, BETA)
     angle = d
