@@ -388,7 +388,9 @@ def reference_root() -> str:
     """The reference checkout the oracle compiles from (oracle/Makefile's
     REF_ROOT: the TDLB_REFERENCE environment variable or its default)."""
     import subprocess
-    r = subprocess.run(["make", "-s", "-C", HERE, "print-ref-root"], capture_output=True, text=True, check=True)
+    env = {k: v for k, v in os.environ.items() if k not in ("MAKEFLAGS", "MAKELEVEL", "MFLAGS")}
+    r = subprocess.run(["make", "-s", "--no-print-directory", "-C", HERE, "print-ref-root"], capture_output=True,
+                       text=True, check=True, env=env)
     return r.stdout.strip()
 
 
