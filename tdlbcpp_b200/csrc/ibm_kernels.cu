@@ -1012,10 +1012,10 @@ cudaError_t launch_ibm_prepare(const IbmArgs& a, float* prep, const int* mcell, 
 
 cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
     bool mask_copied = false;
-    auto cells = [&](int first, int count, bool copy_mask) {
+    auto cells = [&](int first, int count, bool copy_mask, cudaStream_t cs) {
         if (count <= 0) return;
         with_storage(a.storage, [&](auto s) {
-            k_ibm_cells<decltype(s)><<<(count + 255) / 256, 256, 0, st>>>(a, first, count, copy_mask ? 1 : 0);
+            k_ibm_cells<decltype(s)><<<(count + 255) / 256, 256, 0, cs>>>(a, first, count, copy_mask ? 1 : 0);
         });
         mask_copied |= copy_mask;
     };
@@ -1026,39 +1026,31 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
     };
     // mask_new starts as the first segment's (static) touched cells: copied
     // by the (largest) cells launch, else by a copy; only the blade walk
-    // reads or sets mask_new, after both
+    // reads or sets mask_new, at the end of the pass.
+    // Side stream: the blade markers' gather (which reads only the state and
+    // is needed only by the blade walk) and the planes with many cells (an
+    // impeller disk): their cells, then their spread with a full-size tile
+    // and 512 threads, started before the ordinary planes' spread places its
+    // blocks over the SMs. Handle's stream: the other planes' cells and
+    // spread, then, after the side stream, the blade walk.
     cudaError_t err = cudaSuccess;
-    if (a.n_big == 0) {
-        cells(0, a.ncell, true);
-        tail(st);
-    } else {
-        // Planes with many cells (an impeller disk) run on a side stream with
-        // a full-size tile and 512 threads. Their cells are prepared first,
-        // so that their spread starts while the other planes' cells are
-        // prepared: a big-plane block needs a whole SM's shared memory, which
-        // it would not find once the ordinary planes' spread has placed its
-        // blocks over the SMs. The blade markers' gather (which reads only
-        // the state) runs on the side stream too, beside the other planes'
-        // cells; both spreads wait for it.
-        const bool split = a.cell_order != nullptr;
-        cells(0, split ? a.ncell_big : a.ncell, !split);
-        err = cudaEventRecord(a.ev_fork, st);
-        if (err != cudaSuccess) return err;
-        err = cudaStreamWaitEvent(a.side, a.ev_fork, 0);
-        if (err != cudaSuccess) return err;
-        tail(a.side);
-        err = cudaEventRecord(a.ev_tail, a.side);
-        if (err != cudaSuccess) return err;
+    const bool split = a.n_big > 0 && a.cell_order != nullptr;
+    if (!split) cells(0, a.ncell, true, st);   // (before the fork: a big planes' spread reads them)
+    err = cudaEventRecord(a.ev_fork, st);
+    if (err != cudaSuccess) return err;
+    err = cudaStreamWaitEvent(a.side, a.ev_fork, 0);
+    if (err != cudaSuccess) return err;
+    if (split) cells(0, a.ncell_big, false, a.side);
+    tail(a.side);
+    if (a.n_big > 0) {
         k_ibm_spread_bulk<512, 1, false><<<a.n_big, 512, big_bulk_bytes(a.big_tile_cells), a.side>>>(
             a, a.plane_list + a.n_small, a.n_big, a.big_tile_cells);
         err = cudaGetLastError();
         if (err != cudaSuccess) return err;
-        err = cudaEventRecord(a.ev_join, a.side);
-        if (err != cudaSuccess) return err;
-        if (split) cells(a.ncell_big, a.ncell - a.ncell_big, true);
-        err = cudaStreamWaitEvent(st, a.ev_tail, 0);
-        if (err != cudaSuccess) return err;
     }
+    err = cudaEventRecord(a.ev_join, a.side);
+    if (err != cudaSuccess) return err;
+    if (split) cells(a.ncell_big, a.ncell - a.ncell_big, true, st);
     if (!mask_copied) {
         err = cudaMemcpyAsync(a.mask_new, a.mask_static, a.mask_bytes, cudaMemcpyDeviceToDevice, st);
         if (err != cudaSuccess) return err;
@@ -1073,10 +1065,8 @@ cudaError_t launch_ibm(const IbmArgs& a, cudaStream_t st) {
     }
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
-    if (a.n_big > 0) {
-        err = cudaStreamWaitEvent(st, a.ev_join, 0);
-        if (err != cudaSuccess) return err;
-    }
+    err = cudaStreamWaitEvent(st, a.ev_join, 0);
+    if (err != cudaSuccess) return err;
     // the blade levels, once every plane's first segment is in F
     if (a.n_blade > 0) {
         k_ibm_blades<512><<<a.n_blade, 512, (size_t)a.blade_words * sizeof(float), st>>>(a, a.blade_planes, a.n_blade,

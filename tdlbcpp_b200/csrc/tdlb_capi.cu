@@ -77,7 +77,6 @@ void release(tdlb_lattice* h) {
     if (h->ibm) cudaStreamDestroy(h->ibm);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
-    if (h->ev_tail) cudaEventDestroy(h->ev_tail);
     if (h->ev_outer) cudaEventDestroy(h->ev_outer);
     if (h->ev_inner) cudaEventDestroy(h->ev_inner);
     if (h->ev_sync) cudaEventDestroy(h->ev_sync);
@@ -129,14 +128,10 @@ tdlb_lattice* build(const tdlb_config& c, int device) {
         // scheduled ahead of the outer launch's as SMs free up
         int prio_lo = 0, prio_hi = 0;
         TDLB_CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-#ifdef TDLB_EXP_PRIO_LO
-        prio_hi = prio_lo;
-#endif
         TDLB_CK(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, prio_hi));
         TDLB_CK(cudaStreamCreateWithPriority(&h->ibm, cudaStreamNonBlocking, prio_hi));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
-        TDLB_CK(cudaEventCreateWithFlags(&h->ev_tail, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_outer, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_inner, cudaEventDisableTiming));
         TDLB_CK(cudaEventCreateWithFlags(&h->ev_sync, cudaEventDisableTiming));
@@ -774,7 +769,6 @@ tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta) {
     a.side = h->side;
     a.ev_fork = h->ev_fork;
     a.ev_join = h->ev_join;
-    a.ev_tail = h->ev_tail;
     a.A = h->planes(h->state_buf());
     a.state_mode = h->state_mode();
     a.even = h->even ? 1 : 0;

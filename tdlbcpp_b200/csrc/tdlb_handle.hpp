@@ -64,7 +64,7 @@ struct tdlb_lattice {
     int* d_blade_planes = nullptr;
     int n_blade = 0, blade_words = 0;
     cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_tail = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     uint32_t* d_mask_static = nullptr;   // first segment's touched cells
     uint32_t* d_exclude = nullptr;       // excluded output points (1 bit per cell), when set
     std::vector<uint32_t> h_exclude;

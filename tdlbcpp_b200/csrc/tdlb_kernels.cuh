@@ -102,7 +102,7 @@ struct IbmArgs {
     int n_blade, blade_words;   // their count; shared-memory floats of the blade launch
     int big_tile_cells;         // F tile capacity of the big-plane launch
     cudaStream_t side;          // stream of the big-plane launch
-    cudaEvent_t ev_fork, ev_join, ev_tail;
+    cudaEvent_t ev_fork, ev_join;
     Planes A;                   // current state
     int state_mode;             // 0 Simple pops, 1 moments, 2 Esotwist pops, 3 Esotwist moments
     int even;                   // Esotwist parity of the state's read map
