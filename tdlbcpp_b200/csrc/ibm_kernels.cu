@@ -1140,8 +1140,11 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1) k_ibm_spread_
 // bulk copies fill, as k_ibm_spread_bulk does for one lattice. region_cells:
 // the largest tile of the batch's lattices (the group's share of shared
 // memory); each lattice's walk uses its own tile size within it.
+// (One group per CTA: at most 170 registers, so that three such CTAs fit an
+// SM beside the other tank group's fused launch -- 64 tanks: 20,433 -> 21,000
+// MLUPS FP32; 128 registers spill and measured slower.)
 template <int NT, int G>
-__global__ void __launch_bounds__(NT * G, 1) k_ibm_spread_batch_bulk(const IbmArgs* __restrict__ args,
+__global__ void __launch_bounds__(NT * G, G == 1 ? 3 : 1) k_ibm_spread_batch_bulk(const IbmArgs* __restrict__ args,
                                                                     const int2* __restrict__ work, int nwork,
                                                                     int region_cells) {
     extern __shared__ __align__(128) float btile[];             // [G][3][bulk_tile_stride(region_cells)]
