@@ -38,6 +38,18 @@ __device__ __forceinline__ void vstore(float* p, const float (&v)[V]) {
     else if constexpr (V == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
     else *p = v[0];
 }
+// Streaming stores (st.global.cs: first out of L2), for data the kernel does
+// not read again -- Simple's destination buffer and Nu, FP32 storage.
+// Measured on B200 at 400^3: k_step_simple 1.554 -> 1.528-1.535 ms; the
+// in-place Esotwist kernel, which stores to the lines it has just read,
+// measured slower with them (1.676 -> 1.724 ms), and so did the 16-bit Simple
+// step (1.541 -> 1.574 ms whole step); those keep plain stores.
+template <int V>
+__device__ __forceinline__ void vstore_cs(float* p, const float (&v)[V]) {
+    if constexpr (V == 4) __stcs(reinterpret_cast<float4*>(p), make_float4(v[0], v[1], v[2], v[3]));
+    else if constexpr (V == 2) __stcs(reinterpret_cast<float2*>(p), make_float2(v[0], v[1]));
+    else __stcs(p, v[0]);
+}
 
 // Population plane access in storage type S: V elements from element e,
 // decoded to FP32 (RO: read-only, non-coherent path).
@@ -83,10 +95,11 @@ __device__ __forceinline__ float pload1(const float* plane, int e) {
     pload<S, 1, RO>(plane, e, v);
     return v[0];
 }
-template <typename S, int V>
+template <typename S, int V, bool CS = false>
 __device__ __forceinline__ void pstore(float* plane, int e, const float (&v)[V]) {
     if constexpr (sizeof(S) == 4) {
-        vstore<V>(plane + e, v);
+        if constexpr (CS) vstore_cs<V>(plane + e, v);
+        else vstore<V>(plane + e, v);
     } else {
         S* p = reinterpret_cast<S*>(plane) + e;
         if constexpr (V == 4) {
@@ -95,14 +108,23 @@ __device__ __forceinline__ void pstore(float* plane, int e, const float (&v)[V])
             for (int k = 0; k < 4; k++) s4[k] = Storage<S>::enc(v[k]);
             uint2 t;
             memcpy(&t, s4, sizeof t);
-            *reinterpret_cast<uint2*>(p) = t;
+            if constexpr (CS) __stcs(reinterpret_cast<uint2*>(p), t);
+            else *reinterpret_cast<uint2*>(p) = t;
         } else if constexpr (V == 2) {
             S s2[2] = {Storage<S>::enc(v[0]), Storage<S>::enc(v[1])};
             unsigned t;
             memcpy(&t, s2, sizeof t);
-            *reinterpret_cast<unsigned*>(p) = t;
+            if constexpr (CS) __stcs(reinterpret_cast<unsigned*>(p), t);
+            else *reinterpret_cast<unsigned*>(p) = t;
         } else {
-            *p = Storage<S>::enc(v[0]);
+            if constexpr (CS) {
+                const S enc = Storage<S>::enc(v[0]);
+                unsigned short t;
+                memcpy(&t, &enc, sizeof t);
+                __stcs(reinterpret_cast<unsigned short*>(p), t);
+            } else {
+                *p = Storage<S>::enc(v[0]);
+            }
         }
     }
 }
@@ -387,8 +409,12 @@ __device__ __forceinline__ void simple_quad(const Planes& A, const Planes& B, fl
     }
     if (!q.active) return;
 #pragma unroll
-    for (int d = 0; d < NQ; d++) pstore<S, V>(B.p[d], q.e0, f[d]);
-    if (COLLIDE && LES) vstore<V>(Nu + q.e0, nu);
+    for (int d = 0; d < NQ; d++) pstore<S, V, sizeof(S) == 4>(B.p[d], q.e0, f[d]);
+    if constexpr (sizeof(S) == 4) {
+        if (COLLIDE && LES) vstore_cs<V>(Nu + q.e0, nu);
+    } else {
+        if (COLLIDE && LES) vstore<V>(Nu + q.e0, nu);
+    }
 }
 
 // ---------------------------------------------------------------------------
