@@ -22,13 +22,15 @@
 // only where the bit is set, and the next pass treats F as zero where neither
 // the previous pass (mask_old) nor the current one has touched the cell.
 //
-// Per pass (launch_ibm): a copy of the static touched flags into mask_new,
-// k_ibm_cells (moments and starting F of every unique stencil cell of the
-// static markers; the big planes' cells first), k_ibm_gather_tail (weights
-// and stencil moments of every blade marker, which no marker changes), then
-// k_ibm_spread, one CTA per j-plane: the static markers' levels on an F tile
-// in shared memory, then the blade levels on a shared-memory hash table of
-// the plane's blade cells.
+// Per pass (launch_ibm): k_ibm_cells (moments and starting F of every unique
+// stencil cell of the static markers; it also starts mask_new as the static
+// touched flags), k_ibm_gather_tail (weights and stencil moments of every
+// blade marker, which no marker changes), k_ibm_spread_bulk (one plane per
+// group of threads: the static markers' levels on an F tile in shared
+// memory), then k_ibm_blades (the blade levels of the planes that have
+// blades, on a shared-memory hash table of the plane's blade cells). The
+// batched passes run the same steps per lattice, with the blade levels
+// inside their spread.
 #include "tdlb_kernels.cuh"
 #include "tdlb_rotate.hpp"
 
@@ -559,12 +561,12 @@ __device__ __forceinline__ bool blade_levels_tile(const IbmArgs& a, int j, float
     return true;
 }
 
-// One CTA per j-plane: the plane's first-segment levels on an F tile in
+// One group per j-plane: the plane's first-segment levels on an F tile in
 // shared memory (planes with more cells than the tile holds work on cell_F
-// in place), write-back to F, then the blade levels, on a shared-memory
-// table when they fit the tile, else on global F. The touched flags of the
-// first segment never change, so each pass starts mask_new as a copy of them
-// (mask_static) and the blade walk adds its cells.
+// in place), write-back to F, then (BLADES) the blade levels, on a
+// shared-memory table when they fit the tile, else on global F. The touched
+// flags of the first segment never change, so each pass starts mask_new as
+// a copy of them (mask_static) and the blade walk adds its cells.
 // BULK: the group's tile is [3][bulk_tile_stride(tile_cells)] words (F x, y,
 // z), filled by bulk copies of the plane's cell range (bar: the group's
 // mbarrier).
