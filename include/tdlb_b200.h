@@ -250,14 +250,23 @@ int tdlb_checkpoint_write(tdlb_handle h, const char* dir, const char* unit_name,
 int tdlb_checkpoint_read(tdlb_handle h, const char* dir, const char* unit_name);
 
 /* Step-kernel variant: cells per thread (1, 2 or 4 -- float2 / float4
- * traffic). Default: 4 for 16-bit storage with Simple streaming, else 1 (the
- * fastest on B200 at 400^3 for each). Split steps (tdlb_set_overlap) need
+ * traffic). Default: 1 for FP32 storage; for 16-bit storage 4 with Simple
+ * streaming, 2 with Esotwist (the fastest on B200 at 400^3 for each). Split steps (tdlb_set_overlap) need
  * one cell per thread. FP32
  * storage: all variants compute identical results; 16-bit storage: 2 and 4
  * cells per thread use packed FP32x2 arithmetic (results within FP32
  * rounding). A residual box works with every variant (its own launches run
  * one cell per thread). */
 int tdlb_set_cells_per_thread(tdlb_handle h, int v);
+
+/* L2 prefetch of the step kernels (on by default; no counterpart in the
+ * reference). A full step launch walks the lattice in 128-thread tiles of
+ * the flat row-major cell index; every eighth tile's CTA, as it starts,
+ * issues bulk L2 prefetches of the population spans (and Nu) that the tiles
+ * one wave of resident CTAs further on will read, so their loads hit L2.
+ * Results are identical either way (a prefetch moves no data the kernel
+ * sees); the switch is for measurement. on: 0 or 1 (else TDLB_EINVAL). */
+int tdlb_set_l2_prefetch(tdlb_handle h, int on);
 
 /* Residual box of the 16-bit storage forms (no counterpart in the
  * reference, whose storage is FP32). For every population location of the

@@ -217,6 +217,7 @@ def load_library() -> ctypes.CDLL:
         "tdlb_impeller_load_async": (i32, [H, vp]),
         "tdlb_get_stream": (i32, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "tdlb_set_cells_per_thread": (i32, [H, i32]),
+        "tdlb_set_l2_prefetch": (i32, [H, i32]),
         "tdlb_set_residual_box": (i32, [H] + [ctypes.c_int64] * 6),
         "tdlb_get_residual_box": (i32, [H, vp]),
         "tdlb_set_overlap": (i32, [H, i32]),
@@ -463,6 +464,10 @@ class ComputeUnit:
     def set_cells_per_thread(self, v: int):
         """Step-kernel variant (1, 2 or 4 cells per thread)."""
         self._check(self.lib.tdlb_set_cells_per_thread(self.h, v))
+
+    def set_l2_prefetch(self, on: bool):
+        """Step kernels' L2 prefetch one wave ahead (on by default; results identical)."""
+        self._check(self.lib.tdlb_set_l2_prefetch(self.h, 1 if on else 0))
 
     def set_residual_box(self, i0: int, i1: int, j0: int, j1: int, k0: int, k1: int):
         """16-bit storage: keep the locations of the box [i0,i1) x [j0,j1) x [k0,k1)

@@ -58,8 +58,9 @@ template <int V>
 static cudaError_t launch_simple_v(const StepArgs& a, cudaStream_t st) {
     const dim3 grid(step_blocks(a, V)), block(128);
 #define TDLB_SIMPLE(LES, FM, COL, PART)                                                                       \
-    k_step_simple<float, V, LES, FM, COL, PART><<<grid, block, 0, st>>>(a.A, a.B, a.Nu, a.F, a.mask, \
-                                                                      a.g, a.p, a.zone, ResidualBox{}, BoxOut{})
+    k_step_simple<float, V, LES, FM, COL, PART><<<grid, block, 0, st>>>(                                   \
+        a.A, a.B, a.Nu, a.F, a.mask, a.g, a.p,                                                               \
+        launch_walk<k_step_simple<float, V, LES, FM, COL, PART>, COL && !FM>(a), ResidualBox{}, BoxOut{})
     if (!a.collide) TDLB_SIMPLE(false, false, false, 0);
     else if (a.from_moments) { if (a.les) TDLB_SIMPLE(true, true, true, 0); else TDLB_SIMPLE(false, true, true, 0); }
     else if constexpr (V == 1) {
@@ -81,8 +82,14 @@ static cudaError_t launch_simple_v(const StepArgs& a, cudaStream_t st) {
 
 template <int V, bool LES, bool FM, bool COL, int PART>
 static void eso_launch(const StepArgs& a, dim3 grid, cudaStream_t st) {
-    if (a.even) k_step_esotwist<float, V, LES, FM, COL, true, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.F, a.mask, a.g, a.p, a.zone, ResidualBox{}, BoxOut{});
-    else k_step_esotwist<float, V, LES, FM, COL, false, PART><<<grid, 128, 0, st>>>(a.A, a.Nu, a.F, a.mask, a.g, a.p, a.zone, ResidualBox{}, BoxOut{});
+    if (a.even)
+        k_step_esotwist<float, V, LES, FM, COL, true, PART><<<grid, 128, 0, st>>>(
+            a.A, a.Nu, a.F, a.mask, a.g, a.p, launch_walk<k_step_esotwist<float, V, LES, FM, COL, true, PART>, COL && !FM>(a),
+            ResidualBox{}, BoxOut{});
+    else
+        k_step_esotwist<float, V, LES, FM, COL, false, PART><<<grid, 128, 0, st>>>(
+            a.A, a.Nu, a.F, a.mask, a.g, a.p, launch_walk<k_step_esotwist<float, V, LES, FM, COL, false, PART>, COL && !FM>(a),
+            ResidualBox{}, BoxOut{});
 }
 
 template <int V>

@@ -16,8 +16,9 @@ static inline unsigned grid16(const StepArgs& a, int V) {
 // chunk list).
 template <typename S, int V, bool LES, int PART, int BOX>
 static void simple16_part(const StepArgs& a, cudaStream_t st) {
-    k_step_simple<S, V, LES, false, true, PART, BOX><<<grid16(a, V), 128, 0, st>>>(a.A, a.B, a.Nu, a.F,
-                                                                                 a.mask, a.g, a.p, a.zone, a.rr, a.bout);
+    k_step_simple<S, V, LES, false, true, PART, BOX><<<grid16(a, V), 128, 0, st>>>(
+        a.A, a.B, a.Nu, a.F, a.mask, a.g, a.p, launch_walk<k_step_simple<S, V, LES, false, true, PART, BOX>, true>(a),
+        a.rr, a.bout);
 }
 
 template <typename S, int V, bool LES>
@@ -40,8 +41,14 @@ static cudaError_t simple16(const StepArgs& a, cudaStream_t st) {
 template <typename S, int V, bool LES, int PART, int BOX>
 static void eso16_part(const StepArgs& a, cudaStream_t st) {
     const unsigned grid = grid16(a, V);
-    if (a.even) k_step_esotwist<S, V, LES, false, true, true, PART, BOX><<<grid, 128, 0, st>>>(a.A, a.Nu, a.F, a.mask, a.g, a.p, a.zone, a.rr, a.bout);
-    else k_step_esotwist<S, V, LES, false, true, false, PART, BOX><<<grid, 128, 0, st>>>(a.A, a.Nu, a.F, a.mask, a.g, a.p, a.zone, a.rr, a.bout);
+    if (a.even)
+        k_step_esotwist<S, V, LES, false, true, true, PART, BOX><<<grid, 128, 0, st>>>(
+            a.A, a.Nu, a.F, a.mask, a.g, a.p, launch_walk<k_step_esotwist<S, V, LES, false, true, true, PART, BOX>, true>(a),
+            a.rr, a.bout);
+    else
+        k_step_esotwist<S, V, LES, false, true, false, PART, BOX><<<grid, 128, 0, st>>>(
+            a.A, a.Nu, a.F, a.mask, a.g, a.p, launch_walk<k_step_esotwist<S, V, LES, false, true, false, PART, BOX>, true>(a),
+            a.rr, a.bout);
 }
 
 template <typename S, int V, bool LES>

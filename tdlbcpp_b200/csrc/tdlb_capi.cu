@@ -257,6 +257,7 @@ tdlb::StepArgs step_args(tdlb_lattice* h, bool collide) {
     a.collide = collide ? 1 : 0;
     a.even = h->even ? 1 : 0;
     a.vec = h->vec;
+    a.l2_prefetch = h->l2_prefetch;
     a.storage = h->cfg.storage;
     // residual box (16-bit storage): Simple reads the state buffer's
     // residuals and writes the other buffer's; Esotwist updates its one set
@@ -1182,6 +1183,13 @@ int tdlb_set_cells_per_thread(tdlb_handle h, int v) {
     return guarded(h, [&] {
         if (v != 1 && v != 2 && v != 4) throw Fail{TDLB_EINVAL, "cells per thread must be 1, 2 or 4"};
         h->vec = v;
+    });
+}
+
+int tdlb_set_l2_prefetch(tdlb_handle h, int on) {
+    return guarded(h, [&] {
+        if (on != 0 && on != 1) throw Fail{TDLB_EINVAL, "l2 prefetch must be 0 or 1"};
+        h->l2_prefetch = on;
     });
 }
 

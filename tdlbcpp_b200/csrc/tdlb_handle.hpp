@@ -34,6 +34,7 @@ struct tdlb_lattice {
     bool even = true;            // Esotwist parity (ComputeUnit.hpp:116)
     int pass = 0;                // forcing passes so far; mask[pass & 1] is current
     int vec = 4;                 // cells per thread of the step kernels (set per scheme in build())
+    int l2_prefetch = 1;         // full step launches prefetch one wave ahead into L2 (tdlb_set_l2_prefetch)
     bool initialised = false;
 
     // markers: the resident list and its two-segment schedule
@@ -170,10 +171,13 @@ struct tdlb_lattice {
 // Runtime helpers shared by the C-ABI translation units (tdlb_capi.cu).
 namespace tdlb_rt {
 // Default cells per thread of a lattice's step kernel. Measured on B200 at
-// 400^3: FP32 storage and Esotwist are fastest with one cell per thread;
-// 16-bit Simple with four (packed FP32x2 arithmetic: 1.15 vs 1.19 ms).
+// 400^3 with the L2 prefetch on (step kernel alone): FP32 storage is fastest
+// with one cell per thread; 16-bit storage with packed FP32x2 arithmetic,
+// Simple with four (1.08 ms), Esotwist with two (1.35 ms; one: 1.48, four:
+// 1.39).
 inline int default_cells_per_thread(const tdlb_config& c) {
-    return c.storage != TDLB_STORAGE_FP32 && c.streaming == TDLB_STREAMING_SIMPLE ? 4 : 1;
+    if (c.storage == TDLB_STORAGE_FP32) return 1;
+    return c.streaming == TDLB_STREAMING_SIMPLE ? 4 : 2;
 }
 tdlb::StepArgs step_args(tdlb_lattice* h, bool collide);
 tdlb::IbmArgs ibm_args(tdlb_lattice* h, float alpha, float beta);

@@ -1,16 +1,40 @@
 // Internal interface between the host runtime (tdlb_capi.cu) and the kernels.
 #pragma once
+#include <atomic>
 #include "tdlb_common.cuh"
 
 namespace tdlb {
 
 // Chunks of a split step (32 consecutive elements of the flat row*kp + k
-// index, one warp each): the launch takes chunks[0, count).
+// index, one warp each): the launch takes chunks[0, count). A full launch
+// (part 0) takes no list; l2_ahead > 0 turns on its L2 prefetch, that many
+// CTAs ahead of the walk (step_kernels.cuh).
 struct StepPart {
     const int* chunks;
     int count;
+    int l2_ahead;
 };
 constexpr int kSplitChunk = 32;
+
+// One wave of resident 128-thread CTAs of kernel K on the current device (the
+// occupancy its register count allows, times the SMs): the L2 prefetch
+// distance of a full launch. Queried once per kernel; 0 (prefetch off) if the
+// query fails.
+template <auto K>
+int wave_ctas() {
+    static std::atomic<int> n{0};
+    int v = n.load(std::memory_order_relaxed);
+    if (v == 0) {
+        int dev = 0, sms = 0, per = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, K, 128, 0) == cudaSuccess && per > 0 && sms > 0) {
+            v = per * sms;
+            n.store(v, std::memory_order_relaxed);
+        }
+    }
+    return v;
+}
 
 // Arguments of one fused step launch.
 struct StepArgs {
@@ -26,6 +50,7 @@ struct StepArgs {
     int collide;            // 0: transport only (identity collision; known-answer tests)
     int even;               // Esotwist parity (evenStep)
     int vec;                // cells per thread: 1, 2 or 4 (float, float2, float4 traffic)
+    int l2_prefetch;        // full launches of the population form: L2 prefetch one wave ahead
     int storage;            // StorageKind of the population planes
     int part;               // 0: every cell; 1: outer chunks; 2: inner chunks (vec == 1, populations)
     StepPart zone;          // the chunks of part 1 or 2 (box == 2: the chunks near the residual box)
@@ -34,6 +59,16 @@ struct StepArgs {
     int box;                // 0: no residual box; 2: the box launch over `zone` (the chunks near the box, part 2)
     BoxOut bout;            // box launch: its scratch outputs
 };
+
+// The StepPart a launch of kernel K takes: the chunk list (parts 1 and 2) or,
+// for a full launch of the population form (FULL) with a.l2_prefetch on, the
+// L2 prefetch distance of one wave of K's resident CTAs.
+template <auto K, bool FULL>
+StepPart launch_walk(const StepArgs& a) {
+    StepPart w = a.zone;
+    w.l2_ahead = FULL && a.part == 0 && a.l2_prefetch ? wave_ctas<K>() : 0;
+    return w;
+}
 
 cudaError_t launch_step_simple(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_step_esotwist(const StepArgs& a, cudaStream_t st);
