@@ -78,16 +78,46 @@ __device__ __forceinline__ void tank_quad(const TankStep& ts, unsigned t) {
 // Quads of `NT` threads a work item covers: the tank's view is staged in
 // shared memory once per item.
 constexpr int kBatchChunks = 8;
+// Chunks ahead of the one a block starts that it prefetches into L2. Measured
+// on B200 over the 64-tank Esotwist batch (fused launch, ms): FP32 1.381
+// without, 1.267 one chunk ahead, 1.318 two; FP16 1.027, 1.011, 1.016. (A
+// prefetch one wave of resident blocks ahead, as in the plain kernels, spans
+// 8-chunk items and overran L2: 1.52 ms.)
+constexpr int kBatchPrefetchChunks = 1;
+
+// L2 prefetch of the chunk of NT quads from quad q0 of the staged tank: NQ + 1
+// threads issue one bulk prefetch each (plane d's source span of the chunk's
+// elements, shifted as the pull reads them, and Nu's with LES), as the plain
+// kernels do one wave ahead (prefetch_ahead). The from-moments step reads its
+// own cells and takes the same spans.
+template <typename S, int V, int NT, bool ESO>
+__device__ __forceinline__ void prefetch_chunk(const TankStep& ts, unsigned q0) {
+    const int d = (int)threadIdx.x;
+    if (d > NQ || (d == NQ && !ts.les)) return;
+    const Dims& g = ts.g;
+    const long long e0 = (long long)q0 * V, e1 = e0 + (long long)NT * V;
+    if (d == NQ) return prefetch_span(ts.Nu, 4, g.plane, e0, e1);
+    const long long rs = (long long)g.ny * g.kp;
+    long long sh;
+    if (ESO) {
+        const int sg = ts.even ? -1 : 1;
+        sh = (sg * cx_of(d) > 0 ? rs : 0) + (sg * cy_of(d) > 0 ? g.kp : 0);
+    } else {
+        sh = -(cx_of(d) * rs + cy_of(d) * g.kp);
+    }
+    prefetch_span(ts.A.p[d], (int)sizeof(S), g.plane, e0 + sh - 1, e1 + sh + 1);
+}
 
 // Batched step: block b takes work items b, b + grid, ...; an item is
 // kBatchChunks x NT consecutive quads of one tank (fewer at the end of a
-// tank), whose step view is staged in shared memory. 16-bit storage never
-// holds moments, so its from-moments bodies are not built. `counter` (may be
+// tank), whose step view is staged in shared memory; as it starts chunk c of
+// an item, the block prefetches chunk c + ahead into L2 (ahead > 0). 16-bit storage
+// never holds moments, so its from-moments bodies are not built. `counter` (may be
 // NULL) is advanced once: this launch runs after the step's rotation, which
 // reads it.
 template <typename S, int V, int NT, bool ESO>
 __global__ void __launch_bounds__(NT, (ESO ? kEsotwistBlocksPerSM<V> : 4) * 128 / NT) k_batch_step(const TankStep* __restrict__ tanks, const int2* __restrict__ work,
-                                                   int nwork, int* counter) {
+                                                   int nwork, int* counter, int ahead) {
     constexpr bool kFM = sizeof(S) == 4;
     __shared__ TankStep ts;
     if (counter && blockIdx.x == 0 && threadIdx.x == 0) *counter += 1;
@@ -100,6 +130,7 @@ __global__ void __launch_bounds__(NT, (ESO ? kEsotwistBlocksPerSM<V> : 4) * 128 
         for (int c = 0; c < kBatchChunks; c++) {
             const unsigned t0 = (unsigned)wk.y + (unsigned)(c * NT);
             if (t0 >= nquads) break;   // uniform over the block
+            if (ahead > 0 && c + ahead < kBatchChunks) prefetch_chunk<S, V, NT, ESO>(ts, t0 + (unsigned)(ahead * NT));
             const unsigned t = t0 + threadIdx.x;
             if (ts.les) {
                 if (kFM && ts.from_moments) tank_quad<S, V, ESO, true, kFM>(ts, t);
@@ -131,7 +162,7 @@ __global__ void __launch_bounds__(256) k_rotate_batch(const TankRotor* __restric
     o.wDelta = m.wDelta;
 }
 
-using BatchFn = void (*)(const TankStep*, const int2*, int, int*);
+using BatchFn = void (*)(const TankStep*, const int2*, int, int*, int);
 
 template <typename S, bool ESO>
 BatchFn pick(int v, int nt) {
@@ -374,11 +405,13 @@ void advance_step_state(tdlb_lattice* h) {
 // The fused launch over `work`: persistent blocks (bps per SM, each taking
 // items b, b + grid, ...) or, with bps = 0, one block per item, so that the
 // block scheduler fills the SMs the other group's forcing pass leaves free.
+// A block prefetches the chunk kBatchPrefetchChunks chunks after the one it
+// starts, within its item.
 void launch_fused(tdlb_batch_s* b, const TankStep* d_views, const WorkList& work, int* counter, cudaStream_t st) {
     if (work.n == 0) return;
     const tdlb::BatchFn fn = tdlb::batch_kernel(storage_of(b), eso_of(b), b->vec, b->threads);
     const int grid = b->bps > 0 ? std::min(work.n, b->sms * b->bps) : work.n;
-    fn<<<grid, b->threads, 0, st>>>(d_views, work.d, work.n, counter);
+    fn<<<grid, b->threads, 0, st>>>(d_views, work.d, work.n, counter, tdlb::kBatchPrefetchChunks);
     TDLB_BCK(cudaGetLastError());
 }
 
@@ -986,7 +1019,7 @@ int tdlb_batch_autotune(tdlb_batch b, int trials, double* best_ms) {
         try {
             for (const Cand& c : cands) {
                 b->vec = c.v; b->threads = c.nt; b->bps = c.bps;
-                build_work(b);
+                        build_work(b);
                 launch_fused(b, b->d_steps, b->work, nullptr, b->stream);   // warm-up
                 TDLB_BCK(cudaEventRecord(e0, b->stream));
                 for (int r = 0; r < trials; r++) launch_fused(b, b->d_steps, b->work, nullptr, b->stream);
