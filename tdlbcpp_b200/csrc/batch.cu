@@ -78,12 +78,16 @@ __device__ __forceinline__ void tank_quad(const TankStep& ts, unsigned t) {
 // Quads of `NT` threads a work item covers: the tank's view is staged in
 // shared memory once per item.
 constexpr int kBatchChunks = 8;
-// Chunks ahead of the one a block starts that it prefetches into L2. Measured
-// on B200 over the 64-tank Esotwist batch (fused launch, ms): FP32 1.381
-// without, 1.267 one chunk ahead, 1.318 two; FP16 1.027, 1.011, 1.016. (A
+// How far ahead of the chunk a block starts it prefetches into L2: about this
+// many cells, at least one chunk (a chunk is NT x V cells). Measured on B200:
+// the 64-tank Esotwist batch at its autotuned shapes (FP32 256-cell chunks,
+// FP16 1024-cell chunks; fused launch, ms): FP32 1.381 without, 1.267 one
+// chunk ahead, 1.318 two; FP16 1.027, 1.011, 1.016. The server's batches at
+// the default shape (128-cell chunks), the first 64 requests of the serving
+// stream: 20,623 MLUPS without, 20,373 one chunk ahead, 21,243 two. (A
 // prefetch one wave of resident blocks ahead, as in the plain kernels, spans
 // 8-chunk items and overran L2: 1.52 ms.)
-constexpr int kBatchPrefetchChunks = 1;
+constexpr int kBatchPrefetchCells = 256;
 
 // L2 prefetch of the chunk of NT quads from quad q0 of the staged tank: NQ + 1
 // threads issue one bulk prefetch each (plane d's source span of the chunk's
@@ -405,13 +409,14 @@ void advance_step_state(tdlb_lattice* h) {
 // The fused launch over `work`: persistent blocks (bps per SM, each taking
 // items b, b + grid, ...) or, with bps = 0, one block per item, so that the
 // block scheduler fills the SMs the other group's forcing pass leaves free.
-// A block prefetches the chunk kBatchPrefetchChunks chunks after the one it
-// starts, within its item.
+// A block prefetches the chunk about kBatchPrefetchCells cells after the one
+// it starts, within its item.
 void launch_fused(tdlb_batch_s* b, const TankStep* d_views, const WorkList& work, int* counter, cudaStream_t st) {
     if (work.n == 0) return;
     const tdlb::BatchFn fn = tdlb::batch_kernel(storage_of(b), eso_of(b), b->vec, b->threads);
     const int grid = b->bps > 0 ? std::min(work.n, b->sms * b->bps) : work.n;
-    fn<<<grid, b->threads, 0, st>>>(d_views, work.d, work.n, counter, tdlb::kBatchPrefetchChunks);
+    const int ahead = std::max(1, tdlb::kBatchPrefetchCells / (b->threads * b->vec));
+    fn<<<grid, b->threads, 0, st>>>(d_views, work.d, work.n, counter, ahead);
     TDLB_BCK(cudaGetLastError());
 }
 
