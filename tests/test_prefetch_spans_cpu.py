@@ -9,7 +9,9 @@ widths and wave sizes, that each span starts on a 16-byte boundary, has a
 non-zero size that is a multiple of 16 bytes, and stays inside its plane's
 allocation (every plane starts 16-byte aligned and holds a multiple of 64
 elements) -- and that it covers every element the target tiles' threads
-pull from that plane away from the walls and the periodic wrap.
+pull from that plane away from the walls and the periodic wrap. The
+batched kernel's per-chunk prefetch (`prefetch_chunk`, csrc/batch.cu) takes
+the same spans over one chunk and is checked the same way.
 """
 import numpy as np
 import pytest
@@ -98,3 +100,33 @@ def test_prefetch_spans_cover_the_pulls(shape, V, eso, even):
         assert ((byte[sel] >= lo_r[sel]) & (byte[sel] + es <= hi_r[sel])).all(), d
         checked += int(sel.sum())
     assert checked > 0
+
+
+@pytest.mark.parametrize("shape", [(48, 48, 48), (33, 17, 29)])
+@pytest.mark.parametrize("V,NT", [(1, 128), (2, 128), (2, 256), (4, 256)])
+@pytest.mark.parametrize("es", [2, 4])
+@pytest.mark.parametrize("eso,even", [(False, False), (True, True), (True, False)])
+def test_batched_chunk_spans_in_bounds_and_aligned(shape, V, NT, es, eso, even):
+    """`prefetch_chunk` (csrc/batch.cu): the chunk of NT quads from quad q0,
+    for every chunk start a block can prefetch (every multiple of NT up to
+    the tank's quads, and the ones past its end that a short last item
+    asks for)."""
+    nx, ny, nz = shape
+    kp, plane = dims(nx, ny, nz)
+    nquads = nx * ny * (kp // V)
+    q0 = np.arange(0, nquads + 2 * NT * 8, NT, dtype=np.int64)
+    e0 = q0 * V
+    e1 = e0 + NT * V
+    for d in range(18):
+        sh = shift(d, nx, ny, kp, eso, even)
+        a = np.clip(e0 + sh - 1, 0, plane)
+        z = np.clip(e1 + sh + 1, 0, plane)
+        ok = a < z
+        lo = (a[ok] * es) // 16 * 16
+        hi = (z[ok] * es + 15) // 16 * 16
+        assert (hi > lo).all() and (lo >= 0).all() and (hi <= plane * es).all(), d
+    # Nu (FP32) spans
+    a = np.clip(e0, 0, plane)
+    z = np.clip(e1, 0, plane)
+    ok = a < z
+    assert ((z[ok] * 4 + 15) // 16 * 16 <= plane * 4).all()
